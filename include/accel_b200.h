@@ -1,0 +1,184 @@
+/*
+ * accel_b200.h -- C ABI of the B200 Fourier-domain acceleration/jerk search
+ * engine (libaccel_b200.so).
+ *
+ * The engine is a drop-in for the hot path of PRESTO's accelsearch:
+ * template generation (create_subharminfos), plane generation
+ * (subharm_fderivs_vol), harmonic summing (add_ffdotpows,
+ * inmem_add_ffdotpows) and threshold search (search_ffdotpows).  Plain
+ * pointers and sizes only; no CUDA or torch types cross this boundary.
+ * Every call returns AB_OK (0) or a negative AB_ERR_* code; the message of
+ * the last error on a context is available from ab_ctx_last_error().
+ *
+ * Reference interface each entry point replaces (PRESTO 6.0.1):
+ *   ab_obs_init             create_accelobs           src/accel_utils.c:1455-1805
+ *                                                     (geometry/thresholds part)
+ *   ab_prepare              create_subharminfos       src/accel_utils.c:240-288
+ *   ab_subharm_fderivs_vol  subharm_fderivs_vol       src/accel_utils.c:1024-1198
+ *   ab_add_ffdotpows        add_ffdotpows             src/accel_utils.c:1261-1282
+ *   ab_fund_to_ffdotplane   fund_to_ffdotplane        src/accel_utils.c:1219-1233
+ *   ab_inmem_add_ffdotpows  inmem_add_ffdotpows       src/accel_utils.c:1312-1361
+ *   ab_search_ffdotpows     search_ffdotpows          src/accel_utils.c:1412-1452
+ *   ab_search               the block/stage loop of   src/accelsearch.c:161-224
+ *   ab_sort_cands           sort_accelcands           src/accel_utils.c:364-384
+ *   ab_eliminate_harmonics  eliminate_harmonics       src/accel_utils.c:472-549
+ *   ab_candidate_sigma      candidate_sigma           src/characteristics.c:526-546
+ *   ab_power_for_sigma      power_for_sigma           src/characteristics.c:549-559
+ *   ab_gen_response         gen_w_response/gen_z_response/gen_r_response
+ *                                                     src/responses.c:159-418
+ */
+#ifndef ACCEL_B200_H
+#define ACCEL_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AB_OK              0
+#define AB_ERR_ARG        -1   /* invalid argument or unsupported geometry */
+#define AB_ERR_CUDA       -2   /* CUDA runtime error */
+#define AB_ERR_NOMEM      -3   /* device or host allocation failed */
+#define AB_ERR_OVERFLOW   -4   /* hit buffer or output array too small */
+#define AB_ERR_STATE      -5   /* call out of order (e.g. no spectrum) */
+#define AB_ERR_BUDGET     -6   /* request exceeds the HBM budget */
+
+/* fcomplex: include/ransomfft.h:13-16 (interleaved re, im) */
+typedef struct { float r, i; } ab_fcomplex;
+
+/* Search options that reach the hot path; the fields and defaults mirror
+ * the accelsearch command line (clig/accelsearch_cmd.cli,
+ * src/accelsearch_cmd.c:22-61).  Use ab_params_default() to fill them. */
+typedef struct {
+    long long N;          /* time-series samples (.inf N) */
+    double dt;            /* sample time, s (.inf dt) */
+    long long numbins;    /* complex bins in the .fft */
+    int zmax, wmax, wmaxP;/* -zmax, -wmax (wmaxP: -wmax given) */
+    int numharm;          /* -numharm (power of two, <= 32) */
+    float sigma;          /* -sigma */
+    double flo, fhi; int floP, fhiP;
+    double rlo, rhi; int rloP, rhiP;
+    long long lobin;      /* -lobin */
+    int inmemP;           /* -inmem */
+    float nph;            /* > 0: -photon normalisation with this level */
+} ab_params;
+
+/* accelobs geometry (include/accel.h:37-81), hot-path fields only. */
+typedef struct {
+    long long N, numbins, lobin, highestbin;
+    int maxkernlen, corr_uselen, fftlen, numharmstages, numz, numw;
+    int numbetween, inmem, norm_type, rstep;
+    double dt, T, rlo, rhi, dr, zlo, zhi, dz, wlo, whi, dw;
+    float nph, sigma;
+    float powcut[6];
+    long long numindep[6];
+} ab_obs;
+
+/* accelcand search fields (include/accel.h:83-95). */
+typedef struct {
+    float power, sigma;
+    int numharm;
+    double r, z, w;
+} ab_cand;
+
+/* ffdotpows (include/accel.h:120-130) with powers[numws][numzs][numrs]
+ * in caller-owned host memory. */
+typedef struct {
+    long long rlo;
+    int zlo, wlo, numrs, numzs, numws;
+    float *powers;
+    size_t capacity;      /* floats available at powers */
+} ab_ffdotpows;
+
+typedef struct ab_ctx ab_ctx;
+
+void ab_params_default(ab_params *p);
+
+/* Context: one per device and host thread. */
+int  ab_ctx_create(int device, ab_ctx **out);
+void ab_ctx_destroy(ab_ctx *ctx);
+const char *ab_ctx_last_error(const ab_ctx *ctx);
+void *ab_ctx_stream(ab_ctx *ctx);                 /* cudaStream_t of the context */
+int  ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes);
+
+/* Geometry + thresholds (create_accelobs).  Host only. */
+int ab_obs_init(const ab_params *p, ab_obs *obs);
+
+/* Template banks for obs (create_subharminfos); cached on the context. */
+int ab_prepare(ab_ctx *ctx, const ab_obs *obs);
+
+/* Whole-spectrum search: every block and harmonic stage of the main loop.
+ * fft holds obs->numbins bins; fft_on_device != 0 means fft is a device
+ * pointer, else a host pointer copied in by the call.  Candidates come back
+ * in the order the reference's list holds them (increasing r).
+ * first_block/max_blocks restrict the main loop (max_blocks < 0: all). */
+int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
+              long long first_block, long long max_blocks,
+              ab_cand *cands, long long maxcands, long long *numcands);
+
+/* Raw threshold crossings of the last ab_search, in reference visit order
+ * (block, stage, w, z, r): block ordinal, stage, w index, z index, r index,
+ * power.  Returns the count through *numhits. */
+int ab_last_hits(ab_ctx *ctx, long long *block, int *stage, int *wi, int *zi, int *ri,
+                 float *power, long long maxhits, long long *numhits);
+
+/* Per-function drop-ins (one block at a time).  ab_set_spectrum uploads the
+ * .fft bins used by later ab_subharm_fderivs_vol calls; the in-memory full
+ * f-fdot plane (accelobs.ffdotplane) stays resident on the device and is
+ * filled by ab_fund_to_ffdotplane.  fullrhi must equal
+ * fullrlo + rstep - ACCEL_DR, as in the reference's driver loop. */
+int ab_set_spectrum(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host);
+int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum,
+                           double fullrlo, double fullrhi, ab_ffdotpows *out);
+int ab_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
+                     const ab_ffdotpows *sub, int numharm, int harmnum, double fullrlo);
+int ab_fund_to_ffdotplane(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fund);
+int ab_inmem_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
+                           int numharm, int harmnum);
+
+/* Candidate list (the GSList of accelcand built by search_ffdotpows). */
+typedef struct ab_list ab_candlist;
+ab_candlist *ab_candlist_new(void);
+void ab_candlist_free(ab_candlist *l);
+long long ab_candlist_get(const ab_candlist *l, ab_cand *out, long long maxout);
+/* insert_new_accelcand (src/accel_utils.c:387-469); returns 1 if added. */
+int ab_candlist_insert(ab_candlist *l, float power, float sigma, int numharm,
+                       double r, double z, double w);
+int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd,
+                        int numharm, ab_candlist *list);
+
+/* Stage sums of one block of the last ab_search configuration, for parity
+ * checks: out[stage][numws][numzs][numrs] after each stage. */
+int ab_block_stage_sums(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host,
+                        long long block, float *out, size_t capacity);
+
+/* Template generation (kernel set a) on the device, FP64, returned as FP32
+ * (gen_w_response(roffset, numbetween, z, w, numkern)). */
+int ab_gen_response(ab_ctx *ctx, double roffset, int numbetween, double z, double w,
+                    int numkern, ab_fcomplex *out);
+
+/* The FFT'd template (w index wi, z index zi) of bank (numharm, harmnum)
+ * as stored on the device, and its device FFT length. */
+int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int wi, int zi,
+                   ab_fcomplex *out, int maxlen, int *fftlen_dev);
+
+/* Host-side statistics and candidate-list helpers. */
+double ab_candidate_sigma(double power, int numsum, double numtrials);
+double ab_power_for_sigma(double sigma, int numsum, double numtrials);
+double ab_chi2_logp(double chi2, double dof);
+double ab_equivalent_gaussian_sigma(double logp);
+int  ab_sort_cands(ab_cand *cands, long long n);
+long long ab_eliminate_harmonics(ab_cand *cands, long long n);
+
+/* Kernel timing (CUDA events around each launch on the context stream).
+ * kinds: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search. */
+int ab_ctx_set_profiling(ab_ctx *ctx, int on);
+int ab_ctx_kernel_times(ab_ctx *ctx, double *ms, long long *launches, int nkinds);
+int ab_ctx_reset_kernel_times(ab_ctx *ctx);
+long long ab_ctx_launch_count(ab_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

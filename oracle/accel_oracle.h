@@ -1,0 +1,154 @@
+/*
+ * accel_oracle.h -- CPU restatement of PRESTO's accelsearch hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the CUDA
+ * engine in presto_b200/: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load it.  Nothing
+ * in the product links against it.
+ *
+ * Each function restates the reference algorithm (PRESTO 6.0.1) and cites
+ * the reference file:line it follows.  The library is built twice from the
+ * same source (oracle/Makefile):
+ *   liboracle64.so  ORC_REAL=double -- the FP64 oracle used for parity
+ *   liboracle32.so  ORC_REAL=float  -- FP32 arithmetic like the reference's
+ *                                      FFTW single-precision path; used as
+ *                                      the timed CPU baseline
+ *
+ * Pinning: the response generators are pinned to the reference's own
+ * known-answer tests (tests/test_presto_python.py:117-146), the Fresnel
+ * integrals to the reference's fresnl.c compiled from its sources into
+ * oracle/_ref/, and the GSL-boundary statistics to scipy.special.  The full
+ * reference path needs FFTW3f, GSL and glib, which are absent, so it is not
+ * built; plane-level parity is therefore anchored on this restatement.
+ */
+#ifndef ACCEL_ORACLE_H
+#define ACCEL_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float r, i; } orc_fcomplex;          /* include/ransomfft.h:13-16 */
+
+/* Search options that reach the hot path (clig/accelsearch_cmd.cli). */
+typedef struct {
+    long long N;          /* samples in the time series (.inf N) */
+    double dt;            /* sample time (s) */
+    long long numbins;    /* complex bins in the .fft file */
+    int zmax, wmax, wmaxP;
+    int numharm;
+    float sigma;
+    double flo, fhi; int floP, fhiP;
+    double rlo, rhi; int rloP, rhiP;
+    long long lobin;
+    int inmemP;
+    float nph;            /* >0: photon normalisation (-photon) */
+} orc_params;
+
+/* Geometry subset of accelobs (include/accel.h:37-81). */
+typedef struct {
+    long long N, numbins, lobin, highestbin;
+    int maxkernlen, corr_uselen, fftlen, numharmstages, numz, numw;
+    int numbetween, inmem, norm_type, rstep;
+    double dt, T, rlo, rhi, dr, zlo, zhi, dz, wlo, whi, dw;
+    float nph, sigma;
+    float powcut[6];
+    long long numindep[6];
+} orc_obs;
+
+/* One plane (ffdotpows, include/accel.h:120-130), powers[w][z][r]. */
+typedef struct {
+    long long rlo;
+    int zlo, wlo, numrs, numzs, numws;
+    float *powers;
+    unsigned short *rinds, *zinds;     /* borrowed from the bank */
+} orc_ffdot;
+
+typedef struct orc_bank orc_bank;      /* subharminfo + its kernels */
+
+typedef struct {
+    float power, sigma;
+    int numharm;
+    double r, z, w;
+} orc_cand;
+
+typedef struct {
+    long long block;      /* block ordinal in the main loop */
+    int stage, wi, zi, ri;
+    float power;
+} orc_hit;
+
+/* ---- geometry ---- */
+int  orc_next_good_fftlen(int n);
+int  orc_fftlen_from_kernwidth(int kernwidth);
+int  orc_z_resp_halfwidth(double z);
+int  orc_w_resp_halfwidth(double z, double w);
+int  orc_calc_required_z(double harm_fract, double zfull);
+int  orc_calc_required_w(double harm_fract, double wfull);
+double orc_calc_required_r(double harm_fract, double rfull);
+int  orc_obs_init(const orc_params *p, orc_obs *obs);
+
+/* ---- statistics ---- */
+double orc_chi2_logp(double chi2, double dof);
+double orc_equivalent_gaussian_sigma(double logp);
+double orc_candidate_sigma(double power, int numsum, double numtrials);
+double orc_power_for_sigma(double sigma, int numsum, double numtrials);
+double orc_gauss_q(double x);
+double orc_gauss_qinv(double q);
+double orc_chisq_q(double chi2, double dof);
+double orc_chisq_qinv(double q, double dof);
+float  orc_median(float *arr, int n);
+
+/* ---- responses ---- */
+void orc_fresnel(double x, double *s, double *c);
+int  orc_gen_r_response(double roffset, int numbetween, int numkern, orc_fcomplex *out);
+int  orc_gen_z_response(double roffset, int numbetween, double z, int numkern, orc_fcomplex *out);
+int  orc_gen_w_response(double roffset, int numbetween, double z, double w, int numkern,
+                        orc_fcomplex *out);
+
+/* ---- FFT (unnormalised, sign -1 forward / +1 inverse) ---- */
+void orc_cfft_double(double *data, int n, int sign);
+
+/* ---- engine ---- */
+orc_bank *orc_bank_create(const orc_obs *obs, int numharm, int harmnum);
+void      orc_bank_free(orc_bank *b);
+int       orc_bank_info(const orc_bank *b, int *zmax, int *wmax, int *numkern_zdim,
+                        int *numkern_wdim, int *fftlen, int *halfwidth);
+int       orc_bank_kernel(const orc_bank *b, int wi, int zi, orc_fcomplex *out);
+
+int  orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int numharm,
+                             int harmnum, double fullrlo, double fullrhi, orc_bank *bank,
+                             orc_ffdot *out);
+void orc_ffdot_free(orc_ffdot *f);
+void orc_add_ffdotpows(orc_ffdot *fund, const orc_ffdot *sub, int numharm, int harmnum);
+void orc_fund_to_ffdotplane(const orc_ffdot *ffd, const orc_obs *obs, float *plane);
+void orc_inmem_add_ffdotpows(orc_ffdot *fund, const orc_obs *obs, const float *plane,
+                             int numharm, int harmnum);
+
+/* Full search (src/accelsearch.c:161-224).  Hits are recorded in visit
+ * order when hits != NULL.  max_blocks < 0 means all blocks; otherwise only
+ * blocks [first_block, first_block + max_blocks) of the main loop are
+ * searched (bounded CPU samples).  Returns number of candidates or < 0. */
+long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthreads,
+                          long long first_block, long long max_blocks,
+                          orc_cand *cands, long long maxcands,
+                          orc_hit *hits, long long maxhits, long long *numhits,
+                          long long *numblocks_done);
+
+/* Candidate list replay (src/accel_utils.c:387-469 and :1412-1452). */
+typedef struct orc_list orc_list;
+orc_list *orc_list_new(void);
+void      orc_list_free(orc_list *l);
+int       orc_list_insert(orc_list *l, float power, float sigma, int numharm,
+                          double rr, double zz, double ww);
+long long orc_list_get(const orc_list *l, orc_cand *out, long long maxout);
+void      orc_search_ffdotpows(const orc_ffdot *ffd, int numharm, const orc_obs *obs,
+                               orc_list *l, long long block, orc_hit *hits,
+                               long long maxhits, long long *numhits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,394 @@
+"""Python host mirror of the accelsearch hot path over the C ABI of
+libaccel_b200.so (include/accel_b200.h).
+
+Names, argument meanings and defaults follow PRESTO's accelsearch
+(clig/accelsearch_cmd.cli, src/accel_utils.c).  Every compute call goes to
+the CUDA engine; there is no CPU fallback: a missing library or a missing
+GPU raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libaccel_b200.so")
+
+AB_OK = 0
+ERRORS = {-1: "AB_ERR_ARG", -2: "AB_ERR_CUDA", -3: "AB_ERR_NOMEM", -4: "AB_ERR_OVERFLOW",
+          -5: "AB_ERR_STATE", -6: "AB_ERR_BUDGET"}
+
+# Every symbol include/accel_b200.h declares.
+EXPORTS = [
+    "ab_params_default", "ab_ctx_create", "ab_ctx_destroy", "ab_ctx_last_error",
+    "ab_ctx_stream", "ab_ctx_set_hbm_budget", "ab_obs_init", "ab_prepare", "ab_search",
+    "ab_last_hits", "ab_set_spectrum", "ab_subharm_fderivs_vol", "ab_add_ffdotpows",
+    "ab_fund_to_ffdotplane", "ab_inmem_add_ffdotpows", "ab_candlist_new", "ab_candlist_free",
+    "ab_candlist_get", "ab_candlist_insert", "ab_search_ffdotpows", "ab_block_stage_sums", "ab_gen_response",
+    "ab_bank_kernel", "ab_candidate_sigma", "ab_power_for_sigma", "ab_chi2_logp",
+    "ab_equivalent_gaussian_sigma", "ab_sort_cands", "ab_eliminate_harmonics",
+    "ab_ctx_set_profiling", "ab_ctx_kernel_times", "ab_ctx_reset_kernel_times",
+    "ab_ctx_launch_count",
+]
+
+
+class AccelError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    _fields_ = [("N", C.c_longlong), ("dt", C.c_double), ("numbins", C.c_longlong),
+                ("zmax", C.c_int), ("wmax", C.c_int), ("wmaxP", C.c_int),
+                ("numharm", C.c_int), ("sigma", C.c_float),
+                ("flo", C.c_double), ("fhi", C.c_double), ("floP", C.c_int), ("fhiP", C.c_int),
+                ("rlo", C.c_double), ("rhi", C.c_double), ("rloP", C.c_int), ("rhiP", C.c_int),
+                ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float)]
+
+
+class Obs(C.Structure):
+    _fields_ = [("N", C.c_longlong), ("numbins", C.c_longlong), ("lobin", C.c_longlong),
+                ("highestbin", C.c_longlong),
+                ("maxkernlen", C.c_int), ("corr_uselen", C.c_int), ("fftlen", C.c_int),
+                ("numharmstages", C.c_int), ("numz", C.c_int), ("numw", C.c_int),
+                ("numbetween", C.c_int), ("inmem", C.c_int), ("norm_type", C.c_int),
+                ("rstep", C.c_int),
+                ("dt", C.c_double), ("T", C.c_double), ("rlo", C.c_double), ("rhi", C.c_double),
+                ("dr", C.c_double), ("zlo", C.c_double), ("zhi", C.c_double), ("dz", C.c_double),
+                ("wlo", C.c_double), ("whi", C.c_double), ("dw", C.c_double),
+                ("nph", C.c_float), ("sigma", C.c_float),
+                ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6)]
+
+
+class Cand(C.Structure):
+    _fields_ = [("power", C.c_float), ("sigma", C.c_float), ("numharm", C.c_int),
+                ("r", C.c_double), ("z", C.c_double), ("w", C.c_double)]
+
+
+class FFDotPows(C.Structure):
+    _fields_ = [("rlo", C.c_longlong), ("zlo", C.c_int), ("wlo", C.c_int),
+                ("numrs", C.c_int), ("numzs", C.c_int), ("numws", C.c_int),
+                ("powers", C.POINTER(C.c_float)), ("capacity", C.c_size_t)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libaccel_b200.so (built in-tree by presto_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise AccelError(f"{LIBPATH} is missing: run presto_b200.build.build() first")
+    L = C.CDLL(LIBPATH)
+    vp, ll, i, d = C.c_void_p, C.c_longlong, C.c_int, C.c_double
+    L.ab_params_default.argtypes = [C.POINTER(Params)]
+    L.ab_ctx_create.argtypes = [i, C.POINTER(vp)]
+    L.ab_ctx_destroy.argtypes = [vp]
+    L.ab_ctx_last_error.restype = C.c_char_p
+    L.ab_ctx_last_error.argtypes = [vp]
+    L.ab_ctx_stream.restype = vp
+    L.ab_ctx_stream.argtypes = [vp]
+    L.ab_ctx_set_hbm_budget.argtypes = [vp, C.c_size_t]
+    L.ab_obs_init.argtypes = [C.POINTER(Params), C.POINTER(Obs)]
+    L.ab_prepare.argtypes = [vp, C.POINTER(Obs)]
+    L.ab_search.argtypes = [vp, C.POINTER(Obs), vp, i, ll, ll, C.POINTER(Cand), ll,
+                            C.POINTER(ll)]
+    L.ab_last_hits.argtypes = [vp, C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i),
+                               C.POINTER(i), C.POINTER(C.c_float), ll, C.POINTER(ll)]
+    L.ab_set_spectrum.argtypes = [vp, C.POINTER(Obs), vp]
+    L.ab_subharm_fderivs_vol.argtypes = [vp, C.POINTER(Obs), i, i, d, d, C.POINTER(FFDotPows)]
+    L.ab_add_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows),
+                                   C.POINTER(FFDotPows), i, i, d]
+    L.ab_fund_to_ffdotplane.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows)]
+    L.ab_inmem_add_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, i]
+    L.ab_candlist_new.restype = vp
+    L.ab_candlist_free.argtypes = [vp]
+    L.ab_candlist_get.restype = ll
+    L.ab_candlist_get.argtypes = [vp, C.POINTER(Cand), ll]
+    L.ab_candlist_insert.argtypes = [vp, C.c_float, C.c_float, i, d, d, d]
+    L.ab_search_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, vp]
+    L.ab_block_stage_sums.argtypes = [vp, C.POINTER(Obs), vp, ll, vp, C.c_size_t]
+    L.ab_gen_response.argtypes = [vp, d, i, d, d, i, vp]
+    L.ab_bank_kernel.argtypes = [vp, C.POINTER(Obs), i, i, i, i, vp, i, C.POINTER(i)]
+    for name in ("ab_candidate_sigma", "ab_power_for_sigma"):
+        getattr(L, name).restype = d
+        getattr(L, name).argtypes = [d, i, d]
+    L.ab_chi2_logp.restype = d
+    L.ab_chi2_logp.argtypes = [d, d]
+    L.ab_equivalent_gaussian_sigma.restype = d
+    L.ab_equivalent_gaussian_sigma.argtypes = [d]
+    L.ab_sort_cands.argtypes = [C.POINTER(Cand), ll]
+    L.ab_eliminate_harmonics.restype = ll
+    L.ab_eliminate_harmonics.argtypes = [C.POINTER(Cand), ll]
+    L.ab_ctx_set_profiling.argtypes = [vp, i]
+    L.ab_ctx_kernel_times.argtypes = [vp, C.POINTER(d), C.POINTER(ll), i]
+    L.ab_ctx_reset_kernel_times.argtypes = [vp]
+    L.ab_ctx_launch_count.restype = ll
+    L.ab_ctx_launch_count.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def make_params(N, dt, numbins=None, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0,
+                fhi=10000.0, rlo=None, rhi=None, inmem=False, photon=None, lobin=0):
+    """accelsearch options (src/accelsearch_cmd.c:22-61 defaults).  wmax=None
+    means -wmax not given (an explicit -wmax 0 disables in-memory mode,
+    src/accel_utils.c:1795)."""
+    p = Params()
+    lib().ab_params_default(C.byref(p))
+    p.N, p.dt = int(N), float(dt)
+    p.numbins = int(numbins if numbins is not None else N // 2)
+    p.zmax, p.numharm, p.sigma = int(zmax), int(numharm), float(sigma)
+    if wmax is not None:
+        p.wmax, p.wmaxP = int(wmax), 1
+    if rlo is not None:
+        p.rlo, p.rloP, p.floP = float(rlo), 1, 0
+    else:
+        p.flo = float(flo)
+    if rhi is not None:
+        p.rhi, p.rhiP, p.fhiP = float(rhi), 1, 0
+    else:
+        p.fhi = float(fhi)
+    p.inmemP = int(bool(inmem))
+    p.nph = float(photon) if photon else 0.0
+    p.lobin = int(lobin)
+    return p
+
+
+def obs_init(params):
+    o = Obs()
+    rc = lib().ab_obs_init(C.byref(params), C.byref(o))
+    if rc:
+        raise AccelError(f"ab_obs_init: {ERRORS.get(rc, rc)}")
+    return o
+
+
+def num_blocks(obs):
+    n, startr = 0, obs.rlo
+    while startr + obs.rstep < obs.highestbin:
+        n += 1
+        startr += obs.rstep
+    return n
+
+
+class Context:
+    """One CUDA context (device, stream, template-bank cache, scratch)."""
+
+    def __init__(self, device=0):
+        self.L = lib()
+        self.ptr = C.c_void_p()
+        rc = self.L.ab_ctx_create(int(device), C.byref(self.ptr))
+        if rc:
+            raise AccelError(f"ab_ctx_create(device={device}) failed: {ERRORS.get(rc, rc)}")
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self.L.ab_ctx_last_error(self.ptr)
+            raise AccelError(f"{what}: {ERRORS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.ptr:
+            self.L.ab_ctx_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self.L.ab_ctx_stream(self.ptr)
+
+    def prepare(self, obs):
+        self._check(self.L.ab_prepare(self.ptr, C.byref(obs)), "ab_prepare")
+
+    def search(self, obs, fft, first_block=0, max_blocks=-1, maxcands=1 << 20, device_ptr=None):
+        """All blocks and stages of the main search loop; returns the
+        candidate list in the reference's order as a list of tuples
+        (power, sigma, numharm, r, z, w)."""
+        cands = (Cand * maxcands)()
+        n = C.c_longlong()
+        if device_ptr is not None:
+            src, on_dev = C.c_void_p(device_ptr), 1
+        else:
+            fft = np.ascontiguousarray(fft, dtype=np.complex64)
+            if fft.size < obs.numbins:
+                raise AccelError("spectrum shorter than obs.numbins")
+            src, on_dev = C.c_void_p(fft.ctypes.data), 0
+        self._check(self.L.ab_search(self.ptr, C.byref(obs), src, on_dev, int(first_block),
+                                     int(max_blocks), cands, maxcands, C.byref(n)), "ab_search")
+        return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in cands[:n.value]]
+
+    def last_hits(self):
+        n = C.c_longlong()
+        self.L.ab_last_hits(self.ptr, None, None, None, None, None, None, 0, C.byref(n))
+        m = n.value
+        blk = np.zeros(m, np.int64)
+        st, wi, zi, ri = (np.zeros(m, np.int32) for _ in range(4))
+        pw = np.zeros(m, np.float32)
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))
+        self._check(self.L.ab_last_hits(self.ptr, P(blk, C.c_longlong), P(st, C.c_int),
+                                        P(wi, C.c_int), P(zi, C.c_int), P(ri, C.c_int),
+                                        P(pw, C.c_float), m, C.byref(n)), "ab_last_hits")
+        return blk, st, wi, zi, ri, pw
+
+    def block_stage_sums(self, obs, fft, block):
+        nws = max(obs.numw, 1)
+        out = np.zeros((obs.numharmstages, nws, obs.numz, obs.corr_uselen), np.float32)
+        fft = np.ascontiguousarray(fft, dtype=np.complex64)
+        self._check(self.L.ab_block_stage_sums(self.ptr, C.byref(obs), fft.ctypes.data,
+                                               int(block), out.ctypes.data, out.size),
+                    "ab_block_stage_sums")
+        return out
+
+    # ---- per-function drop-ins -------------------------------------------------
+    def set_spectrum(self, obs, fft):
+        fft = np.ascontiguousarray(fft, dtype=np.complex64)
+        self._check(self.L.ab_set_spectrum(self.ptr, C.byref(obs), fft.ctypes.data),
+                    "ab_set_spectrum")
+
+    def subharm_fderivs_vol(self, obs, numharm, harmnum, fullrlo, fullrhi):
+        f = FFDotPows()
+        self.L.ab_subharm_fderivs_vol(self.ptr, C.byref(obs), numharm, harmnum, fullrlo,
+                                      fullrhi, C.byref(f))        # sizes only
+        need = f.numws * f.numzs * f.numrs
+        buf = np.zeros(max(need, 1), np.float32)
+        f.powers = buf.ctypes.data_as(C.POINTER(C.c_float))
+        f.capacity = buf.size
+        self._check(self.L.ab_subharm_fderivs_vol(self.ptr, C.byref(obs), numharm, harmnum,
+                                                  fullrlo, fullrhi, C.byref(f)),
+                    "ab_subharm_fderivs_vol")
+        meta = dict(rlo=f.rlo, zlo=f.zlo, wlo=f.wlo, numrs=f.numrs, numzs=f.numzs,
+                    numws=f.numws)
+        return meta, buf[:need].reshape(f.numws, f.numzs, f.numrs).copy()
+
+    @staticmethod
+    def _ffd(meta, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float32)
+        f = FFDotPows(meta["rlo"], meta["zlo"], meta["wlo"], meta["numrs"], meta["numzs"],
+                      meta["numws"], arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size)
+        return f, arr
+
+    def add_ffdotpows(self, obs, fund_meta, fund, sub_meta, sub, numharm, harmnum, fullrlo):
+        ff, fa = self._ffd(fund_meta, fund.copy())
+        sf, sa = self._ffd(sub_meta, sub)
+        self._check(self.L.ab_add_ffdotpows(self.ptr, C.byref(obs), C.byref(ff), C.byref(sf),
+                                            numharm, harmnum, fullrlo), "ab_add_ffdotpows")
+        return fa
+
+    def fund_to_ffdotplane(self, obs, meta, fund):
+        f, a = self._ffd(meta, fund)
+        self._check(self.L.ab_fund_to_ffdotplane(self.ptr, C.byref(obs), C.byref(f)),
+                    "ab_fund_to_ffdotplane")
+
+    def inmem_add_ffdotpows(self, obs, meta, fund, numharm, harmnum):
+        f, a = self._ffd(meta, fund.copy())
+        self._check(self.L.ab_inmem_add_ffdotpows(self.ptr, C.byref(obs), C.byref(f), numharm,
+                                                  harmnum), "ab_inmem_add_ffdotpows")
+        return a
+
+    def search_ffdotpows(self, obs, meta, plane, numharm, candlist):
+        f, a = self._ffd(meta, plane)
+        self._check(self.L.ab_search_ffdotpows(self.ptr, C.byref(obs), C.byref(f), numharm,
+                                               candlist.ptr), "ab_search_ffdotpows")
+
+    def gen_response(self, kind, numbetween, numkern, z=0.0, w=0.0, roffset=0.0):
+        out = np.zeros(numkern, np.complex64)
+        if kind == "r":
+            z, w = 0.0, 0.0
+        elif kind == "z":
+            w = 0.0
+        self._check(self.L.ab_gen_response(self.ptr, roffset, numbetween, z, w, numkern,
+                                           out.ctypes.data), "ab_gen_response")
+        return out
+
+    def bank_kernel(self, obs, numharm, harmnum, wi, zi):
+        L = C.c_int()
+        self._check(self.L.ab_bank_kernel(self.ptr, C.byref(obs), numharm, harmnum, wi, zi,
+                                          None, 0, C.byref(L)), "ab_bank_kernel")
+        out = np.zeros(L.value, np.complex64)
+        self._check(self.L.ab_bank_kernel(self.ptr, C.byref(obs), numharm, harmnum, wi, zi,
+                                          out.ctypes.data, L.value, C.byref(L)), "ab_bank_kernel")
+        return out
+
+    # ---- timing -------------------------------------------------------------
+    def set_profiling(self, on):
+        self.L.ab_ctx_set_profiling(self.ptr, int(on))
+
+    def kernel_times(self):
+        ms = (C.c_double * 4)()
+        n = (C.c_longlong * 4)()
+        self.L.ab_ctx_kernel_times(self.ptr, ms, n, 4)
+        return list(ms), list(n)
+
+    def reset_kernel_times(self):
+        self.L.ab_ctx_reset_kernel_times(self.ptr)
+
+    def launch_count(self):
+        return self.L.ab_ctx_launch_count(self.ptr)
+
+
+class CandList:
+    """The candidate list search_ffdotpows grows (GSList of accelcand)."""
+
+    def __init__(self):
+        self.L = lib()
+        self.ptr = self.L.ab_candlist_new()
+
+    def insert(self, power, sigma, numharm, r, z, w):
+        return self.L.ab_candlist_insert(self.ptr, power, sigma, numharm, r, z, w)
+
+    def get(self):
+        n = self.L.ab_candlist_get(self.ptr, None, 0)
+        arr = (Cand * max(n, 1))()
+        self.L.ab_candlist_get(self.ptr, arr, n)
+        return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in arr[:n]]
+
+    def __del__(self):
+        try:
+            self.L.ab_candlist_free(self.ptr)
+        except Exception:
+            pass
+
+
+def candidate_sigma(power, numsum, numtrials):
+    return lib().ab_candidate_sigma(float(power), int(numsum), float(numtrials))
+
+
+def power_for_sigma(sigma, numsum, numtrials):
+    return lib().ab_power_for_sigma(float(sigma), int(numsum), float(numtrials))
+
+
+def sort_cands(cands):
+    n = len(cands)
+    arr = (Cand * max(n, 1))(*[Cand(*c) for c in cands])
+    lib().ab_sort_cands(arr, n)
+    return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in arr[:n]]
+
+
+def eliminate_harmonics(cands):
+    n = len(cands)
+    arr = (Cand * max(n, 1))(*[Cand(*c) for c in cands])
+    m = lib().ab_eliminate_harmonics(arr, n)
+    return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in arr[:m]]
+
+
+class AccelSearch:
+    """accelsearch for one spectrum: options as on the command line."""
+
+    def __init__(self, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0, fhi=10000.0,
+                 rlo=None, rhi=None, inmem=False, photon=None, lobin=0, device=0, ctx=None):
+        self.opts = dict(zmax=zmax, wmax=wmax, numharm=numharm, sigma=sigma, flo=flo, fhi=fhi,
+                         rlo=rlo, rhi=rhi, inmem=inmem, photon=photon, lobin=lobin)
+        self.ctx = ctx or Context(device)
+
+    def obs(self, N, dt, numbins=None):
+        return obs_init(make_params(N, dt, numbins, **self.opts))
+
+    def __call__(self, fft, N, dt):
+        fft = np.ascontiguousarray(fft, dtype=np.complex64)
+        obs = self.obs(N, dt, fft.size)
+        return self.ctx.search(obs, fft)

@@ -1,0 +1,846 @@
+// ab_engine.cu -- device orchestration behind the C ABI of accel_b200.h:
+// context and memory management, the template-bank cache, block batching of
+// the whole-spectrum search, the per-function drop-ins, and kernel timing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ab_host.h"
+#include "ab_index.h"
+#include "ab_kernels.h"
+
+using namespace ab;
+
+namespace {
+
+constexpr int kTwLog2 = 14;                 // FP64 twiddle table for FFTs up to 16384
+constexpr int kNumKinds = 4;                // templates, prep, corr, harmsum
+
+template <typename T> struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t want)
+    {
+        if (want <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) n = want;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+struct ab_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    size_t hbm_budget = 0;
+    size_t scratch_budget = 8ull << 30;
+
+    // template banks
+    ab_bankset bs{};
+    bool have_banks = false;
+    int bank_inmem = -1;
+    DevBuf<float2> tmpl;
+    DevBuf<ab_bank> dbanks;
+    DevBuf<double2> tw64;
+    DevBuf<float2> resp;
+
+    // spectrum, scratch, planes
+    DevBuf<float2> fft;
+    long long fft_bins = 0;
+    bool fft_valid = false;
+    DevBuf<float2> xhat;
+    DevBuf<float> planes;
+    DevBuf<float> fullplane;
+    DevBuf<double> startr;
+    DevBuf<CorrItem> items;
+    DevBuf<float> dbg;
+    DevBuf<float> tmpa, tmpb;
+
+    // hits
+    DevBuf<unsigned long long> keys;
+    DevBuf<float> pows;
+    DevBuf<unsigned int> count;
+    unsigned int hit_cap = 1u << 23;
+    std::vector<unsigned long long> hkeys;
+    std::vector<float> hpows;
+    std::vector<double> hstart;
+
+    // timing
+    bool prof = false;
+    double kms[kNumKinds] = {0, 0, 0, 0};
+    long long kn[kNumKinds] = {0, 0, 0, 0};
+    long long launches = 0;
+    std::vector<cudaEvent_t> evpool;
+    std::vector<std::pair<int, int>> evpending;   // (kind, event index)
+    int evused = 0;
+};
+
+static int fail(ab_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(ctx, AB_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                    \
+                        cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+
+// ---- timing helpers -------------------------------------------------------
+static void tick(ab_ctx *ctx, int kind, bool begin)
+{
+    if (!ctx->prof) return;
+    if (ctx->evused >= (int) ctx->evpool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->evpool.push_back(e);
+    }
+    int idx = ctx->evused++;
+    cudaEventRecord(ctx->evpool[idx], ctx->stream);
+    if (!begin) ctx->evpending.push_back({kind, idx});
+}
+
+static void harvest(ab_ctx *ctx)
+{
+    if (!ctx->prof) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &pe : ctx->evpending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->evpool[pe.second - 1], ctx->evpool[pe.second]);
+        ctx->kms[pe.first] += ms;
+        ctx->kn[pe.first] += 1;
+    }
+    ctx->evpending.clear();
+    ctx->evused = 0;
+}
+
+// ---- banks ----------------------------------------------------------------
+static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
+{
+    ab_bankset nb;
+    int rc = ab_bankset_init(obs, &nb);
+    if (rc) return fail(ctx, rc, "unsupported search geometry (FFT span above 4096 or "
+                                 "circular wrap into valid cells)");
+    bool same = ctx->have_banks && nb.nbanks == ctx->bs.nbanks;
+    for (int i = 0; same && i < nb.nbanks; i++) {
+        const ab_bank &a = nb.b[i], &b = ctx->bs.b[i];
+        same = a.numharm == b.numharm && a.harmnum == b.harmnum && a.zmax == b.zmax &&
+               a.wmax == b.wmax && a.L == b.L;
+    }
+    if (same) {
+        // strides (numrs_max) may change with the spectrum length; templates do not
+        ctx->bs = nb;
+        CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks,
+                           cudaMemcpyHostToDevice, ctx->stream));
+        return AB_OK;
+    }
+    if (ctx->tw64.n == 0) {
+        CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
+        launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
+        CK(cudaGetLastError());
+    }
+    CK(ctx->tmpl.ensure((size_t) nb.tmpl_total));
+    CK(ctx->dbanks.ensure(AB_MAX_BANKS));
+    CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    for (int i = 0; i < nb.nbanks; i++) {
+        tick(ctx, 0, true);
+        cudaError_t e = launch_templates(&nb.b[i], ctx->tmpl.p + nb.b[i].tmpl_off, nullptr,
+                                         ctx->tw64.p, kTwLog2, nullptr, 0, ctx->stream);
+        tick(ctx, 0, false);
+        ctx->launches++;
+        if (e != cudaSuccess)
+            return fail(ctx, AB_ERR_CUDA, "template generation failed: %s", cudaGetErrorString(e));
+    }
+    ctx->bs = nb;
+    ctx->have_banks = true;
+    return AB_OK;
+}
+
+static SearchConsts make_consts(const ab_obs *obs, const ab_bankset &bs)
+{
+    SearchConsts sc{};
+    sc.obs_zlo = obs->zlo;
+    sc.obs_wlo = obs->wlo;
+    sc.obs_rlo = obs->rlo;
+    sc.obs_lobin = obs->lobin;
+    sc.numbins = obs->numbins;
+    sc.rlen = (obs->highestbin + obs->corr_uselen) * (long long) AB_RDR;
+    sc.clip_col = (long long) obs->rlo * AB_RDR;
+    sc.corr_uselen = obs->corr_uselen;
+    sc.rstep = obs->rstep;
+    sc.numz = obs->numz;
+    sc.numws = obs->numw > 0 ? obs->numw : 1;
+    sc.stages = obs->numharmstages;
+    sc.inmem = obs->inmem;
+    sc.nbanks = bs.nbanks;
+    sc.nph = obs->nph;
+    for (int i = 0; i < AB_MAX_STAGES; i++) sc.powcut[i] = i < obs->numharmstages ? obs->powcut[i] : 0.f;
+    return sc;
+}
+
+// Correlation work items of one batch of nblk blocks, grouped by FFT length.
+struct CorrPlan {
+    std::vector<CorrItem> items;
+    int Ls[8];
+    int off[8], cnt[8];
+    int nL = 0;
+};
+
+static void build_corr_plan(const ab_bankset &bs, int nblk, int bank_lo, int bank_hi, CorrPlan &p)
+{
+    p.items.clear();
+    p.nL = 0;
+    for (int L = 512; L <= 4096; L <<= 1) {
+        int start = (int) p.items.size();
+        const int G = 4096 / L, tile = 16 * G;
+        for (int k = bank_lo; k < bank_hi; k++) {
+            const ab_bank &b = bs.b[k];
+            if (b.L != L) continue;
+            for (int t0 = 0; t0 < b.ntmpl; t0 += tile)
+                for (int bi = 0; bi < nblk; bi++)
+                    p.items.push_back(CorrItem{bi, k, t0, std::min(tile, b.ntmpl - t0)});
+        }
+        int n = (int) p.items.size() - start;
+        if (n > 0) {
+            p.Ls[p.nL] = L;
+            p.off[p.nL] = start;
+            p.cnt[p.nL] = n;
+            p.nL++;
+        }
+    }
+}
+
+static int run_corr(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, const CorrPlan &p,
+                    const CorrItem *ditems, float *planes, long long ppb, float *fullplane)
+{
+    for (int i = 0; i < p.nL; i++) {
+        tick(ctx, 2, true);
+        cudaError_t e = launch_corr(p.Ls[i], ctx->dbanks.p, sc, bb, ditems + p.off[i], p.cnt[i],
+                                    ctx->xhat.p, ctx->bs.xhat_per_block, ctx->tmpl.p, planes,
+                                    ppb, fullplane, ctx->stream);
+        tick(ctx, 2, false);
+        ctx->launches++;
+        if (e != cudaSuccess)
+            return fail(ctx, AB_ERR_CUDA, "correlation launch failed: %s", cudaGetErrorString(e));
+    }
+    return AB_OK;
+}
+
+static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                    int bank_lo, int bank_hi)
+{
+    tick(ctx, 1, true);
+    cudaError_t e = launch_prep(ctx->dbanks.p + bank_lo, ctx->bs.b + bank_lo, bank_hi - bank_lo,
+                                sc, bb, fft, ctx->xhat.p, ctx->bs.xhat_per_block, ctx->stream);
+    tick(ctx, 1, false);
+    ctx->launches += bank_hi - bank_lo;
+    if (e != cudaSuccess)
+        return fail(ctx, AB_ERR_CUDA, "prep launch failed: %s", cudaGetErrorString(e));
+    return AB_OK;
+}
+
+// Core search over main-loop blocks [first, first+count).  Hits accumulate in
+// the context's hit buffer (reset here).  dbg_block >= 0 dumps its stage sums.
+static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long long first,
+                       long long count, long long dbg_block)
+{
+    const ab_bankset &bs = ctx->bs;
+    SearchConsts sc = make_consts(obs, bs);
+    long long nmain = ab_num_blocks(obs), npre = ab_num_preblocks(obs);
+    if (first < 0) first = 0;
+    if (count < 0 || first + count > nmain) count = nmain - first;
+    if (count < 0) count = 0;
+    if (nmain >= (1ll << AB_KEY_BBITS) || sc.numz >= (1 << AB_KEY_ZBITS) ||
+        sc.numws >= (1 << AB_KEY_WBITS) || obs->corr_uselen >= (1 << AB_KEY_RBITS))
+        return fail(ctx, AB_ERR_ARG, "search too large for the hit key layout");
+    ctx->hstart.resize((size_t) (nmain + npre + 1));
+    ab_block_starts(obs, ctx->hstart.data(), nmain);
+    ab_preblock_starts(obs, ctx->hstart.data() + nmain, npre);
+    CK(ctx->startr.ensure(ctx->hstart.size()));
+    CK(cudaMemcpyAsync(ctx->startr.p, ctx->hstart.data(), sizeof(double) * (nmain + npre),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx->keys.ensure(ctx->hit_cap));
+    CK(ctx->pows.ensure(ctx->hit_cap));
+    CK(ctx->count.ensure(1));
+    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned), ctx->stream));
+    HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
+    const int nstage = obs->numharmstages;
+    const size_t dbg_floats = (size_t) nstage * sc.numws * sc.numz * obs->corr_uselen;
+    if (dbg_block >= 0) CK(ctx->dbg.ensure(dbg_floats));
+
+    if (obs->inmem) {
+        // full plane: every block (pre-pass and main loop) is correlated into
+        // it; sums read rows of lower frequency, so the whole plane comes first
+        long long nall = nmain + npre;
+        size_t rows = (size_t) sc.numz * sc.rlen;
+        CK(ctx->fullplane.ensure(rows));
+        long long first_col = 2 * (long long) (npre > 0 ? 8.0 : obs->rlo);
+        if (first_col > sc.rlen) first_col = sc.rlen;
+        if (first_col > 0)
+            CK(cudaMemset2DAsync(ctx->fullplane.p, sizeof(float) * sc.rlen, 0,
+                                 sizeof(float) * first_col, sc.numz, ctx->stream));
+        CK(ctx->xhat.ensure((size_t) std::max<long long>(nall, 1) * bs.xhat_per_block));
+        CorrPlan plan;
+        // item arrays are built per launch size
+        for (int pass = 0; pass < 2; pass++) {
+            long long nb = pass == 0 ? npre : nmain;
+            if (nb == 0) continue;
+            BlockBatch bb{ctx->startr.p + (pass == 0 ? nmain : 0), 0, (int) nb, pass == 0};
+            int rc = run_prep(ctx, sc, bb, dfft, 0, 1);
+            if (rc) return rc;
+            build_corr_plan(bs, (int) nb, 0, 1, plan);
+            CK(ctx->items.ensure(plan.items.size()));
+            CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
+                               cudaMemcpyHostToDevice, ctx->stream));
+            rc = run_corr(ctx, sc, bb, plan, ctx->items.p, nullptr, 0, ctx->fullplane.p);
+            if (rc) return rc;
+            // the item upload is reused by the next pass: wait before overwriting
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        if (count > 0) {
+            BlockBatch bb{ctx->startr.p + first, first, (int) count, 0};
+            tick(ctx, 3, true);
+            cudaError_t e = launch_harmsum_inmem(sc, bb, ctx->fullplane.p, hb,
+                                                 dbg_block >= 0 ? ctx->dbg.p : nullptr,
+                                                 (int) (dbg_block - first), ctx->stream);
+            tick(ctx, 3, false);
+            ctx->launches++;
+            if (e != cudaSuccess)
+                return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
+        }
+        return AB_OK;
+    }
+
+    // standard mode: batches of blocks, each correlated for every bank, then summed
+    const size_t per_block = (size_t) bs.plane_per_block * sizeof(float) +
+                             (size_t) bs.xhat_per_block * sizeof(float2);
+    long long B = (long long) (ctx->scratch_budget / std::max<size_t>(per_block, 1));
+    if (B < 1) B = 1;
+    if (B > 512) B = 512;
+    if (B > count) B = std::max<long long>(count, 1);
+    CK(ctx->planes.ensure((size_t) B * bs.plane_per_block));
+    CK(ctx->xhat.ensure((size_t) B * bs.xhat_per_block));
+    CorrPlan full, tail;
+    build_corr_plan(bs, (int) B, 0, bs.nbanks, full);
+    long long rem = count % B;
+    if (rem) build_corr_plan(bs, (int) rem, 0, bs.nbanks, tail);
+    CK(ctx->items.ensure(full.items.size() + tail.items.size()));
+    CK(cudaMemcpyAsync(ctx->items.p, full.items.data(), sizeof(CorrItem) * full.items.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    if (rem)
+        CK(cudaMemcpyAsync(ctx->items.p + full.items.size(), tail.items.data(),
+                           sizeof(CorrItem) * tail.items.size(), cudaMemcpyHostToDevice, ctx->stream));
+    for (long long b0 = first; b0 < first + count; b0 += B) {
+        int nb = (int) std::min<long long>(B, first + count - b0);
+        BlockBatch bb{ctx->startr.p + b0, b0, nb, 0};
+        int rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
+        if (rc) return rc;
+        const CorrPlan &p = (nb == B) ? full : tail;
+        const CorrItem *di = ctx->items.p + ((nb == B) ? 0 : full.items.size());
+        rc = run_corr(ctx, sc, bb, p, di, ctx->planes.p, bs.plane_per_block, nullptr);
+        if (rc) return rc;
+        int dbi = (dbg_block >= b0 && dbg_block < b0 + nb) ? (int) (dbg_block - b0) : -1;
+        tick(ctx, 3, true);
+        cudaError_t e = launch_harmsum_std(ctx->dbanks.p, sc, bb, ctx->planes.p, bs.plane_per_block,
+                                           hb, dbi >= 0 ? ctx->dbg.p : nullptr, dbi, ctx->stream);
+        tick(ctx, 3, false);
+        ctx->launches++;
+        if (e != cudaSuccess)
+            return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
+    }
+    return AB_OK;
+}
+
+static int fetch_hits(ab_ctx *ctx, long long *nhits)
+{
+    unsigned n = 0;
+    CK(cudaMemcpyAsync(&n, ctx->count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (n > ctx->hit_cap) {
+        ctx->hkeys.clear();
+        ctx->hpows.clear();
+        return fail(ctx, AB_ERR_OVERFLOW, "%u threshold crossings exceed the hit buffer (%u)", n,
+                    ctx->hit_cap);
+    }
+    ctx->hkeys.resize(n);
+    ctx->hpows.resize(n);
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->hkeys.data(), ctx->keys.p, sizeof(unsigned long long) * n,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->hpows.data(), ctx->pows.p, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    *nhits = n;
+    return AB_OK;
+}
+
+static int use_device(ab_ctx *ctx)
+{
+    CK(cudaSetDevice(ctx->device));
+    return AB_OK;
+}
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int ab_ctx_create(int device, ab_ctx **out)
+{
+    if (!out) return AB_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+        return AB_ERR_CUDA;
+    ab_ctx *ctx = new ab_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return AB_ERR_CUDA;
+    }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    ctx->hbm_budget = (size_t) (0.85 * (double) fr);
+    ctx->scratch_budget = std::min<size_t>(8ull << 30, ctx->hbm_budget / 4);
+    *out = ctx;
+    return AB_OK;
+}
+
+void ab_ctx_destroy(ab_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->tmpl.release();
+    ctx->dbanks.release();
+    ctx->tw64.release();
+    ctx->resp.release();
+    ctx->fft.release();
+    ctx->xhat.release();
+    ctx->planes.release();
+    ctx->fullplane.release();
+    ctx->startr.release();
+    ctx->items.release();
+    ctx->dbg.release();
+    ctx->tmpa.release();
+    ctx->tmpb.release();
+    ctx->keys.release();
+    ctx->pows.release();
+    ctx->count.release();
+    for (auto e : ctx->evpool) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *ab_ctx_last_error(const ab_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+void *ab_ctx_stream(ab_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+int ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes)
+{
+    if (!ctx || bytes == 0) return AB_ERR_ARG;
+    ctx->hbm_budget = bytes;
+    ctx->scratch_budget = std::min<size_t>(8ull << 30, bytes / 4);
+    return AB_OK;
+}
+
+int ab_prepare(ab_ctx *ctx, const ab_obs *obs)
+{
+    if (!ctx || !obs) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = ensure_banks(ctx, obs);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    harvest(ctx);
+    return AB_OK;
+}
+
+static int upload_spectrum(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft)
+{
+    CK(ctx->fft.ensure((size_t) obs->numbins));
+    CK(cudaMemcpyAsync(ctx->fft.p, fft, sizeof(float2) * obs->numbins, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    ctx->fft_bins = obs->numbins;
+    ctx->fft_valid = true;
+    return AB_OK;
+}
+
+int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
+              long long first_block, long long max_blocks, ab_cand *cands, long long maxcands,
+              long long *numcands)
+{
+    if (!ctx || !obs || !fft) return fail(ctx, AB_ERR_ARG, "null argument");
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = ensure_banks(ctx, obs);
+    if (rc) return rc;
+    const float2 *dfft;
+    if (fft_on_device) {
+        dfft = reinterpret_cast<const float2 *>(fft);
+    } else {
+        rc = upload_spectrum(ctx, obs, fft);
+        if (rc) return rc;
+        dfft = ctx->fft.p;
+    }
+    rc = search_core(ctx, obs, dfft, first_block, max_blocks, -1);
+    if (rc) return rc;
+    long long nh = 0;
+    rc = fetch_hits(ctx, &nh);
+    harvest(ctx);
+    if (rc) return rc;
+    ab_list *l = ab_list_new();
+    long long nmain = ab_num_blocks(obs);
+    rc = ab_replay_hits(obs, ctx->hkeys.data(), ctx->hpows.data(), nh, ctx->hstart.data(), nmain, l);
+    if (rc) {
+        ab_list_free(l);
+        return fail(ctx, rc, "hit replay failed");
+    }
+    long long n = ab_list_get(l, cands, maxcands);
+    ab_list_free(l);
+    if (numcands) *numcands = n;
+    if (cands && n > maxcands) return fail(ctx, AB_ERR_OVERFLOW, "%lld candidates > maxcands", n);
+    return AB_OK;
+}
+
+int ab_last_hits(ab_ctx *ctx, long long *block, int *stage, int *wi, int *zi, int *ri, float *power,
+                 long long maxhits, long long *numhits)
+{
+    if (!ctx) return AB_ERR_ARG;
+    long long n = (long long) ctx->hkeys.size();
+    std::vector<size_t> order(n);
+    for (long long i = 0; i < n; i++) order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](size_t a, size_t b) { return ctx->hkeys[a] < ctx->hkeys[b]; });
+    for (long long i = 0; i < n && i < maxhits; i++) {
+        unsigned long long k = ctx->hkeys[order[i]];
+        if (ri) ri[i] = (int) (k & 0xFFFF);
+        k >>= AB_KEY_RBITS;
+        if (zi) zi[i] = (int) (k & 0xFFF);
+        k >>= AB_KEY_ZBITS;
+        if (wi) wi[i] = (int) (k & 0x7F);
+        k >>= AB_KEY_WBITS;
+        if (stage) stage[i] = (int) (k & 0x7);
+        k >>= AB_KEY_SBITS;
+        if (block) block[i] = (long long) k;
+        if (power) power[i] = ctx->hpows[order[i]];
+    }
+    if (numhits) *numhits = n;
+    return n > maxhits ? AB_ERR_OVERFLOW : AB_OK;
+}
+
+int ab_block_stage_sums(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host,
+                        long long block, float *out, size_t capacity)
+{
+    if (!ctx || !obs || !fft_host || !out) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = ensure_banks(ctx, obs);
+    if (rc) return rc;
+    size_t need = (size_t) obs->numharmstages * (obs->numw > 0 ? obs->numw : 1) * obs->numz *
+                  obs->corr_uselen;
+    if (capacity < need) return fail(ctx, AB_ERR_OVERFLOW, "need %zu floats", need);
+    rc = upload_spectrum(ctx, obs, fft_host);
+    if (rc) return rc;
+    rc = search_core(ctx, obs, ctx->fft.p, block, 1, block);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out, ctx->dbg.p, sizeof(float) * need, cudaMemcpyDeviceToHost, ctx->stream));
+    long long nh;
+    rc = fetch_hits(ctx, &nh);
+    harvest(ctx);
+    return rc;
+}
+
+int ab_set_spectrum(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host)
+{
+    if (!ctx || !obs || !fft_host) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = upload_spectrum(ctx, obs, fft_host);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+static int find_bank(const ab_bankset &bs, int numharm, int harmnum)
+{
+    for (int i = 0; i < bs.nbanks; i++)
+        if (bs.b[i].numharm == numharm && bs.b[i].harmnum == harmnum) return i;
+    return -1;
+}
+
+int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum,
+                           double fullrlo, double fullrhi, ab_ffdotpows *out)
+{
+    if (!ctx || !obs || !out) return AB_ERR_ARG;
+    if (!ctx->fft_valid || ctx->fft_bins != obs->numbins)
+        return fail(ctx, AB_ERR_STATE, "no spectrum uploaded (ab_set_spectrum)");
+    if (fullrhi != fullrlo + obs->rstep - AB_DR)
+        return fail(ctx, AB_ERR_ARG, "fullrhi must be fullrlo + rstep - 0.5");
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = ensure_banks(ctx, obs);
+    if (rc) return rc;
+    int k = find_bank(ctx->bs, numharm, harmnum);
+    if (k < 0) return fail(ctx, AB_ERR_ARG, "no template bank for harmonic %d/%d", harmnum, numharm);
+    const ab_bank &b = ctx->bs.b[k];
+    ab_hgeom g = ab_harm_geom(fullrlo, fullrhi, numharm, harmnum, obs->zlo, obs->wlo,
+                              obs->corr_uselen);
+    size_t need = (size_t) b.nw * b.nz * g.numrs;
+    if (g.numrs > b.numrs_max)
+        return fail(ctx, AB_ERR_ARG, "block start %.1f is not on the search's block grid", fullrlo);
+    out->rlo = g.rlo;
+    out->zlo = g.zlo;
+    out->wlo = g.wlo;
+    out->numrs = g.numrs;
+    out->numzs = b.nz;
+    out->numws = b.nw;
+    if (!out->powers || out->capacity < need)
+        return fail(ctx, AB_ERR_OVERFLOW, "plane needs %zu floats", need);
+    SearchConsts sc = make_consts(obs, ctx->bs);
+    sc.inmem = 0;                              // the block plane, not the full plane
+    CK(ctx->startr.ensure(1));
+    CK(cudaMemcpyAsync(ctx->startr.p, &fullrlo, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx->xhat.ensure((size_t) ctx->bs.xhat_per_block));
+    CK(ctx->planes.ensure((size_t) ctx->bs.plane_per_block));
+    BlockBatch bb{ctx->startr.p, 0, 1, 0};
+    rc = run_prep(ctx, sc, bb, ctx->fft.p, k, k + 1);
+    if (rc) return rc;
+    CorrPlan plan;
+    build_corr_plan(ctx->bs, 1, k, k + 1, plan);
+    CK(ctx->items.ensure(plan.items.size()));
+    CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    rc = run_corr(ctx, sc, bb, plan, ctx->items.p, ctx->planes.p, ctx->bs.plane_per_block, nullptr);
+    if (rc) return rc;
+    CK(cudaMemcpy2DAsync(out->powers, sizeof(float) * g.numrs, ctx->planes.p + b.plane_off,
+                         sizeof(float) * b.numrs_max, sizeof(float) * g.numrs, (size_t) b.nw * b.nz,
+                         cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    harvest(ctx);
+    return AB_OK;
+}
+
+int ab_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund, const ab_ffdotpows *sub,
+                     int numharm, int harmnum, double fullrlo)
+{
+    if (!ctx || !obs || !fund || !sub) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    size_t nf = (size_t) fund->numws * fund->numzs * fund->numrs;
+    size_t ns = (size_t) sub->numws * sub->numzs * sub->numrs;
+    CK(ctx->tmpa.ensure(nf));
+    CK(ctx->tmpb.ensure(ns));
+    CK(cudaMemcpyAsync(ctx->tmpa.p, fund->powers, nf * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->tmpb.p, sub->powers, ns * 4, cudaMemcpyHostToDevice, ctx->stream));
+    double f = (double) harmnum / (double) numharm;
+    CK(launch_add_ffdot(ctx->tmpa.p, ctx->tmpb.p, fund->numws, fund->numzs, fund->numrs, sub->numzs,
+                        sub->numrs, f, fund->wlo, sub->wlo, fullrlo, sub->rlo, obs->zlo, sub->zlo,
+                        ctx->stream));
+    ctx->launches++;
+    CK(cudaMemcpyAsync(fund->powers, ctx->tmpa.p, nf * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_fund_to_ffdotplane(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fund)
+{
+    if (!ctx || !obs || !fund || !obs->inmem) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    long long rlen = (obs->highestbin + obs->corr_uselen) * (long long) AB_RDR;
+    size_t rows = (size_t) obs->numz * rlen;
+    bool fresh = ctx->fullplane.n < rows;
+    CK(ctx->fullplane.ensure(rows));
+    if (fresh) CK(cudaMemsetAsync(ctx->fullplane.p, 0, rows * sizeof(float), ctx->stream));
+    if (fund->rlo * AB_RDR + fund->numrs > rlen) return fail(ctx, AB_ERR_ARG, "block beyond plane");
+    CK(cudaMemcpy2DAsync(ctx->fullplane.p + fund->rlo * AB_RDR, sizeof(float) * rlen, fund->powers,
+                         sizeof(float) * fund->numrs, sizeof(float) * fund->numrs, fund->numzs,
+                         cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_inmem_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund, int numharm,
+                           int harmnum)
+{
+    if (!ctx || !obs || !fund || !obs->inmem) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    long long rlen = (obs->highestbin + obs->corr_uselen) * (long long) AB_RDR;
+    if (ctx->fullplane.n < (size_t) obs->numz * rlen)
+        return fail(ctx, AB_ERR_STATE, "no in-memory plane (ab_fund_to_ffdotplane)");
+    size_t nf = (size_t) fund->numzs * fund->numrs;
+    CK(ctx->tmpa.ensure(nf));
+    CK(cudaMemcpyAsync(ctx->tmpa.p, fund->powers, nf * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_inmem_add(ctx->tmpa.p, ctx->fullplane.p, rlen, fund->numzs, fund->numrs,
+                        (int) fund->rlo, fund->zlo, (double) harmnum / (double) numharm, ctx->stream));
+    ctx->launches++;
+    CK(cudaMemcpyAsync(fund->powers, ctx->tmpa.p, nf * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+ab_candlist *ab_candlist_new(void) { return ab_list_new(); }
+void ab_candlist_free(ab_candlist *l) { ab_list_free(l); }
+long long ab_candlist_get(const ab_candlist *l, ab_cand *out, long long maxout)
+{
+    return ab_list_get(l, out, maxout);
+}
+
+int ab_candlist_insert(ab_candlist *l, float power, float sigma, int numharm, double r, double z,
+                       double w)
+{
+    if (!l) return AB_ERR_ARG;
+    return ab_list_insert(l, power, sigma, numharm, r, z, w);
+}
+
+int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
+                        ab_candlist *list)
+{
+    if (!ctx || !obs || !ffd || !list) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    int stage = 0;
+    while ((1 << stage) < numharm) stage++;
+    if ((1 << stage) != numharm || stage >= obs->numharmstages) return fail(ctx, AB_ERR_ARG, "numharm");
+    size_t n = (size_t) ffd->numws * ffd->numzs * ffd->numrs;
+    CK(ctx->tmpa.ensure(n));
+    CK(cudaMemcpyAsync(ctx->tmpa.p, ffd->powers, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx->keys.ensure(ctx->hit_cap));
+    CK(ctx->pows.ensure(ctx->hit_cap));
+    CK(ctx->count.ensure(1));
+    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned), ctx->stream));
+    HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
+    CK(launch_threshold(ctx->tmpa.p, ffd->numws, ffd->numzs, ffd->numrs, obs->powcut[stage], stage,
+                        hb, ctx->stream));
+    ctx->launches++;
+    long long nh = 0;
+    rc = fetch_hits(ctx, &nh);
+    if (rc) return rc;
+    // keys hold (stage, w, z, r) with block 0; the plane's own rlo/zlo/wlo
+    // give the candidate coordinates (src/accel_utils.c:1431-1433)
+    std::vector<size_t> order(nh);
+    for (long long i = 0; i < nh; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return ctx->hkeys[a] < ctx->hkeys[b]; });
+    for (long long i = 0; i < nh; i++) {
+        unsigned long long k = ctx->hkeys[order[i]];
+        int ri = (int) (k & 0xFFFF);
+        k >>= AB_KEY_RBITS;
+        int zi = (int) (k & 0xFFF);
+        k >>= AB_KEY_ZBITS;
+        int wi = (int) (k & 0x7F);
+        float pw = ctx->hpows[order[i]];
+        float sig = (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
+        double rr = (ffd->rlo + ri * (double) AB_DR) / (double) numharm;
+        double zz = (ffd->zlo + zi * (double) AB_DZ) / (double) numharm;
+        double ww = (ffd->wlo + wi * (double) AB_DW) / (double) numharm;
+        ab_list_insert(list, pw, sig, numharm, rr, zz, ww);
+    }
+    return AB_OK;
+}
+
+int ab_gen_response(ab_ctx *ctx, double roffset, int numbetween, double z, double w, int numkern,
+                    ab_fcomplex *out)
+{
+    if (!ctx || !out) return AB_ERR_ARG;
+    if (roffset < 0.0 || roffset >= 1.0 || numbetween < 1 || numbetween >= 20000 ||
+        numkern < numbetween || numkern % (2 * numbetween))
+        return fail(ctx, AB_ERR_ARG, "bad response arguments (src/responses.c:344-360)");
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    if (ctx->tw64.n == 0) {
+        CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
+        launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
+    }
+    CK(ctx->resp.ensure((size_t) numkern));
+    cudaError_t e = launch_response(roffset, numbetween, z, w, numkern, ctx->resp.p, ctx->tw64.p,
+                                    kTwLog2, nullptr, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, AB_ERR_ARG, "response generation: %s", cudaGetErrorString(e));
+    ctx->launches++;
+    CK(cudaMemcpyAsync(out, ctx->resp.p, sizeof(float2) * numkern, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int wi, int zi,
+                   ab_fcomplex *out, int maxlen, int *fftlen_dev)
+{
+    if (!ctx || !obs) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    rc = ensure_banks(ctx, obs);
+    if (rc) return rc;
+    int k = find_bank(ctx->bs, numharm, harmnum);
+    if (k < 0) return fail(ctx, AB_ERR_ARG, "no bank %d/%d", harmnum, numharm);
+    const ab_bank &b = ctx->bs.b[k];
+    if (fftlen_dev) *fftlen_dev = b.L;
+    if (wi < 0 || wi >= b.nw || zi < 0 || zi >= b.nz) return fail(ctx, AB_ERR_ARG, "template index");
+    if (!out) return AB_OK;
+    if (maxlen < b.L) return fail(ctx, AB_ERR_OVERFLOW, "need %d", b.L);
+    CK(cudaMemcpyAsync(out, ctx->tmpl.p + b.tmpl_off + (long long) (wi * b.nz + zi) * b.L,
+                       sizeof(float2) * b.L, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    harvest(ctx);
+    return AB_OK;
+}
+
+int ab_ctx_set_profiling(ab_ctx *ctx, int on)
+{
+    if (!ctx) return AB_ERR_ARG;
+    ctx->prof = on != 0;
+    return AB_OK;
+}
+
+int ab_ctx_kernel_times(ab_ctx *ctx, double *ms, long long *launches, int nkinds)
+{
+    if (!ctx) return AB_ERR_ARG;
+    for (int i = 0; i < nkinds && i < kNumKinds; i++) {
+        if (ms) ms[i] = ctx->kms[i];
+        if (launches) launches[i] = ctx->kn[i];
+    }
+    return AB_OK;
+}
+
+int ab_ctx_reset_kernel_times(ab_ctx *ctx)
+{
+    if (!ctx) return AB_ERR_ARG;
+    for (int i = 0; i < kNumKinds; i++) {
+        ctx->kms[i] = 0;
+        ctx->kn[i] = 0;
+    }
+    ctx->launches = 0;
+    return AB_OK;
+}
+
+long long ab_ctx_launch_count(ab_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

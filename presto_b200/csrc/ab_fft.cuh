@@ -1,0 +1,258 @@
+// ab_fft.cuh -- shared-memory FFTs for sm_100a.
+//
+// FP32 complex FFT of power-of-two length L in [256, 4096], Stockham
+// auto-sort with radix-16 passes (plus one radix-2/4/8 pass), computed by a
+// "group" of NT = L/16 threads that each hold 16 points in registers in the
+// strided layout v[m] = x[t + NT*m].  A 256-thread CTA runs 4096/L groups
+// side by side; every group owns (L + L/16) float2 of padded shared memory.
+// Twiddles depend only on the thread, so they are computed once (FP64
+// sincospi, rounded to FP32) and kept in registers across transforms.
+//
+// FP64 complex FFT (radix-2, in shared memory) for the one-off template
+// generation.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ab {
+
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+// a * (S i)
+template <int S> __device__ __forceinline__ float2 mul_i(float2 a)
+{
+    return S < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+
+// exp(S 2 pi i m / 16) applied to a, with the trivial angles special-cased.
+template <int S, int M> __device__ __forceinline__ float2 tw16(float2 a)
+{
+    constexpr int m = M & 15;
+    constexpr float C1 = 0.92387953251128675613f;   // cos(pi/8)
+    constexpr float S1 = 0.38268343236508977173f;   // sin(pi/8)
+    constexpr float H = 0.70710678118654752440f;    // cos(pi/4)
+    if constexpr (m == 0) {
+        return a;
+    } else if constexpr (m == 4) {
+        return mul_i<S>(a);
+    } else if constexpr (m == 8) {
+        return make_float2(-a.x, -a.y);
+    } else if constexpr (m == 12) {
+        return mul_i<-S>(a);
+    } else if constexpr (m == 2 || m == 6 || m == 10 || m == 14) {
+        // (+-1 +- i) H
+        constexpr float cr = (m == 2 || m == 14) ? H : -H;
+        constexpr float ci = ((m == 2 || m == 6) ? H : -H) * (S < 0 ? -1.f : 1.f);
+        return make_float2(fmaf(a.x, cr, -a.y * ci), fmaf(a.x, ci, a.y * cr));
+    } else {
+        constexpr float cr = (m == 1 || m == 15) ? C1 : (m == 3 || m == 13) ? S1
+                           : (m == 5 || m == 11) ? -S1 : -C1;
+        constexpr float si = (m == 1 || m == 7) ? S1 : (m == 3 || m == 5) ? C1
+                           : (m == 9 || m == 15) ? -S1 : -C1;
+        constexpr float ci = si * (S < 0 ? -1.f : 1.f);
+        return make_float2(fmaf(a.x, cr, -a.y * ci), fmaf(a.x, ci, a.y * cr));
+    }
+}
+
+template <int S> __device__ __forceinline__ void dft2(float2 *x)
+{
+    float2 t = x[0];
+    x[0] = t + x[1];
+    x[1] = t - x[1];
+}
+
+template <int S> __device__ __forceinline__ void dft4v(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
+{
+    float2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_i<S>(a1 - a3);
+    a0 = t0 + t2;
+    a2 = t0 - t2;
+    a1 = t1 + t3;
+    a3 = t1 - t3;
+}
+
+template <int S> __device__ __forceinline__ void dft4(float2 *x) { dft4v<S>(x[0], x[1], x[2], x[3]); }
+
+template <int S> __device__ __forceinline__ void dft8(float2 *x)
+{
+    dft4v<S>(x[0], x[2], x[4], x[6]);
+    dft4v<S>(x[1], x[3], x[5], x[7]);
+    float2 o1 = tw16<S, 2>(x[3]), o2 = tw16<S, 4>(x[5]), o3 = tw16<S, 6>(x[7]);
+    float2 e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6], o0 = x[1];
+    x[0] = e0 + o0; x[4] = e0 - o0;
+    x[1] = e1 + o1; x[5] = e1 - o1;
+    x[2] = e2 + o2; x[6] = e2 - o2;
+    x[3] = e3 + o3; x[7] = e3 - o3;
+}
+
+template <int S> __device__ __forceinline__ void dft16(float2 *x)
+{
+    // n = 4 n1 + n2, k = k1 + 4 k2
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) dft4v<S>(x[n2], x[4 + n2], x[8 + n2], x[12 + n2]);
+    // x[n2 + 4 k1] = A[n2][k1]; twiddle by w16^(n2 k1)
+    x[5] = tw16<S, 1>(x[5]);
+    x[9] = tw16<S, 2>(x[9]);
+    x[13] = tw16<S, 3>(x[13]);
+    x[6] = tw16<S, 2>(x[6]);
+    x[10] = tw16<S, 4>(x[10]);
+    x[14] = tw16<S, 6>(x[14]);
+    x[7] = tw16<S, 3>(x[7]);
+    x[11] = tw16<S, 6>(x[11]);
+    x[15] = tw16<S, 9>(x[15]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) dft4v<S>(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+    // x[4 k1 + k2] = X[k1 + 4 k2]  -> natural order
+    float2 y[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) y[k1 + 4 * k2] = x[4 * k1 + k2];
+#pragma unroll
+    for (int i = 0; i < 16; i++) x[i] = y[i];
+}
+
+template <int R, int S> __device__ __forceinline__ void dft(float2 *x)
+{
+    if constexpr (R == 2) dft2<S>(x);
+    else if constexpr (R == 4) dft4<S>(x);
+    else if constexpr (R == 8) dft8<S>(x);
+    else dft16<S>(x);
+}
+
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+
+template <int L> struct FftShape {
+    static constexpr int NT = L / 16;                 // threads per transform
+    static constexpr int G = 256 / NT;                // transforms per 256-thread CTA
+    static constexpr int R3 = L / 256;                // radix of the third pass (1: none)
+    static constexpr int NB3 = (R3 > 1) ? 16 / R3 : 0;
+    static constexpr int NTW = 15 + NB3 * (R3 > 1 ? R3 - 1 : 0);
+    static constexpr int SMEM = L + L / 16;           // padded float2 per transform
+    static_assert(L >= 256 && L <= 4096 && (L & (L - 1)) == 0, "FFT length");
+};
+
+// Per-thread twiddles of passes 2 and 3 (pass 1 has none).
+template <int L, int S> struct FftTw {
+    float2 w[FftShape<L>::NTW];
+    __device__ __forceinline__ void init(int t)
+    {
+        using SH = FftShape<L>;
+        // pass 2: R = 16, LS = 16, one butterfly, k = t mod 16
+        {
+            int k = t & 15;
+#pragma unroll
+            for (int q = 1; q < 16; q++) {
+                double s, c;
+                sincospi(2.0 * (double) (q * k) / 256.0, &s, &c);
+                w[q - 1] = make_float2((float) c, (float) (S * s));
+            }
+        }
+        if constexpr (SH::R3 > 1) {
+#pragma unroll
+            for (int b = 0; b < SH::NB3; b++) {
+                int k = (t + SH::NT * b) & 255;
+#pragma unroll
+                for (int q = 1; q < SH::R3; q++) {
+                    double s, c;
+                    sincospi(2.0 * (double) (q * k) / (double) L, &s, &c);
+                    w[15 + b * (SH::R3 - 1) + q - 1] = make_float2((float) c, (float) (S * s));
+                }
+            }
+        }
+    }
+};
+
+// One Stockham pass.  v holds x[t + NT m]; results of a non-final pass go
+// through shared memory and come back in the same strided layout.
+template <int L, int R, int LS, int S, bool LAST, int TWOFF>
+__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const float2 *tw)
+{
+    constexpr int NT = L / 16, NB = 16 / R;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        float2 x[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) x[q] = v[b + q * NB];
+        if constexpr (LS > 1) {
+#pragma unroll
+            for (int q = 1; q < R; q++) x[q] = cmul(x[q], tw[TWOFF + b * (R - 1) + q - 1]);
+        }
+        dft<R, S>(x);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int s = 0; s < R; s++) v[b + s * NB] = x[s];
+        } else {
+            int j = t + NT * b;
+            int k = j & (LS - 1);
+            int base = (j - k) * R + k;
+#pragma unroll
+            for (int s = 0; s < R; s++) sm[pad16(base + s * LS)] = x[s];
+        }
+    }
+    if constexpr (!LAST) {
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; m++) v[m] = sm[pad16(t + NT * m)];
+        __syncthreads();
+    }
+}
+
+// Full transform of the group's data, in place in v.  Must be called by all
+// threads of the CTA (it contains __syncthreads).
+template <int L, int S>
+__device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const FftTw<L, S> &tw)
+{
+    using SH = FftShape<L>;
+    if constexpr (SH::R3 > 1) {
+        fft_pass<L, 16, 1, S, false, 0>(v, sm, t, tw.w);
+        fft_pass<L, 16, 16, S, false, 0>(v, sm, t, tw.w);
+        fft_pass<L, SH::R3, 256, S, true, 15>(v, sm, t, tw.w);
+    } else {
+        fft_pass<L, 16, 1, S, false, 0>(v, sm, t, tw.w);
+        fft_pass<L, 16, 16, S, true, 0>(v, sm, t, tw.w);
+    }
+}
+
+// ---------------------------------------------------------------------
+// FP64 radix-2 FFT in shared memory (templates).  tw[m] = exp(S 2 pi i m/n)
+// for m < n/2 (global table).  All threads of the CTA call it.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ double2 dmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ void fft64_inplace(double2 *x, int n, int log2n, const double2 *tw)
+{
+    // bit reversal
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int j = __brev(i) >> (32 - log2n);
+        if (j > i) {
+            double2 a = x[i];
+            x[i] = x[j];
+            x[j] = a;
+        }
+    }
+    __syncthreads();
+    for (int half = 1, st = n >> 1; half < n; half <<= 1, st >>= 1) {
+        for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
+            int grp = b / half, k = b - grp * half;
+            int i0 = grp * 2 * half + k, i1 = i0 + half;
+            double2 w = tw[k * st];
+            double2 u = x[i0], v = dmul(x[i1], w);
+            x[i0] = make_double2(u.x + v.x, u.y + v.y);
+            x[i1] = make_double2(u.x - v.x, u.y - v.y);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace ab

@@ -1,0 +1,826 @@
+// ab_kernels.cu -- sm_100a kernels of the acceleration/jerk search engine.
+//
+//   (a) k_templates   FP64 response templates (gen_w/z/r_response,
+//                     src/responses.c:159-418), placed (place_complex_kernel,
+//                     src/corr_prep.c:92-114) and FFT'd in FP64, stored FP32.
+//   (b) k_prep        per (block, harmonic): amplitudes with zero padding
+//                     (src/accel_utils.c:993-1022), block-median
+//                     normalisation (:1079-1099), spread (src/corr_prep.c:62-74)
+//                     and forward FFT (:1117-1121).
+//       k_corr<L>     template correlation: data * conj(kernel), inverse FFT,
+//                     |.|^2 / L^2 over the valid cells (:1140-1193).
+//   (c)+(d) k_harmsum_*  harmonic sums (add_ffdotpows :1261-1282,
+//                     inmem_add_ffdotpows :1312-1361) fused with the threshold
+//                     of search_ffdotpows (:1412-1452), hits compacted with
+//                     warp ballots into a (key, power) list.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "ab_fft.cuh"
+#include "ab_index.h"
+#include "ab_kernels.h"
+
+namespace ab {
+
+// ======================================================================
+// FP64 Fresnel integrals (power series / Lentz continued fraction for
+// erfc((1-i) sqrt(pi)/2 x), Numerical Recipes 2ed section 6.9).
+// ======================================================================
+__device__ void fresnel64(double xin, double *s, double *c)
+{
+    double x = fabs(xin), S, C;
+    if (x < 1e-300) {
+        S = 0.0;
+        C = 0.0;
+    } else if (x <= 1.8) {
+        double t = 0.5 * M_PI * x * x, term = x, sc = 0.0, ss = 0.0;
+        for (int k = 0; k < 200; k++) {
+            double contrib = term / (2 * k + 1);
+            switch (k & 3) {
+                case 0: sc += contrib; break;
+                case 1: ss += contrib; break;
+                case 2: sc -= contrib; break;
+                default: ss -= contrib; break;
+            }
+            term *= t / (k + 1);
+            if (k > 4 && fabs(term) < 1e-18 * (fabs(sc) + fabs(ss))) break;
+        }
+        C = sc;
+        S = ss;
+    } else {
+        const double fpmin = 1e-300;
+        double px2 = M_PI * x * x;
+        double br = 1.0, bi = -px2, cr = 1.0 / fpmin, ci = 0.0;
+        double den = br * br + bi * bi;
+        double dr = br / den, di = -bi / den, hr = dr, hi = di;
+        for (int n = 1; n < 100000; n++) {
+            double an = -(double) (2 * n - 1) * (double) (2 * n);
+            br += 4.0;
+            double tr = an * dr + br, ti = an * di + bi;
+            den = tr * tr + ti * ti;
+            dr = tr / den;
+            di = -ti / den;
+            den = cr * cr + ci * ci;
+            cr = br + an * cr / den;
+            ci = bi - an * ci / den;
+            double delr = cr * dr - ci * di, deli = cr * di + ci * dr;
+            double nhr = hr * delr - hi * deli, nhi = hr * deli + hi * delr;
+            hr = nhr;
+            hi = nhi;
+            if (fabs(delr - 1.0) + fabs(deli) < 1e-16) break;
+        }
+        double sp, cp;
+        sincospi(0.5 * x * x, &sp, &cp);             // e^{i pi x^2 / 2}
+        double ar = x * (cp + sp), ai = x * (sp - cp);
+        double fr = ar * hr - ai * hi, fi = ar * hi + ai * hr;
+        double gr = 1.0 - fr, gi = -fi;
+        C = 0.5 * (gr - gi);
+        S = 0.5 * (gr + gi);
+    }
+    if (xin < 0.0) {
+        C = -C;
+        S = -S;
+    }
+    *s = S;
+    *c = C;
+}
+
+// gen_r_response point c (src/responses.c:159-225), written with direct
+// sin/cos of the exact argument instead of the trig recursion.
+__device__ double2 r_resp_point(double roffset, int numbetween, int numkern, int c)
+{
+    double rbypi = numkern / (double) (2 * numbetween) + roffset - (double) c / numbetween;
+    double s, co;
+    sincospi(rbypi, &s, &co);
+    double r = M_PI * rbypi;
+    double sinc = (r == 0.0) ? 1.0 : s / r;
+    double2 v = make_double2(co * sinc, s * sinc);
+    if (roffset < 1E-3 && c == numkern / 2) {
+        double t = roffset * roffset;
+        v = make_double2(1 - 6.579736267392905746 * t, roffset * (M_PI - 10.335425560099940058 * t));
+    }
+    return v;
+}
+
+// gen_z_response point c (src/responses.c:228-316)
+__device__ double2 z_resp_point(double roffset, int numbetween, double z, int numkern, int c)
+{
+    double absz = fabs(z);
+    if (absz < 1E-4) return r_resp_point(roffset, numbetween, numkern, c);
+    double startr = roffset - (0.5 * z), ip;
+    double startroffset = (startr < 0) ? 1.0 + modf(startr, &ip) : modf(startr, &ip);
+    int signz = (z < 0.0) ? -1 : 1;
+    double zd = signz * M_SQRT2 / sqrt(absz);
+    double cons = zd / 2.0;
+    double pibyz = M_PI / z;
+    startr += numkern / (double) (2 * numbetween);
+    double r = startr + c * (-1.0 / numbetween);
+    double yy = r * zd;
+    double zz = yy + z * zd;
+    double xx = pibyz * r * r;
+    double sx, cx;
+    sincos(xx, &sx, &cx);
+    double fsy, fcy, fsz, fcz;
+    fresnel64(yy, &fsy, &fcy);
+    fresnel64(zz, &fsz, &fcz);
+    double tr = signz * (fcz - fcy), ti = fsy - fsz;
+    double2 v = make_double2((tr * cx - ti * sx) * cons, -(tr * sx + ti * cx) * cons);
+    if (startroffset < 1E-3 && absz < 1E-3 && c == numkern / 2) {
+        double z2 = z * z, x2 = startroffset * startroffset;
+        v.x = 1.0 - 0.16449340668482264365 * z2;
+        v.y = -0.5235987755982988731 * z;
+        v.x += startroffset * 1.6449340668482264365 * z;
+        v.y += startroffset * (M_PI - 0.5167712780049970029 * z2);
+        v.x += x2 * (-6.579736267392905746 + 0.9277056288952613070 * z2);
+        v.y += x2 * (3.1006276680299820175 * z);
+    }
+    return v;
+}
+
+__global__ void k_twiddle64(double2 *tw, int n, int sign)
+{
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n / 2) {
+        double s, c;
+        sincospi(2.0 * (double) m / (double) n, &s, &c);
+        tw[m] = make_double2(c, sign * s);
+    }
+}
+
+void launch_twiddle64(double2 *tw, int n, int sign, cudaStream_t st)
+{
+    k_twiddle64<<<(n / 2 + 255) / 256, 256, 0, st>>>(tw, n, sign);
+}
+
+__device__ __forceinline__ int ilog2(int n) { return 31 - __clz(n); }
+
+// FP64 radix-2 FFT with a shared twiddle table of exp(-2 pi i m / NMAX).
+__device__ void fft64_tab(double2 *x, int n, const double2 *tw, int nmax)
+{
+    int log2n = ilog2(n), tstride = nmax / n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int j = __brev(i) >> (32 - log2n);
+        if (j > i) {
+            double2 a = x[i];
+            x[i] = x[j];
+            x[j] = a;
+        }
+    }
+    __syncthreads();
+    for (int half = 1; half < n; half <<= 1) {
+        int st = (n / (2 * half)) * tstride;
+        for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
+            int grp = b / half, k = b - grp * half;
+            int i0 = grp * 2 * half + k, i1 = i0 + half;
+            double2 w = tw[k * st];
+            double2 u = x[i0], v = dmul(x[i1], w);
+            x[i0] = make_double2(u.x + v.x, u.y + v.y);
+            x[i1] = make_double2(u.x - v.x, u.y - v.y);
+        }
+        __syncthreads();
+    }
+}
+
+// One CTA per template.  mode 0: bank template (placed, FFT'd, FP32 into
+// out + t*L).  mode 1: raw response of numkern points into out.
+// Dynamic shared memory: (L + nfft_max) double2.
+struct TmplArgs {
+    int mode, zmax, wmax, nz, L, t_base;
+    double roffset, z1, w1;           // mode 1 parameters
+    int numbetween, numkern1;
+    const double2 *tw;                // exp(-2 pi i m / NMAX), m < NMAX/2
+    int nmax;
+    float2 *out;
+};
+
+__global__ void __launch_bounds__(256) k_templates(TmplArgs a)
+{
+    extern __shared__ double2 dsm[];
+    int t = a.t_base + blockIdx.x;
+    double z, w;
+    int numbetween, numkern;
+    if (a.mode == 0) {
+        int wi = t / a.nz, zi = t - wi * a.nz;
+        z = -a.zmax + zi * AB_DZ;
+        w = -a.wmax + wi * AB_DW;
+        numbetween = AB_NUMBETWEEN;
+        numkern = 2 * AB_NUMBETWEEN * ab_resp_halfwidth(z, w);
+    } else {
+        z = a.z1;
+        w = a.w1;
+        numbetween = a.numbetween;
+        numkern = a.numkern1;
+    }
+    const double roffset = (a.mode == 0) ? 0.0 : a.roffset;
+    if (a.mode == 0 && numkern > a.L) return;       // host validates; keeps stores in range
+    const int L = a.L, half = numkern / 2;
+    double2 *placed = dsm;              // [L]   (mode 0)
+    double2 *chirp = dsm + L;           // [nfft]
+    if (a.mode == 0)
+        for (int i = threadIdx.x; i < L; i += blockDim.x) placed[i] = make_double2(0.0, 0.0);
+    if (fabs(w) < 1E-4) {
+        for (int c = threadIdx.x; c < numkern; c += blockDim.x) {
+            double2 v = z_resp_point(roffset, numbetween, z, numkern, c);
+            if (a.mode == 0) placed[c >= half ? c - half : L - half + c] = v;
+            else a.out[c] = make_float2((float) v.x, (float) v.y);
+        }
+        __syncthreads();
+    } else {
+        // gen_w_response (src/responses.c:333-418): chirp of npts samples,
+        // zero padded to npts*numbetween, Fourier transformed.
+        int npts = 1;
+        int need = 6 * ab_resp_halfwidth(z, w) + 200 + numkern / numbetween;
+        while (npts < need) npts <<= 1;
+        int nfft = npts * numbetween;
+        double dt = 1.0 / (double) npts, amp = 2.0 * dt;
+        int fbar = npts / 4;
+        double f = ((double) fbar + roffset) - 0.5 * z + w / 12.0;
+        double fd = (z - 0.5 * w) / 2.0, fdd = w / 6.0;
+        for (int i = threadIdx.x; i < nfft; i += blockDim.x) {
+            double v = 0.0;
+            if (i < npts) {
+                double tt = i * dt;
+                v = amp * cospi(2.0 * (tt * (tt * (tt * fdd + fd) + f)));
+            }
+            chirp[i] = make_double2(v, 0.0);
+        }
+        __syncthreads();
+        fft64_tab(chirp, nfft, a.tw, a.nmax);
+        int first = fbar * numbetween - numkern / 2;
+        for (int c = threadIdx.x; c < numkern; c += blockDim.x) {
+            double2 v = chirp[first + c];
+            if (a.mode == 0) placed[c >= half ? c - half : L - half + c] = v;
+            else a.out[c] = make_float2((float) v.x, (float) v.y);
+        }
+        __syncthreads();
+    }
+    if (a.mode == 0) {
+        fft64_tab(placed, L, a.tw, a.nmax);
+        float2 *o = a.out + (size_t) t * L;
+        for (int i = threadIdx.x; i < L; i += blockDim.x)
+            o[i] = make_float2((float) placed[i].x, (float) placed[i].y);
+    }
+}
+
+static int chirp_len(double z, double w, int numkern, int numbetween)
+{
+    if (fabs(w) < 1E-4) return 0;
+    int need = 6 * ab_resp_halfwidth(z, w) + 200 + numkern / numbetween, n = 1;
+    while (n < need) n <<= 1;
+    return n * numbetween;
+}
+
+cudaError_t launch_templates(const ab_bank *b, float2 *bank_out, const double2 *tw_place,
+                             const double2 *tw_all, int max_log2, double2 *scratch,
+                             size_t scratch_elems, cudaStream_t st)
+{
+    (void) tw_place;
+    (void) scratch;
+    (void) scratch_elems;
+    int nfft_max = 0;
+    for (int wi = 0; wi < b->nw; wi++) {
+        double w = -b->wmax + wi * AB_DW;
+        for (int zi = 0; zi < b->nz; zi++) {
+            double z = -b->zmax + zi * AB_DZ;
+            int nk = 2 * AB_NUMBETWEEN * ab_resp_halfwidth(z, w);
+            int n = chirp_len(z, w, nk, AB_NUMBETWEEN);
+            if (n > nfft_max) nfft_max = n;
+        }
+    }
+    int nmax = 1 << max_log2;
+    if (nfft_max > nmax || b->L > nmax) return cudaErrorInvalidValue;
+    size_t smem = (size_t) (b->L + nfft_max) * sizeof(double2);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_templates, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    TmplArgs a{};
+    a.mode = 0;
+    a.zmax = b->zmax;
+    a.wmax = b->wmax;
+    a.nz = b->nz;
+    a.L = b->L;
+    a.tw = tw_all;
+    a.nmax = nmax;
+    a.out = bank_out;
+    const int chunk = 65535;
+    for (int t0 = 0; t0 < b->ntmpl; t0 += chunk) {
+        a.t_base = t0;
+        int n = b->ntmpl - t0 < chunk ? b->ntmpl - t0 : chunk;
+        k_templates<<<n, 256, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_response(double roffset, int numbetween, double z, double w, int numkern,
+                            float2 *out, const double2 *tw_all, int max_log2, double2 *scratch,
+                            cudaStream_t st)
+{
+    (void) scratch;
+    int nfft = chirp_len(z, w, numkern, numbetween);
+    int nmax = 1 << max_log2;
+    if (nfft > nmax) return cudaErrorInvalidValue;
+    size_t smem = (size_t) nfft * sizeof(double2);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_templates, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    TmplArgs a{};
+    a.mode = 1;
+    a.L = 0;
+    a.roffset = roffset;
+    a.z1 = z;
+    a.w1 = w;
+    a.numbetween = numbetween;
+    a.numkern1 = numkern;
+    a.tw = tw_all;
+    a.nmax = nmax;
+    a.out = out;
+    k_templates<<<1, 256, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ======================================================================
+// (b) spectrum preparation
+// ======================================================================
+__device__ __forceinline__ void block_geom(const SearchConsts &sc, const ab_bank &b, double startr,
+                                           ab_hgeom *g)
+{
+    *g = ab_harm_geom(startr, startr + sc.rstep - AB_DR, b.numharm, b.harmnum, sc.obs_zlo,
+                      sc.obs_wlo, sc.corr_uselen);
+}
+
+// Bitonic sort of n2 (power of two) floats in shared memory.
+__device__ void bitonic_sort(float *a, int n2)
+{
+    for (int k = 2; k <= n2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                int l = i ^ j;
+                if (l > i) {
+                    float x = a[i], y = a[l];
+                    bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        a[i] = y;
+                        a[l] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int LH>
+__global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+                                              const float2 *fft, float2 *xhat,
+                                              long long xhat_per_block)
+{
+    using SH = FftShape<LH>;
+    extern __shared__ float2 fsm[];
+    __shared__ double s_norm;
+    const int bank = blockIdx.x, bi = blockIdx.y;
+    const ab_bank b = banks[bank];
+    ab_hgeom g;
+    block_geom(sc, b, bb.startr[bi], &g);
+    const long long lobin = g.rlo - b.hw0;
+    const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
+
+    if (sc.nph > 0.0f) {
+        if (threadIdx.x == 0) s_norm = 1.0 / sqrt((double) sc.nph);
+    } else {
+        // block median of |X|^2 in float (POWER(), no FMA), src/accel_utils.c:1087-1099
+        float *pw = reinterpret_cast<float *>(fsm);
+        int n2 = 1;
+        while (n2 < numdata) n2 <<= 1;
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+            float p = INFINITY;
+            if (i < numdata) {
+                long long bin = lobin + i - sc.obs_lobin;
+                float2 v = (bin >= 0 && bin < sc.numbins) ? fft[bin] : make_float2(0.f, 0.f);
+                p = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+            }
+            pw[i] = p;
+        }
+        __syncthreads();
+        bitonic_sort(pw, n2);
+        if (threadIdx.x == 0) {
+            double m;
+            if (numdata & 1) m = pw[numdata / 2];
+            else m = 0.5 * ((double) pw[(numdata - 1) / 2] + (double) pw[numdata / 2]);
+            float med = (float) m;
+            s_norm = 1.0 / sqrt((double) med / 0.69314718055994530942);
+        }
+    }
+    __syncthreads();
+    const double norm = s_norm;
+    // spread data d[i] = norm * x[i] (i < numdata) at even samples; the
+    // L-point transform of the spread data is the L/2-point transform of d,
+    // repeated twice, so only that half is computed and stored.
+    const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
+    float2 *sm = fsm + grp * SH::SMEM;
+    FftTw<LH, -1> tw;
+    tw.init(t);
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        int i = t + SH::NT * m;
+        float2 x = make_float2(0.f, 0.f);
+        if (i < numdata) {
+            long long bin = lobin + i - sc.obs_lobin;
+            if (bin >= 0 && bin < sc.numbins) {
+                float2 a = fft[bin];
+                x = make_float2((float) ((double) a.x * norm), (float) ((double) a.y * norm));
+            }
+        }
+        v[m] = x;
+    }
+    __syncthreads();                    // pw aliases the FFT scratch
+    fft_run<LH, -1>(v, sm, t, tw);
+    if (grp == 0) {
+        float2 *o = xhat + (long long) bi * xhat_per_block + b.xhat_off;
+#pragma unroll
+        for (int m = 0; m < 16; m++) o[t + SH::NT * m] = v[m];
+    }
+}
+
+cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                        const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                        float2 *xhat, long long xhat_per_block, cudaStream_t st)
+{
+    // one launch per distinct L (banks of equal L are contiguous or not; launch per bank)
+    for (int k = 0; k < nbanks; k++) {
+        const ab_bank &b = banks_host[k];
+        int numdata = b.fftlen_ref / AB_NUMBETWEEN, n2 = 1;
+        while (n2 < numdata) n2 <<= 1;
+        int LH = b.L / 2;
+        size_t fftsm = (size_t) 256 * 16 * 17 / 16 * sizeof(float2);  // G * SMEM float2
+        size_t smem = fftsm > (size_t) n2 * sizeof(float) ? fftsm : (size_t) n2 * sizeof(float);
+        dim3 grid(1, bb.nblk);
+        // launch a 1-bank grid by offsetting the bank pointer
+        const ab_bank *bp = banks_dev + k;
+        switch (LH) {
+#define AB_PREP_CASE(N)                                                                       \
+    case N:                                                                                   \
+        cudaFuncSetAttribute(k_prep<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+        k_prep<N><<<grid, 256, smem, st>>>(bp, sc, bb, fft, xhat, xhat_per_block);           \
+        break;
+            AB_PREP_CASE(256)
+            AB_PREP_CASE(512)
+            AB_PREP_CASE(1024)
+            AB_PREP_CASE(2048)
+#undef AB_PREP_CASE
+            default:
+                return cudaErrorInvalidValue;
+        }
+    }
+    return cudaGetLastError();
+}
+
+// ======================================================================
+// (b) correlation
+// ======================================================================
+template <int L>
+__global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+                                              const CorrItem *items, const float2 *xhat,
+                                              long long xhat_per_block, const float2 *tmpl,
+                                              float *planes, long long plane_per_block,
+                                              float *fullplane)
+{
+    using SH = FftShape<L>;
+    extern __shared__ float2 fsm[];
+    float2 *xs = fsm;                                   // [L/2]
+    const CorrItem it = items[blockIdx.x];
+    const ab_bank b = banks[it.bank];
+    const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
+    float2 *sm = fsm + L / 2 + grp * SH::SMEM;
+    const float2 *xsrc = xhat + (long long) it.bi * xhat_per_block + b.xhat_off;
+    for (int i = threadIdx.x; i < L / 2; i += blockDim.x) xs[i] = xsrc[i];
+    ab_hgeom g;
+    block_geom(sc, b, bb.startr[it.bi], &g);
+    const int offset = 2 * b.hw0;
+    const int numrs = g.numrs;
+    const float invL2 = 1.0f / ((float) L * (float) L);
+    FftTw<L, 1> tw;
+    tw.init(t);
+    __syncthreads();
+    const int iters = (it.nt + SH::G - 1) / SH::G;
+    for (int k = 0; k < iters; k++) {
+        const int tl = it.t0 + k * SH::G + grp;
+        const bool valid = tl < it.t0 + it.nt;
+        float2 v[16];
+        if (valid) {
+            const float2 *kp = tmpl + b.tmpl_off + (long long) tl * L;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                int i = t + SH::NT * m;
+                v[m] = cmulc(xs[i & (L / 2 - 1)], __ldg(kp + i));
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; m++) v[m] = make_float2(0.f, 0.f);
+        }
+        fft_run<L, 1>(v, sm, t, tw);
+        if (valid) {
+            float *out;
+            long long lim = numrs;
+            if (sc.inmem) {
+                // full f-fdot plane row tl (numws = 1), column 2 rlo + kk
+                // (fund_to_ffdotplane, src/accel_utils.c:1219-1233)
+                out = fullplane + (long long) tl * sc.rlen + g.rlo * AB_RDR;
+                if (bb.is_pre) {
+                    long long room = sc.clip_col - g.rlo * AB_RDR;
+                    if (room < lim) lim = room;
+                }
+            } else {
+                out = planes + (long long) it.bi * plane_per_block + b.plane_off +
+                      (long long) tl * b.numrs_max;
+                if (lim > b.numrs_max) lim = b.numrs_max;
+            }
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                int kk = t + SH::NT * m - offset;
+                if (kk >= 0 && kk < lim) out[kk] = fmaf(v[m].x, v[m].x, v[m].y * v[m].y) * invL2;
+            }
+        }
+    }
+}
+
+cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
+                        const BlockBatch &bb, const CorrItem *items, int nitems,
+                        const float2 *xhat, long long xhat_per_block, const float2 *tmpl,
+                        float *planes, long long plane_per_block, float *fullplane,
+                        cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    size_t smem = (size_t) (L / 2 + 256 * 17) * sizeof(float2);
+    switch (L) {
+#define AB_CORR_CASE(N)                                                                       \
+    case N:                                                                                   \
+        cudaFuncSetAttribute(k_corr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+        k_corr<N><<<nitems, 256, smem, st>>>(banks_dev, sc, bb, items, xhat, xhat_per_block,  \
+                                             tmpl, planes, plane_per_block, fullplane);       \
+        break;
+        AB_CORR_CASE(512)
+        AB_CORR_CASE(1024)
+        AB_CORR_CASE(2048)
+        AB_CORR_CASE(4096)
+#undef AB_CORR_CASE
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ======================================================================
+// (c)+(d) harmonic sums fused with the threshold search
+// ======================================================================
+__device__ __forceinline__ void emit_hit(bool hit, unsigned long long key, float pw, HitBuf hb)
+{
+    unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (!mask) return;
+    int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(hb.count, (unsigned) __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+        unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
+        if (idx < hb.cap) {
+            hb.keys[idx] = key;
+            hb.pows[idx] = pw;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long make_key(long long block, int stage, int wi, int zi,
+                                                       int ri)
+{
+    return ((unsigned long long) block << (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS + AB_KEY_SBITS)) |
+           ((unsigned long long) stage << (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS)) |
+           ((unsigned long long) wi << (AB_KEY_RBITS + AB_KEY_ZBITS)) |
+           ((unsigned long long) zi << AB_KEY_RBITS) | (unsigned long long) ri;
+}
+
+constexpr int HS_ZT = 16;      // z rows per CTA
+constexpr int HS_RC = 1024;    // r cells per CTA
+
+// Standard mode: CTA = (block, fundamental w row, z tile, r chunk).
+__global__ void __launch_bounds__(256) k_harmsum_std(const ab_bank *banks, SearchConsts sc,
+                                                     BlockBatch bb, const float *planes,
+                                                     long long plane_per_block, HitBuf hb,
+                                                     float *dbg, int dbg_bi)
+{
+    extern __shared__ unsigned short rsm[];             // [nsub][HS_RC]
+    __shared__ int s_zind[AB_MAX_BANKS][HS_ZT];
+    __shared__ int s_wind[AB_MAX_BANKS];
+    __shared__ long long s_base[AB_MAX_BANKS];
+    const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
+    int x = blockIdx.x;
+    const int zt = x % nzt;
+    x /= nzt;
+    const int wi = x % sc.numws;
+    const int bi = x / sc.numws;
+    const int r0 = blockIdx.y * HS_RC;
+    const int z0 = zt * HS_ZT;
+    const double startr = bb.startr[bi];
+    const double lastr = startr + sc.rstep - AB_DR;
+    const ab_bank b0 = banks[0];
+    const ab_hgeom g0 = ab_harm_geom(startr, lastr, 1, 1, sc.obs_zlo, sc.obs_wlo, sc.corr_uselen);
+    const int nsub = sc.nbanks - 1;
+    const float *pb = planes + (long long) bi * plane_per_block;
+    for (int h = 0; h < nsub; h++) {
+        const ab_bank bh = banks[h + 1];
+        const ab_hgeom gh = ab_harm_geom(startr, lastr, bh.numharm, bh.harmnum, sc.obs_zlo,
+                                         sc.obs_wlo, sc.corr_uselen);
+        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
+            int r = r0 + c;
+            int ri = (r < g0.numrs) ? ab_rind(startr, r, bh.f, gh.rlo) : 0;
+            rsm[h * HS_RC + c] = (unsigned short) min(max(ri, 0), bh.numrs_max - 1);
+        }
+        if (threadIdx.x < HS_ZT) {
+            int z = z0 + threadIdx.x;
+            int zi = (z < sc.numz) ? ab_zind(sc.obs_zlo, z, bh.f, gh.zlo) : 0;
+            s_zind[h][threadIdx.x] = min(max(zi, 0), bh.nz - 1);
+        }
+        if (threadIdx.x == 0) {
+            s_wind[h] = min(max(ab_wind(g0.wlo, wi, bh.f, gh.wlo), 0), bh.nw - 1);
+            s_base[h] = bh.plane_off;
+        }
+    }
+    __syncthreads();
+    const long long block = bb.block0 + bi;
+    const int zend = min(z0 + HS_ZT, sc.numz);
+    for (int z = z0; z < zend; z++) {
+        const float *frow = pb + b0.plane_off + ((long long) wi * sc.numz + z) * b0.numrs_max;
+        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
+            const int r = r0 + c;
+            const bool ok = r < g0.numrs;
+            float sum = ok ? frow[r] : 0.f;
+            emit_hit(ok && !(sum <= sc.powcut[0]), make_key(block, 0, wi, z, r), sum, hb);
+            if (dbg && bi == dbg_bi && ok) dbg[(((long long) 0 * sc.numws + wi) * sc.numz + z) * g0.numrs + r] = sum;
+            int h = 0;
+            for (int s = 1; s < sc.stages; s++) {
+                const int nh = 1 << (s - 1);
+                for (int j = 0; j < nh; j++, h++) {
+                    const ab_bank &bh = banks[h + 1];
+                    if (ok) {
+                        const float *srow = pb + s_base[h] +
+                                            ((long long) s_wind[h] * bh.nz + s_zind[h][z - z0]) * bh.numrs_max;
+                        sum += srow[rsm[h * HS_RC + c]];
+                    }
+                }
+                emit_hit(ok && !(sum <= sc.powcut[s]), make_key(block, s, wi, z, r), sum, hb);
+                if (dbg && bi == dbg_bi && ok)
+                    dbg[(((long long) s * sc.numws + wi) * sc.numz + z) * g0.numrs + r] = sum;
+            }
+        }
+    }
+}
+
+cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
+                               const BlockBatch &bb, const float *planes,
+                               long long plane_per_block, HitBuf hb, float *dbg, int dbg_bi,
+                               cudaStream_t st)
+{
+    int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
+    dim3 grid((unsigned) (bb.nblk * sc.numws * nzt), (sc.corr_uselen + HS_RC - 1) / HS_RC);
+    size_t smem = (size_t) (sc.nbanks > 1 ? sc.nbanks - 1 : 1) * HS_RC * sizeof(unsigned short);
+    cudaFuncSetAttribute(k_harmsum_std, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    k_harmsum_std<<<grid, 256, smem, st>>>(banks_dev, sc, bb, planes, plane_per_block, hb, dbg, dbg_bi);
+    return cudaGetLastError();
+}
+
+// In-memory mode: the fundamental block and its subharmonics are read from
+// the full f-fdot plane.  CTA = (block, z tile, r chunk).
+__global__ void __launch_bounds__(256) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
+                                                       const float *plane, HitBuf hb, float *dbg,
+                                                       int dbg_bi)
+{
+    extern __shared__ int ism[];                        // [nsub][HS_RC]
+    __shared__ int s_zind[32][HS_ZT];
+    const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
+    const int zt = blockIdx.x % nzt, bi = blockIdx.x / nzt;
+    const int r0 = blockIdx.y * HS_RC, z0 = zt * HS_ZT;
+    const double startr = bb.startr[bi];
+    const ab_hgeom g0 = ab_harm_geom(startr, startr + sc.rstep - AB_DR, 1, 1, sc.obs_zlo,
+                                     sc.obs_wlo, sc.corr_uselen);
+    const int rlo = (int) g0.rlo;
+    int h = 0;
+    for (int s = 1; s < sc.stages; s++)
+        for (int hn = 1; hn < (1 << s); hn += 2, h++) {
+            const double f = (double) hn / (double) (1 << s);
+            for (int c = threadIdx.x; c < HS_RC; c += blockDim.x)
+                ism[h * HS_RC + c] = (r0 + c < g0.numrs)
+                    ? (int) min(max((long long) ab_inmem_rind(rlo, r0 + c, f), 0ll), sc.rlen - 1) : 0;
+            if (threadIdx.x < HS_ZT) {
+                int z = z0 + threadIdx.x;
+                s_zind[h][threadIdx.x] = (z < sc.numz) ? min(max(ab_inmem_zind(g0.zlo, z, f), 0), sc.numz - 1) : 0;
+            }
+        }
+    __syncthreads();
+    const long long block = bb.block0 + bi;
+    const int zend = min(z0 + HS_ZT, sc.numz);
+    for (int z = z0; z < zend; z++) {
+        const float *frow = plane + (long long) z * sc.rlen + (long long) rlo * AB_RDR;
+        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
+            const int r = r0 + c;
+            const bool ok = r < g0.numrs;
+            float sum = ok ? frow[r] : 0.f;
+            emit_hit(ok && !(sum <= sc.powcut[0]), make_key(block, 0, 0, z, r), sum, hb);
+            if (dbg && bi == dbg_bi && ok) dbg[((long long) 0 * sc.numz + z) * g0.numrs + r] = sum;
+            int hh = 0;
+            for (int s = 1; s < sc.stages; s++) {
+                const int nh = 1 << (s - 1);
+                for (int j = 0; j < nh; j++, hh++)
+                    if (ok) sum += plane[(long long) s_zind[hh][z - z0] * sc.rlen + ism[hh * HS_RC + c]];
+                emit_hit(ok && !(sum <= sc.powcut[s]), make_key(block, s, 0, z, r), sum, hb);
+                if (dbg && bi == dbg_bi && ok) dbg[((long long) s * sc.numz + z) * g0.numrs + r] = sum;
+            }
+        }
+    }
+}
+
+cudaError_t launch_harmsum_inmem(const SearchConsts &sc, const BlockBatch &bb,
+                                 const float *fullplane, HitBuf hb, float *dbg, int dbg_bi,
+                                 cudaStream_t st)
+{
+    int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
+    int nsub = (1 << (sc.stages - 1)) - 1;
+    dim3 grid((unsigned) (bb.nblk * nzt), (sc.corr_uselen + HS_RC - 1) / HS_RC);
+    size_t smem = (size_t) (nsub > 0 ? nsub : 1) * HS_RC * sizeof(int);
+    cudaFuncSetAttribute(k_harmsum_inmem, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    k_harmsum_inmem<<<grid, 256, smem, st>>>(sc, bb, fullplane, hb, dbg, dbg_bi);
+    return cudaGetLastError();
+}
+
+// ======================================================================
+// per-function drop-in helpers
+// ======================================================================
+__global__ void k_add_ffdot(float *fund, const float *sub, int numws, int numzs, int numrs,
+                            int sub_numzs, int sub_numrs, double f, int fund_wlo, int sub_wlo,
+                            double fullrlo, long long sub_rlo, double obs_zlo, int sub_zlo)
+{
+    long long n = (long long) numws * numzs * numrs;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        int kk = (int) (i % numrs);
+        long long rest = i / numrs;
+        int jj = (int) (rest % numzs), ii = (int) (rest / numzs);
+        int wind = ab_wind(fund_wlo, ii, f, sub_wlo);
+        int zind = ab_zind(obs_zlo, jj, f, sub_zlo);
+        int rind = ab_rind(fullrlo, kk, f, sub_rlo);
+        fund[i] += sub[((long long) wind * sub_numzs + zind) * sub_numrs + rind];
+    }
+}
+
+cudaError_t launch_add_ffdot(float *fund, const float *sub, int numws, int numzs, int numrs,
+                             int sub_numzs, int sub_numrs, double f, int fund_wlo, int sub_wlo,
+                             double fullrlo, long long sub_rlo, double obs_zlo, int sub_zlo,
+                             cudaStream_t st)
+{
+    k_add_ffdot<<<296, 256, 0, st>>>(fund, sub, numws, numzs, numrs, sub_numzs, sub_numrs, f,
+                                      fund_wlo, sub_wlo, fullrlo, sub_rlo, obs_zlo, sub_zlo);
+    return cudaGetLastError();
+}
+
+__global__ void k_inmem_add(float *fund, const float *plane, long long rlen, int numzs, int numrs,
+                            int fund_rlo, int fund_zlo, double f)
+{
+    long long n = (long long) numzs * numrs;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x) {
+        int jj = (int) (i % numrs), ii = (int) (i / numrs);
+        int zind = ab_inmem_zind(fund_zlo, ii, f);
+        int rind = ab_inmem_rind(fund_rlo, jj, f);
+        fund[i] += plane[(long long) zind * rlen + rind];
+    }
+}
+
+cudaError_t launch_inmem_add(float *fund, const float *plane, long long rlen, int numzs,
+                             int numrs, int fund_rlo, int fund_zlo, double f, cudaStream_t st)
+{
+    k_inmem_add<<<296, 256, 0, st>>>(fund, plane, rlen, numzs, numrs, fund_rlo, fund_zlo, f);
+    return cudaGetLastError();
+}
+
+__global__ void k_threshold(const float *pw, int numws, int numzs, int numrs, float powcut,
+                            int stage, HitBuf hb)
+{
+    long long n = (long long) numws * numzs * numrs;
+    long long nloop = (n + 31) / 32 * 32;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < nloop;
+         i += (long long) gridDim.x * blockDim.x) {
+        bool ok = i < n;
+        float p = ok ? pw[i] : 0.f;
+        int kk = ok ? (int) (i % numrs) : 0;
+        long long rest = ok ? i / numrs : 0;
+        int jj = (int) (rest % numzs), ii = (int) (rest / numzs);
+        emit_hit(ok && !(p <= powcut), make_key(0, stage, ii, jj, kk), p, hb);
+    }
+}
+
+cudaError_t launch_threshold(const float *pw, int numws, int numzs, int numrs, float powcut,
+                             int stage, HitBuf hb, cudaStream_t st)
+{
+    k_threshold<<<296, 256, 0, st>>>(pw, numws, numzs, numrs, powcut, stage, hb);
+    return cudaGetLastError();
+}
+
+}  // namespace ab

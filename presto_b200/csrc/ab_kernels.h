@@ -1,0 +1,79 @@
+// ab_kernels.h -- device-side structures and launch wrappers shared by the
+// kernel file and the engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ab_host.h"
+
+namespace ab {
+
+// Read-only per-search constants passed by value to every kernel.
+struct SearchConsts {
+    double obs_zlo, obs_wlo, obs_rlo;
+    long long obs_lobin, numbins;
+    long long rlen;            // in-memory plane row length (floats)
+    long long clip_col;        // pre-pass blocks write only columns < clip_col
+    int corr_uselen, rstep, numz, numws, stages, inmem, nbanks;
+    float nph;
+    float powcut[AB_MAX_STAGES];
+};
+
+// Blocks of one launch: global ordinal block0 + i, start frequency startr[i].
+struct BlockBatch {
+    const double *startr;      // device array [nblk]
+    long long block0;          // key ordinal of item 0
+    int nblk;
+    int is_pre;                // pre-pass blocks (in-memory mode only)
+};
+
+struct CorrItem {              // one CTA of the correlation kernel
+    int bi, bank, t0, nt;
+};
+
+struct HitBuf {
+    unsigned long long *keys;
+    float *pows;
+    unsigned int *count;
+    unsigned int cap;
+};
+
+// kernel set (a): templates
+void launch_twiddle64(double2 *tw, int n, int sign, cudaStream_t st);
+cudaError_t launch_templates(const ab_bank *bank, float2 *bank_out, const double2 *tw_place,
+                             const double2 *tw_chirp_all, int chirp_max_log2,
+                             double2 *scratch, size_t scratch_elems, cudaStream_t st);
+cudaError_t launch_response(double roffset, int numbetween, double z, double w, int numkern,
+                            float2 *out, const double2 *tw_chirp_all, int chirp_max_log2,
+                            double2 *scratch, cudaStream_t st);
+
+// kernel set (b): spectrum preparation and correlation
+cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                        const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                        float2 *xhat, long long xhat_per_block, cudaStream_t st);
+cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
+                        const BlockBatch &bb, const CorrItem *items, int nitems,
+                        const float2 *xhat, long long xhat_per_block, const float2 *tmpl,
+                        float *planes, long long plane_per_block, float *fullplane,
+                        cudaStream_t st);
+
+// kernel sets (c)+(d): harmonic summing fused with the threshold search
+cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
+                               const BlockBatch &bb, const float *planes,
+                               long long plane_per_block, HitBuf hb, float *dbg,
+                               int dbg_bi, cudaStream_t st);
+cudaError_t launch_harmsum_inmem(const SearchConsts &sc, const BlockBatch &bb,
+                                 const float *fullplane, HitBuf hb, float *dbg, int dbg_bi,
+                                 cudaStream_t st);
+
+// per-function drop-in helpers
+cudaError_t launch_add_ffdot(float *fund, const float *sub, int numws, int numzs, int numrs,
+                             int sub_numzs, int sub_numrs, double f, int fund_wlo, int sub_wlo,
+                             double fullrlo, long long sub_rlo, double obs_zlo, int sub_zlo,
+                             cudaStream_t st);
+cudaError_t launch_inmem_add(float *fund, const float *plane, long long rlen, int numzs,
+                             int numrs, int fund_rlo, int fund_zlo, double f, cudaStream_t st);
+cudaError_t launch_threshold(const float *pw, int numws, int numzs, int numrs, float powcut,
+                             int stage, HitBuf hb, cudaStream_t st);
+
+}  // namespace ab
