@@ -1,0 +1,349 @@
+"""Throughput bench of the B200 accelsearch engine.
+
+One step = one complete accelsearch of one synthetic spectrum (every block
+and harmonic stage, candidates collected) through the engine.  The default
+workload is the larger acceleration search: N = 2^23 samples at 64 us,
+zmax = 600, numharm = 16, sigma = 2, with 3 injected 8-harmonic pulsars
+(seeded synthetic data of that shape).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       : value = f-fdot cells/s with the spectrum resident in HBM
+             (device-timed with CUDA events on the engine's stream, L2
+             flushed between steps); e2e = the same metric through the
+             public C ABI with the spectrum in pinned host memory
+             (host->device copy and the candidate read-back inside the
+             timed region).  Under torchrun every rank searches its own
+             spectra (independent DM trials: replicas, weak scaling).
+reference  : the CPU restatement of the reference's accelsearch (FP32
+             arithmetic like its FFTW path, all host threads) timed on a
+             bounded sample of blocks of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "cfg2": dict(N=1 << 23, dt=64e-6, zmax=600, wmax=None, numharm=16, sigma=2.0,
+                 desc="accelsearch N=2^23 dt=64us zmax=600 numharm=16 sigma=2; "
+                      "3 injected 8-harmonic pulsars (A=0.02/harmonic), N(0,1) noise"),
+    "cfg2s": dict(N=1 << 20, dt=64e-6, zmax=600, wmax=None, numharm=16, sigma=2.0,
+                  desc="profiling case: cfg2 search parameters on N=2^20"),
+    "cfg1": dict(N=1 << 20, dt=64e-6, zmax=200, wmax=None, numharm=8, sigma=2.0,
+                 desc="accelsearch N=2^20 dt=64us zmax=200 numharm=8 sigma=2 (in-memory); "
+                      "one sinusoid f=123.4 Hz z=40 A=0.05"),
+    "cfg3": dict(N=1 << 22, dt=64e-6, zmax=200, wmax=300, numharm=8, sigma=2.0,
+                 desc="jerk search N=2^22 dt=64us zmax=200 wmax=300 numharm=8 sigma=2; "
+                      "2 injected 4-harmonic sinusoids"),
+}
+METRIC = "f-fdot cells/s"
+UNIT = "cells/s"
+
+
+def make_spectrum(name, seed_offset=0):
+    from presto_b200 import synth
+    w = WORKLOADS[name]
+    if name in ("cfg2", "cfg2s"):
+        return synth.cfg2_spectrum(N=w["N"], dt=w["dt"], seed=2000 + seed_offset)[0]
+    if name == "cfg3":
+        return synth.cfg3_spectrum(N=w["N"], dt=w["dt"], seed=3000 + seed_offset)[0]
+    return synth.cfg1_spectrum(N=w["N"], dt=w["dt"], seed=1000 + seed_offset)
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.proc = device, None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "out", "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def cpu_sample(name, threads, budget_s=20.0, first_block=200):
+    """Times the oracle port (FP32) on a bounded block sample of the workload;
+    returns (searches/s, cells/s, description)."""
+    import presto_b200 as pb
+    from oracle import pyoracle as po
+    w = WORKLOADS[name]
+    fft = make_spectrum(name)
+    p = po.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
+                       numharm=w["numharm"], sigma=w["sigma"])
+    obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
+                                     numharm=w["numharm"], sigma=w["sigma"]))
+    counts = pb.algorithmic_counts(obs)
+    t0 = time.perf_counter()
+    po.accelsearch(p, fft, nthreads=threads, first_block=first_block, max_blocks=0, prec=32)
+    t_setup = time.perf_counter() - t0
+    nb = 2
+    t0 = time.perf_counter()
+    _, _, done = po.accelsearch(p, fft, nthreads=threads, first_block=first_block, max_blocks=nb,
+                                prec=32)
+    t_two = time.perf_counter() - t0 - t_setup
+    per_block = max(t_two / max(done, 1), 1e-6)
+    more = int(max(0, (budget_s - 2 * t_setup - t_two) / per_block))
+    more = min(more, 64)
+    if more > 0 and not obs.inmem:
+        t0 = time.perf_counter()
+        _, _, done2 = po.accelsearch(p, fft, nthreads=threads, first_block=first_block,
+                                     max_blocks=more, prec=32)
+        per_block = (time.perf_counter() - t0 - t_setup) / max(done2, 1)
+        nb = done2
+    t_search = t_setup + per_block * counts["blocks"]
+    desc = (f"oracle port FP32 (scalar mixed-radix FFT, not FFTW), {threads} threads: template "
+            f"banks {t_setup:.2f} s + {nb} blocks timed at {per_block * 1e3:.1f} ms/block, "
+            f"scaled to {counts['blocks']} blocks")
+    return 1.0 / t_search, counts["cells"] / t_search, desc
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    name = args.workload
+    vals = []
+    desc = ""
+    for _ in range(args.warmup + args.steps):
+        sps, cps, desc = cpu_sample(name, threads, budget_s=args.cpu_budget / max(args.steps, 1))
+        vals.append(cps)
+    v = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": name, "desc": WORKLOADS[name]["desc"]},
+            "searches_per_s": v / max(1.0, 1.0) / _cells_per_search(name),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _cells_per_search(name):
+    import presto_b200 as pb
+    w = WORKLOADS[name]
+    obs = pb.obs_init(pb.make_params(w["N"], w["dt"], w["N"] // 2, zmax=w["zmax"], wmax=w["wmax"],
+                                     numharm=w["numharm"], sigma=w["sigma"]))
+    return pb.algorithmic_counts(obs)["cells"]
+
+
+def run_ours(args):
+    import torch
+    import presto_b200 as pb
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    name = args.workload
+    w = WORKLOADS[name]
+    fft = make_spectrum(name, seed_offset=rank)
+    ctx = pb.Context(local)
+    if args.scratch_mb:
+        ctx.L.ab_ctx_set_hbm_budget(ctx.ptr, int(args.scratch_mb) * 4 << 20)
+    obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
+                                     numharm=w["numharm"], sigma=w["sigma"]))
+    counts = pb.algorithmic_counts(obs)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    dev_fft = torch.from_numpy(fft.view(np.float32).copy()).to(f"cuda:{local}")
+    torch.cuda.synchronize()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")   # 256 MiB > L2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident value ----
+    for _ in range(args.warmup):
+        ctx.search(obs, None, device_ptr=dev_fft.data_ptr())
+    ctx.reset_kernel_times()
+    ctx.set_profiling(True)
+    launches0 = ctx.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    ncands = 0
+    barrier()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            ev[k][0].record(stream)
+            ncands = len(ctx.search(obs, None, device_ptr=dev_fft.data_ptr()))
+            ev[k][1].record(stream)
+        barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    launches = ctx.launch_count() - launches0
+    kms, kn = ctx.kernel_times()
+    ctx.set_profiling(False)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    total_cells = counts["cells"] * args.steps * world
+    value = total_cells / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    host = torch.from_numpy(fft.view(np.float32).copy()).pin_memory()
+    host_np = host.numpy().view(np.complex64)
+    ctx.search(obs, host_np)
+    barrier()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.search(obs, host_np)
+    e1.record(stream)
+    barrier()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    nhits = len(ctx.last_hits()[0])
+
+    # ---- roofline of the dominant kernel (correlation) ----
+    corr_ms_per_search = kms[2] / args.steps
+    achieved = counts["corr_flops"] / (corr_ms_per_search / 1e3) / 1e12
+    fp32_peak = measured_fp32_peak(ctx)
+    harm_ms = kms[3] / args.steps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": name, "desc": w["desc"], "N": w["N"], "zmax": w["zmax"],
+                       "wmax": w["wmax"], "numharm": w["numharm"], "blocks": counts["blocks"],
+                       "cells_per_search": counts["cells"],
+                       "l2": "256 MiB buffer written between timed steps",
+                       "parallelism": f"replicas x{world} (independent spectra per GPU)"},
+            "searches_per_s": value / counts["cells"],
+            "candidates_per_search": ncands,
+            "gpu_launches": int(launches),
+            "e2e": {"value": counts["cells"] * args.steps * world / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(fft.nbytes),
+                    "d2h_bytes_per_step": int(4 + 12 * nhits),
+                    "searches_per_s": args.steps * world / (e2e_ms / 1e3)},
+            "roofline": {"bound": "fp32", "kernel": "k_corr (template correlation)",
+                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": None,
+                         "flops_per_search": counts["corr_flops"],
+                         "kernel_ms_per_search": corr_ms_per_search,
+                         "peak_source": "measured in-run FP32 FMA loop (MEASURED_PEAKS.json "
+                                        "holds no FP32 CUDA-core figure)"},
+            "roofline_harmsum": {"bound": "hbm", "kernel": "k_harmsum (sum + search)",
+                                 "achieved": counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9,
+                                 "peak": hbm, "unit": "GB/s",
+                                 "frac": counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9 / hbm,
+                                 "kernel_ms_per_search": harm_ms},
+            "kernel_ms_per_search": {"templates": kms[0] / args.steps, "prep": kms[1] / args.steps,
+                                     "corr": corr_ms_per_search, "harmsum": harm_ms},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            sps, cps, desc = cpu_sample(name, os.cpu_count() or 1, budget_s=args.cpu_budget)
+            line["cpu_baseline"] = {"value": cps, "unit": UNIT, "cores": os.cpu_count() or 1,
+                                    "kind": "port", "sample": desc, "searches_per_s": sps}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def measured_fp32_peak(ctx):
+    import ctypes as C
+    import presto_b200 as pb
+    v = C.c_double()
+    rc = pb.lib().ab_measure_fp32_peak(ctx.ptr, C.byref(v))
+    return v.value if rc == 0 else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="cfg2")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scratch-mb", type=int, default=0,
+                    help="cap the engine's block scratch (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

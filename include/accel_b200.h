@@ -105,6 +105,14 @@ int  ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes);
 /* Geometry + thresholds (create_accelobs).  Host only. */
 int ab_obs_init(const ab_params *p, ab_obs *obs);
 
+/* Template-bank geometry of obs in the reference's harmonic order (host
+ * only).  info[8*k ..] = numharm, harmnum, numkern_zdim, numkern_wdim,
+ * reference fftlen, device FFT length, kernel half width, largest numrs. */
+int ab_bank_geometry(const ab_obs *obs, int *nbanks, int *info, int maxbanks);
+
+/* Number of blocks of the main search loop (src/accelsearch.c:187-224). */
+long long ab_num_blocks_main(const ab_obs *obs);
+
 /* Template banks for obs (create_subharminfos); cached on the context. */
 int ab_prepare(ab_ctx *ctx, const ab_obs *obs);
 
@@ -177,6 +185,11 @@ int ab_ctx_set_profiling(ab_ctx *ctx, int on);
 int ab_ctx_kernel_times(ab_ctx *ctx, double *ms, long long *launches, int nkinds);
 int ab_ctx_reset_kernel_times(ab_ctx *ctx);
 long long ab_ctx_launch_count(ab_ctx *ctx);
+
+/* Measured FP32 FMA throughput of this device (TFLOP/s), the denominator of
+ * the correlation kernel's roofline: 8 independent FMA chains per thread over
+ * 8 CTAs of 256 threads per SM, best of 5 timed runs. */
+int ab_measure_fp32_peak(ab_ctx *ctx, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -4,6 +4,6 @@ a drop-in for the hot path of PRESTO's accelsearch.
 The compute lives in libaccel_b200.so (CUDA for sm_100a + host C) behind the
 C ABI in include/accel_b200.h; this package is its Python host mirror.
 """
-from .accel import (AccelError, AccelSearch, CandList, Context, candidate_sigma,  # noqa: F401
-                    eliminate_harmonics, lib, make_params, num_blocks, obs_init,
-                    power_for_sigma, sort_cands)
+from .accel import (AccelError, AccelSearch, CandList, Context, algorithmic_counts,  # noqa: F401
+                    bank_geometry, candidate_sigma, eliminate_harmonics, lib, make_params,
+                    num_blocks, obs_init, power_for_sigma, sort_cands)

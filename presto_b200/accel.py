@@ -28,7 +28,7 @@ EXPORTS = [
     "ab_bank_kernel", "ab_candidate_sigma", "ab_power_for_sigma", "ab_chi2_logp",
     "ab_equivalent_gaussian_sigma", "ab_sort_cands", "ab_eliminate_harmonics",
     "ab_ctx_set_profiling", "ab_ctx_kernel_times", "ab_ctx_reset_kernel_times",
-    "ab_ctx_launch_count",
+    "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
 ]
 
 
@@ -124,6 +124,10 @@ def lib():
     L.ab_ctx_set_profiling.argtypes = [vp, i]
     L.ab_ctx_kernel_times.argtypes = [vp, C.POINTER(d), C.POINTER(ll), i]
     L.ab_ctx_reset_kernel_times.argtypes = [vp]
+    L.ab_bank_geometry.argtypes = [C.POINTER(Obs), C.POINTER(i), C.POINTER(i), i]
+    L.ab_num_blocks_main.restype = ll
+    L.ab_num_blocks_main.argtypes = [C.POINTER(Obs)]
+    L.ab_measure_fp32_peak.argtypes = [vp, C.POINTER(d)]
     L.ab_ctx_launch_count.restype = ll
     L.ab_ctx_launch_count.argtypes = [vp]
     _lib = L
@@ -165,11 +169,43 @@ def obs_init(params):
 
 
 def num_blocks(obs):
-    n, startr = 0, obs.rlo
-    while startr + obs.rstep < obs.highestbin:
-        n += 1
-        startr += obs.rstep
-    return n
+    """Blocks of the main search loop (src/accelsearch.c:187-224)."""
+    return int(lib().ab_num_blocks_main(C.byref(obs)))
+
+
+def bank_geometry(obs):
+    """Per template bank: dict(numharm, harmnum, nz, nw, fftlen_ref, L, hw, numrs_max)."""
+    n = C.c_int()
+    rc = lib().ab_bank_geometry(C.byref(obs), C.byref(n), None, 0)
+    if rc:
+        raise AccelError(f"ab_bank_geometry: {ERRORS.get(rc, rc)}")
+    info = (C.c_int * (8 * n.value))()
+    lib().ab_bank_geometry(C.byref(obs), C.byref(n), info, n.value)
+    keys = ("numharm", "harmnum", "nz", "nw", "fftlen_ref", "L", "hw", "numrs_max")
+    return [dict(zip(keys, info[8 * k:8 * k + 8])) for k in range(n.value)]
+
+
+def algorithmic_counts(obs):
+    """Work of one search: f-fdot cells (numrs x numz x max(numw,1) per block
+    per stage), correlation FLOPs at the reference FFT lengths
+    (numz_h numw_h (5 L log2 L + 8 L) + 5 L log2 L per block and harmonic),
+    and harmonic-sum/search bytes when unfused (4 B per cell per stage read,
+    4 B per subharmonic gather, 8 B read-modify-write per later stage)."""
+    import math
+    nb = num_blocks(obs)
+    nws = max(obs.numw, 1)
+    fund_cells = nb * obs.corr_uselen * obs.numz * nws
+    cells = fund_cells * obs.numharmstages
+    numharm = 1 << (obs.numharmstages - 1)
+    flops = 0.0
+    for b in bank_geometry(obs):
+        L = b["fftlen_ref"]
+        f = 5.0 * L * math.log2(L)
+        flops += b["nz"] * b["nw"] * (f + 8.0 * L) + f
+    flops *= nb
+    sum_bytes = 4.0 * fund_cells * obs.numharmstages + 4.0 * fund_cells * (numharm - 1) + \
+        8.0 * fund_cells * (obs.numharmstages - 1)
+    return dict(blocks=nb, cells=cells, corr_flops=flops, harmsum_bytes=sum_bytes)
 
 
 class Context:

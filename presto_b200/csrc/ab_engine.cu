@@ -77,6 +77,8 @@ struct ab_ctx {
     DevBuf<unsigned long long> keys;
     DevBuf<float> pows;
     DevBuf<unsigned int> count;
+    DevBuf<float> sigs;
+    std::vector<float> hsigs;
     unsigned int hit_cap = 1u << 23;
     std::vector<unsigned long long> hkeys;
     std::vector<float> hpows;
@@ -377,8 +379,17 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     return AB_OK;
 }
 
-static int fetch_hits(ab_ctx *ctx, long long *nhits)
+static int fetch_hits(ab_ctx *ctx, long long *nhits, const ab_obs *obs = nullptr)
 {
+    if (obs) {
+        SigmaConsts c{};
+        for (int i = 0; i < AB_MAX_STAGES; i++)
+            c.numindep[i] = i < obs->numharmstages ? (double) obs->numindep[i] : 1.0;
+        CK(ctx->sigs.ensure(ctx->hit_cap));
+        HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
+        CK(launch_sigma(hb, ctx->sigs.p, c, ctx->stream));
+        ctx->launches++;
+    }
     unsigned n = 0;
     CK(cudaMemcpyAsync(&n, ctx->count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -395,6 +406,11 @@ static int fetch_hits(ab_ctx *ctx, long long *nhits)
                            cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaMemcpyAsync(ctx->hpows.data(), ctx->pows.p, sizeof(float) * n, cudaMemcpyDeviceToHost,
                            ctx->stream));
+        if (obs) {
+            ctx->hsigs.resize(n);
+            CK(cudaMemcpyAsync(ctx->hsigs.data(), ctx->sigs.p, sizeof(float) * n,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        }
         CK(cudaStreamSynchronize(ctx->stream));
     }
     *nhits = n;
@@ -514,12 +530,13 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
     rc = search_core(ctx, obs, dfft, first_block, max_blocks, -1);
     if (rc) return rc;
     long long nh = 0;
-    rc = fetch_hits(ctx, &nh);
+    rc = fetch_hits(ctx, &nh, obs);
     harvest(ctx);
     if (rc) return rc;
     ab_list *l = ab_list_new();
     long long nmain = ab_num_blocks(obs);
-    rc = ab_replay_hits(obs, ctx->hkeys.data(), ctx->hpows.data(), nh, ctx->hstart.data(), nmain, l);
+    rc = ab_replay_hits(obs, ctx->hkeys.data(), ctx->hpows.data(), ctx->hsigs.data(), nh,
+                        ctx->hstart.data(), nmain, l);
     if (rc) {
         ab_list_free(l);
         return fail(ctx, rc, "hit replay failed");
@@ -842,5 +859,35 @@ int ab_ctx_reset_kernel_times(ab_ctx *ctx)
 }
 
 long long ab_ctx_launch_count(ab_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int ab_measure_fp32_peak(ab_ctx *ctx, double *tflops)
+{
+    if (!ctx || !tflops) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(ctx->tmpa.ensure(1));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int iters = 1 << 14;
+    double best = 0.0;
+    for (int k = 0; k < 7; k++) {
+        cudaEventRecord(e0, ctx->stream);
+        cudaError_t e = launch_fma_peak(ctx->tmpa.p, iters, sms, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "fma probe: %s", cudaGetErrorString(e));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        double fl = 2.0 * 8.0 * iters * 256.0 * 8.0 * sms;
+        if (k >= 2 && ms > 0) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = best;
+    return AB_OK;
+}
 
 }  // extern "C"

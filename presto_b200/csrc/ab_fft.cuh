@@ -134,46 +134,78 @@ template <int L> struct FftShape {
     static constexpr int G = 256 / NT;                // transforms per 256-thread CTA
     static constexpr int R3 = L / 256;                // radix of the third pass (1: none)
     static constexpr int NB3 = (R3 > 1) ? 16 / R3 : 0;
-    static constexpr int NTW = 15 + NB3 * (R3 > 1 ? R3 - 1 : 0);
     static constexpr int SMEM = L + L / 16;           // padded float2 per transform
     static_assert(L >= 256 && L <= 4096 && (L & (L - 1)) == 0, "FFT length");
 };
 
-// Per-thread twiddles of passes 2 and 3 (pass 1 has none).
+// Per-thread twiddles of passes 2 and 3 (pass 1 has none), stored as the
+// base powers w, w^2, w^4, w^8 of each butterfly's root w; the other powers
+// are formed with at most three complex products (a few ulp of error).
 template <int L, int S> struct FftTw {
-    float2 w[FftShape<L>::NTW];
+    using SH = FftShape<L>;
+    static constexpr int NBASE3 = SH::R3 >= 16 ? 4 : SH::R3 >= 8 ? 3 : SH::R3 >= 4 ? 2 : 1;
+    float2 b2[4];                                   // pass 2: w = exp(S 2 pi i k / 256)
+    float2 b3[SH::NB3 > 0 ? SH::NB3 : 1][NBASE3];   // pass 3: w = exp(S 2 pi i k / L)
     __device__ __forceinline__ void init(int t)
     {
-        using SH = FftShape<L>;
-        // pass 2: R = 16, LS = 16, one butterfly, k = t mod 16
-        {
-            int k = t & 15;
+        int k = t & 15;
 #pragma unroll
-            for (int q = 1; q < 16; q++) {
-                double s, c;
-                sincospi(2.0 * (double) (q * k) / 256.0, &s, &c);
-                w[q - 1] = make_float2((float) c, (float) (S * s));
-            }
+        for (int e = 0; e < 4; e++) {
+            double s, c;
+            sincospi(2.0 * (double) (k << e) / 256.0, &s, &c);
+            b2[e] = make_float2((float) c, (float) (S * s));
         }
         if constexpr (SH::R3 > 1) {
 #pragma unroll
             for (int b = 0; b < SH::NB3; b++) {
-                int k = (t + SH::NT * b) & 255;
+                int kk = (t + SH::NT * b) & 255;
 #pragma unroll
-                for (int q = 1; q < SH::R3; q++) {
+                for (int e = 0; e < NBASE3; e++) {
                     double s, c;
-                    sincospi(2.0 * (double) (q * k) / (double) L, &s, &c);
-                    w[15 + b * (SH::R3 - 1) + q - 1] = make_float2((float) c, (float) (S * s));
+                    sincospi(2.0 * (double) (kk << e) / (double) L, &s, &c);
+                    b3[b][e] = make_float2((float) c, (float) (S * s));
                 }
             }
         }
     }
 };
 
+// x[q] *= w^q for q = 1..R-1, w^q built from the base powers.
+template <int R>
+__device__ __forceinline__ void apply_tw(float2 *x, const float2 *bs)
+{
+    if constexpr (R >= 2) x[1] = cmul(x[1], bs[0]);
+    if constexpr (R >= 4) {
+        x[2] = cmul(x[2], bs[1]);
+        float2 p3 = cmul(bs[1], bs[0]);
+        x[3] = cmul(x[3], p3);
+        if constexpr (R >= 8) {
+            x[4] = cmul(x[4], bs[2]);
+            float2 p5 = cmul(bs[2], bs[0]), p6 = cmul(bs[2], bs[1]), p7 = cmul(p6, bs[0]);
+            x[5] = cmul(x[5], p5);
+            x[6] = cmul(x[6], p6);
+            x[7] = cmul(x[7], p7);
+            if constexpr (R >= 16) {
+                x[8] = cmul(x[8], bs[3]);
+                float2 p9 = cmul(bs[3], bs[0]), p10 = cmul(bs[3], bs[1]), p12 = cmul(bs[3], bs[2]);
+                x[9] = cmul(x[9], p9);
+                x[10] = cmul(x[10], p10);
+                x[11] = cmul(x[11], cmul(p10, bs[0]));
+                x[12] = cmul(x[12], p12);
+                x[13] = cmul(x[13], cmul(p12, bs[0]));
+                float2 p14 = cmul(p12, bs[1]);
+                x[14] = cmul(x[14], p14);
+                x[15] = cmul(x[15], cmul(p14, bs[0]));
+            }
+        }
+    }
+}
+
 // One Stockham pass.  v holds x[t + NT m]; results of a non-final pass go
 // through shared memory and come back in the same strided layout.
-template <int L, int R, int LS, int S, bool LAST, int TWOFF>
-__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const float2 *tw)
+// PASS: 1, 2 or 3 (selects the twiddle bases).
+template <int L, int R, int LS, int S, bool LAST, int PASS>
+__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const FftTw<L, S> &tw)
 {
     constexpr int NT = L / 16, NB = 16 / R;
 #pragma unroll
@@ -181,10 +213,8 @@ __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, con
         float2 x[R];
 #pragma unroll
         for (int q = 0; q < R; q++) x[q] = v[b + q * NB];
-        if constexpr (LS > 1) {
-#pragma unroll
-            for (int q = 1; q < R; q++) x[q] = cmul(x[q], tw[TWOFF + b * (R - 1) + q - 1]);
-        }
+        if constexpr (PASS == 2) apply_tw<R>(x, tw.b2);
+        if constexpr (PASS == 3) apply_tw<R>(x, tw.b3[b]);
         dft<R, S>(x);
         if constexpr (LAST) {
 #pragma unroll
@@ -212,12 +242,12 @@ __device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, cons
 {
     using SH = FftShape<L>;
     if constexpr (SH::R3 > 1) {
-        fft_pass<L, 16, 1, S, false, 0>(v, sm, t, tw.w);
-        fft_pass<L, 16, 16, S, false, 0>(v, sm, t, tw.w);
-        fft_pass<L, SH::R3, 256, S, true, 15>(v, sm, t, tw.w);
+        fft_pass<L, 16, 1, S, false, 1>(v, sm, t, tw);
+        fft_pass<L, 16, 16, S, false, 2>(v, sm, t, tw);
+        fft_pass<L, SH::R3, 256, S, true, 3>(v, sm, t, tw);
     } else {
-        fft_pass<L, 16, 1, S, false, 0>(v, sm, t, tw.w);
-        fft_pass<L, 16, 16, S, true, 0>(v, sm, t, tw.w);
+        fft_pass<L, 16, 1, S, false, 1>(v, sm, t, tw);
+        fft_pass<L, 16, 16, S, true, 2>(v, sm, t, tw);
     }
 }
 

@@ -391,16 +391,42 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
 /* ------------------------------------------------------------------ */
 /* candidate list: insert_new_accelcand (src/accel_utils.c:387-469)    */
 /* ------------------------------------------------------------------ */
-typedef struct ab_node { ab_cand c; struct ab_node *next; } ab_node;
-struct ab_list { ab_node *head; };
+/* The reference keeps an r-ordered singly linked list and walks it from
+ * the head for every threshold crossing.  Here the list is an array: the
+ * walk's stopping node ("first node with r >= rr, else the last node") is
+ * found by binary search while the array is ordered, and by the same
+ * linear walk otherwise (the reference can place a new candidate before
+ * a last node exactly 15 bins lower, which breaks the ordering). */
+struct ab_list {
+    ab_cand *c;
+    long long n, cap;
+    int ordered;
+};
 
-ab_list *ab_list_new(void) { return (ab_list *) calloc(1, sizeof(ab_list)); }
+ab_list *ab_list_new(void)
+{
+    ab_list *l = (ab_list *) calloc(1, sizeof(ab_list));
+    if (l) l->ordered = 1;
+    return l;
+}
 
 void ab_list_free(ab_list *l)
 {
     if (!l) return;
-    for (ab_node *n = l->head; n;) { ab_node *x = n->next; free(n); n = x; }
+    free(l->c);
     free(l);
+}
+
+static int list_reserve(ab_list *l, long long want)
+{
+    if (want <= l->cap) return 0;
+    long long nc = l->cap ? 2 * l->cap : 256;
+    while (nc < want) nc *= 2;
+    ab_cand *p = (ab_cand *) realloc(l->c, sizeof(ab_cand) * (size_t) nc);
+    if (!p) return -1;
+    l->c = p;
+    l->cap = nc;
+    return 0;
 }
 
 static void set_cand(ab_cand *c, float power, float sigma, int numharm, double rr,
@@ -410,101 +436,147 @@ static void set_cand(ab_cand *c, float power, float sigma, int numharm, double r
     c->r = rr; c->z = zz; c->w = ww;
 }
 
+static void list_check_order(ab_list *l, long long i)
+{
+    if (i > 0 && l->c[i - 1].r > l->c[i].r) l->ordered = 0;
+    if (i + 1 < l->n && l->c[i].r > l->c[i + 1].r) l->ordered = 0;
+}
+
 int ab_list_insert(ab_list *l, float power, float sigma, int numharm,
                    double rr, double zz, double ww)
 {
-    if (!l->head) {
-        l->head = (ab_node *) calloc(1, sizeof(ab_node));
-        set_cand(&l->head->c, power, sigma, numharm, rr, zz, ww);
+    if (list_reserve(l, l->n + 1)) return -1;
+    ab_cand *c = l->c;
+    if (l->n == 0) {
+        set_cand(&c[0], power, sigma, numharm, rr, zz, ww);
+        l->n = 1;
         return 1;
     }
+    long long t;                       /* the walk's stopping node */
+    if (l->ordered) {
+        long long lo = 0, hi = l->n - 1;          /* search [0, n-1) */
+        while (lo < hi) {
+            long long mid = (lo + hi) / 2;
+            if (c[mid].r < rr) lo = mid + 1; else hi = mid;
+        }
+        t = lo;
+    } else {
+        t = 0;
+        while (t < l->n - 1 && c[t].r < rr) t++;
+    }
+    long long p = t - 1;
     int added = 0;
-    ab_node *cur = l->head, *prev = NULL;
-    while (cur->next && cur->c.r < rr) { prev = cur; cur = cur->next; }
-    double next_diff = fabs(rr - cur->c.r);
-    double prev_diff = prev ? fabs(rr - prev->c.r) : AB_CLOSEST_R + 1.0;
+    double next_diff = fabs(rr - c[t].r);
+    double prev_diff = p >= 0 ? fabs(rr - c[p].r) : AB_CLOSEST_R + 1.0;
     if (prev_diff < AB_CLOSEST_R) {
-        if (prev->c.sigma < sigma) {
-            set_cand(&prev->c, power, sigma, numharm, rr, zz, ww);
+        if (c[p].sigma < sigma) {
+            set_cand(&c[p], power, sigma, numharm, rr, zz, ww);
+            list_check_order(l, p);
             added = 1;
         }
-        if (next_diff < AB_CLOSEST_R && cur->c.sigma < sigma) {
-            if (added) {             /* the new candidate already replaced prev */
-                prev->next = cur->next;
-                free(cur);
+        if (next_diff < AB_CLOSEST_R && c[t].sigma < sigma) {
+            if (added) {              /* the new candidate already replaced prev */
+                memmove(&c[t], &c[t + 1], sizeof(ab_cand) * (size_t) (l->n - t - 1));
+                l->n--;
             } else {
-                set_cand(&cur->c, power, sigma, numharm, rr, zz, ww);
+                set_cand(&c[t], power, sigma, numharm, rr, zz, ww);
+                list_check_order(l, t);
                 added = 1;
             }
         }
     } else if (next_diff < AB_CLOSEST_R) {
-        if (cur->c.sigma < sigma) {
-            set_cand(&cur->c, power, sigma, numharm, rr, zz, ww);
+        if (c[t].sigma < sigma) {
+            set_cand(&c[t], power, sigma, numharm, rr, zz, ww);
+            list_check_order(l, t);
             added = 1;
         }
     } else {
-        ab_node *n = (ab_node *) calloc(1, sizeof(ab_node));
-        set_cand(&n->c, power, sigma, numharm, rr, zz, ww);
         added = 1;
-        if (!cur->next && cur->c.r < rr - AB_CLOSEST_R) {
-            cur->next = n;
-        } else if (prev) {
-            prev->next = n;
-            n->next = cur;
-        } else {
-            n->next = l->head;
-            l->head = n;
-        }
+        long long at = (t == l->n - 1 && c[t].r < rr - AB_CLOSEST_R) ? l->n : t;
+        memmove(&c[at + 1], &c[at], sizeof(ab_cand) * (size_t) (l->n - at));
+        set_cand(&c[at], power, sigma, numharm, rr, zz, ww);
+        l->n++;
+        list_check_order(l, at);
     }
     return added;
 }
 
 long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout)
 {
-    long long n = 0;
-    for (const ab_node *p = l->head; p; p = p->next, n++)
-        if (out && n < maxout) out[n] = p->c;
-    return n;
+    if (out)
+        for (long long i = 0; i < l->n && i < maxout; i++) out[i] = l->c[i];
+    return l->n;
 }
 
-static int cmp_key(const void *a, const void *b)
+/* LSD radix sort of (key, index) by the 62-bit key, 16 bits per pass. */
+static int radix_order(const unsigned long long *keys, long long n, unsigned *order)
 {
-    unsigned long long x = *(const unsigned long long *) a, y = *(const unsigned long long *) b;
-    return (x > y) - (x < y);
+    unsigned *tmp = (unsigned *) malloc(sizeof(unsigned) * (size_t) n);
+    unsigned long long *k0 = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
+    unsigned long long *k1 = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
+    size_t *cnt = (size_t *) malloc(sizeof(size_t) * 65536);
+    if (!tmp || !k0 || !k1 || !cnt) {
+        free(tmp); free(k0); free(k1); free(cnt);
+        return AB_ERR_NOMEM;
+    }
+    for (long long i = 0; i < n; i++) { order[i] = (unsigned) i; k0[i] = keys[i]; }
+    for (int pass = 0; pass < 4; pass++) {
+        int sh = 16 * pass;
+        memset(cnt, 0, sizeof(size_t) * 65536);
+        for (long long i = 0; i < n; i++) cnt[(k0[i] >> sh) & 0xFFFF]++;
+        size_t sum = 0;
+        for (int d = 0; d < 65536; d++) { size_t c = cnt[d]; cnt[d] = sum; sum += c; }
+        for (long long i = 0; i < n; i++) {
+            size_t pos = cnt[(k0[i] >> sh) & 0xFFFF]++;
+            k1[pos] = k0[i];
+            tmp[pos] = order[i];
+        }
+        unsigned long long *kt = k0; k0 = k1; k1 = kt;
+        memcpy(order, tmp, sizeof(unsigned) * (size_t) n);
+    }
+    free(tmp); free(k0); free(k1); free(cnt);
+    return AB_OK;
 }
 
-/* Device hits carry (key, power); sort by key (= reference visit order:
- * block, stage, w, z, r) and replay search_ffdotpows' per-hit work. */
-int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows,
+/* Device hits carry (key, power, sigma); the key orders them as the
+ * reference visits them (block, stage, w, z, r).  Replays search_ffdotpows'
+ * per-hit work (src/accel_utils.c:1430-1442).  sigs may be NULL, in which
+ * case candidate_sigma is evaluated here. */
+int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows, const float *sigs,
                    long long nhits, const double *startr_tab, long long ntab, ab_list *l)
 {
     if (nhits <= 0) return AB_OK;
-    typedef struct { unsigned long long k; float p; } kp;
-    kp *arr = (kp *) malloc(sizeof(kp) * (size_t) nhits);
-    if (!arr) return AB_ERR_NOMEM;
-    for (long long i = 0; i < nhits; i++) { arr[i].k = keys[i]; arr[i].p = pows[i]; }
-    qsort(arr, (size_t) nhits, sizeof(kp), cmp_key);
+    unsigned *order = (unsigned *) malloc(sizeof(unsigned) * (size_t) nhits);
+    if (!order) return AB_ERR_NOMEM;
+    int rc = radix_order(keys, nhits, order);
+    if (rc) { free(order); return rc; }
+    long long cur_block = -1;
+    ab_hgeom g = {0, 0, 0, 0};
     for (long long i = 0; i < nhits; i++) {
-        unsigned long long k = arr[i].k;
+        unsigned long long k = keys[order[i]];
         int ri = (int) (k & 0xFFFF); k >>= AB_KEY_RBITS;
         int zi = (int) (k & 0xFFF); k >>= AB_KEY_ZBITS;
         int wi = (int) (k & 0x7F); k >>= AB_KEY_WBITS;
         int stage = (int) (k & 0x7); k >>= AB_KEY_SBITS;
         long long block = (long long) k;
-        if (block >= ntab) { free(arr); return AB_ERR_ARG; }
+        if (block >= ntab) { free(order); return AB_ERR_ARG; }
+        if (block != cur_block) {
+            /* the fundamental plane of the block (src/accel_utils.c:1034-1039) */
+            double startr = startr_tab[block];
+            g = ab_harm_geom(startr, startr + obs->rstep - AB_DR, 1, 1, obs->zlo, obs->wlo,
+                             obs->corr_uselen);
+            cur_block = block;
+        }
         int numharm = 1 << stage;
-        double startr = startr_tab[block];
-        /* the fundamental plane of the block (src/accel_utils.c:1034-1039) */
-        ab_hgeom g = ab_harm_geom(startr, startr + obs->rstep - AB_DR, 1, 1, obs->zlo,
-                                  obs->wlo, obs->corr_uselen);
-        float pw = arr[i].p;
-        float sig = (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
+        float pw = pows[order[i]];
+        float sig = sigs ? sigs[order[i]]
+                         : (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
         double rr = (g.rlo + ri * (double) AB_DR) / (double) numharm;
         double zz = (g.zlo + zi * (double) AB_DZ) / (double) numharm;
         double ww = (g.wlo + wi * (double) AB_DW) / (double) numharm;
-        ab_list_insert(l, pw, sig, numharm, rr, zz, ww);
+        if (ab_list_insert(l, pw, sig, numharm, rr, zz, ww) < 0) { free(order); return AB_ERR_NOMEM; }
     }
-    free(arr);
+    free(order);
     return AB_OK;
 }
 
@@ -576,3 +648,23 @@ long long ab_eliminate_harmonics(ab_cand *c, long long n)
     free(gone);
     return m;
 }
+
+int ab_bank_geometry(const ab_obs *obs, int *nbanks, int *info, int maxbanks)
+{
+    ab_bankset bs;
+    if (!obs || !nbanks) return AB_ERR_ARG;
+    int rc = ab_bankset_init(obs, &bs);
+    if (rc) return rc;
+    *nbanks = bs.nbanks;
+    if (!info) return AB_OK;
+    if (maxbanks < bs.nbanks) return AB_ERR_OVERFLOW;
+    for (int k = 0; k < bs.nbanks; k++) {
+        const ab_bank *b = &bs.b[k];
+        int *o = info + 8 * k;
+        o[0] = b->numharm; o[1] = b->harmnum; o[2] = b->nz; o[3] = b->nw;
+        o[4] = b->fftlen_ref; o[5] = b->L; o[6] = b->hw0; o[7] = b->numrs_max;
+    }
+    return AB_OK;
+}
+
+long long ab_num_blocks_main(const ab_obs *obs) { return obs ? ab_num_blocks(obs) : -1; }

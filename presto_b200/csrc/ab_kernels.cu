@@ -598,78 +598,91 @@ __device__ __forceinline__ unsigned long long make_key(long long block, int stag
            ((unsigned long long) zi << AB_KEY_RBITS) | (unsigned long long) ri;
 }
 
-constexpr int HS_ZT = 16;      // z rows per CTA
-constexpr int HS_RC = 1024;    // r cells per CTA
+constexpr int HS_ZT = 64;      // z rows per CTA
+constexpr int HS_RT = 256;     // r cells per CTA (one per thread)
 
-// Standard mode: CTA = (block, fundamental w row, z tile, r chunk).
+// Stage thresholds, fused: pow > powcut[s] after each stage's adds.  A
+// single warp vote per cell skips the compaction when no lane crossed.
+template <int STAGES>
+__device__ __forceinline__ void flush_hits(unsigned mask, const float *sums, long long block, int wi,
+                                           int z, int r, HitBuf hb)
+{
+    if (!__any_sync(0xffffffffu, mask != 0u)) return;
+#pragma unroll
+    for (int s = 0; s < STAGES; s++)
+        emit_hit((mask >> s) & 1u, make_key(block, s, wi, z, r), sums[s], hb);
+}
+
+// Standard mode.  CTA = (block, fundamental w row, tile of HS_ZT z rows,
+// HS_RT r cells); each thread owns one r cell, keeps its subharmonic r
+// indices (rinds) in registers and walks the z rows.  Plane row offsets of
+// every subharmonic for the tile's rows are staged in shared memory.
+template <int STAGES>
 __global__ void __launch_bounds__(256) k_harmsum_std(const ab_bank *banks, SearchConsts sc,
                                                      BlockBatch bb, const float *planes,
                                                      long long plane_per_block, HitBuf hb,
                                                      float *dbg, int dbg_bi)
 {
-    extern __shared__ unsigned short rsm[];             // [nsub][HS_RC]
-    __shared__ int s_zind[AB_MAX_BANKS][HS_ZT];
-    __shared__ int s_wind[AB_MAX_BANKS];
-    __shared__ long long s_base[AB_MAX_BANKS];
+    constexpr int NSUB = (1 << (STAGES - 1)) - 1;
+    __shared__ int s_row[NSUB > 0 ? NSUB : 1][HS_ZT];
     const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
     int x = blockIdx.x;
     const int zt = x % nzt;
     x /= nzt;
     const int wi = x % sc.numws;
     const int bi = x / sc.numws;
-    const int r0 = blockIdx.y * HS_RC;
+    const int r = blockIdx.y * HS_RT + threadIdx.x;
     const int z0 = zt * HS_ZT;
     const double startr = bb.startr[bi];
     const double lastr = startr + sc.rstep - AB_DR;
-    const ab_bank b0 = banks[0];
     const ab_hgeom g0 = ab_harm_geom(startr, lastr, 1, 1, sc.obs_zlo, sc.obs_wlo, sc.corr_uselen);
-    const int nsub = sc.nbanks - 1;
+    const bool ok = r < g0.numrs;
     const float *pb = planes + (long long) bi * plane_per_block;
-    for (int h = 0; h < nsub; h++) {
-        const ab_bank bh = banks[h + 1];
+    int rind[NSUB > 0 ? NSUB : 1];
+#pragma unroll
+    for (int h = 0; h < NSUB; h++) {
+        const ab_bank &bh = banks[h + 1];
         const ab_hgeom gh = ab_harm_geom(startr, lastr, bh.numharm, bh.harmnum, sc.obs_zlo,
                                          sc.obs_wlo, sc.corr_uselen);
-        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
-            int r = r0 + c;
-            int ri = (r < g0.numrs) ? ab_rind(startr, r, bh.f, gh.rlo) : 0;
-            rsm[h * HS_RC + c] = (unsigned short) min(max(ri, 0), bh.numrs_max - 1);
-        }
-        if (threadIdx.x < HS_ZT) {
-            int z = z0 + threadIdx.x;
+        int ri = ok ? ab_rind(startr, r, bh.f, gh.rlo) : 0;
+        rind[h] = min(max(ri, 0), bh.numrs_max - 1);
+        const int wind = min(max(ab_wind(g0.wlo, wi, bh.f, gh.wlo), 0), bh.nw - 1);
+        for (int zz = threadIdx.x; zz < HS_ZT; zz += blockDim.x) {
+            int z = z0 + zz;
             int zi = (z < sc.numz) ? ab_zind(sc.obs_zlo, z, bh.f, gh.zlo) : 0;
-            s_zind[h][threadIdx.x] = min(max(zi, 0), bh.nz - 1);
-        }
-        if (threadIdx.x == 0) {
-            s_wind[h] = min(max(ab_wind(g0.wlo, wi, bh.f, gh.wlo), 0), bh.nw - 1);
-            s_base[h] = bh.plane_off;
+            zi = min(max(zi, 0), bh.nz - 1);
+            s_row[h][zz] = (int) (bh.plane_off + ((long long) wind * bh.nz + zi) * bh.numrs_max);
         }
     }
     __syncthreads();
+    float pc[STAGES];
+#pragma unroll
+    for (int s = 0; s < STAGES; s++) pc[s] = sc.powcut[s];
+    const long long f_off = banks[0].plane_off + (long long) wi * sc.numz * banks[0].numrs_max;
+    const int f_stride = banks[0].numrs_max;
     const long long block = bb.block0 + bi;
     const int zend = min(z0 + HS_ZT, sc.numz);
+    const bool dump = dbg && bi == dbg_bi && ok;
     for (int z = z0; z < zend; z++) {
-        const float *frow = pb + b0.plane_off + ((long long) wi * sc.numz + z) * b0.numrs_max;
-        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
-            const int r = r0 + c;
-            const bool ok = r < g0.numrs;
-            float sum = ok ? frow[r] : 0.f;
-            emit_hit(ok && !(sum <= sc.powcut[0]), make_key(block, 0, wi, z, r), sum, hb);
-            if (dbg && bi == dbg_bi && ok) dbg[(((long long) 0 * sc.numws + wi) * sc.numz + z) * g0.numrs + r] = sum;
-            int h = 0;
-            for (int s = 1; s < sc.stages; s++) {
-                const int nh = 1 << (s - 1);
-                for (int j = 0; j < nh; j++, h++) {
-                    const ab_bank &bh = banks[h + 1];
-                    if (ok) {
-                        const float *srow = pb + s_base[h] +
-                                            ((long long) s_wind[h] * bh.nz + s_zind[h][z - z0]) * bh.numrs_max;
-                        sum += srow[rsm[h * HS_RC + c]];
-                    }
-                }
-                emit_hit(ok && !(sum <= sc.powcut[s]), make_key(block, s, wi, z, r), sum, hb);
-                if (dbg && bi == dbg_bi && ok)
-                    dbg[(((long long) s * sc.numws + wi) * sc.numz + z) * g0.numrs + r] = sum;
-            }
+        const int zz = z - z0;
+        float sums[STAGES];
+        float sum = ok ? pb[f_off + (long long) z * f_stride + r] : 0.f;
+        sums[0] = sum;
+        unsigned mask = (ok && !(sum <= pc[0])) ? 1u : 0u;
+        int h = 0;
+#pragma unroll
+        for (int s = 1; s < STAGES; s++) {
+#pragma unroll
+            for (int j = 0; j < (1 << (s - 1)); j++, h++)
+                if (ok) sum += pb[s_row[h][zz] + rind[h]];
+            sums[s] = sum;
+            if (ok && !(sum <= pc[s])) mask |= 1u << s;
+        }
+        flush_hits<STAGES>(mask, sums, block, wi, z, r, hb);
+        if (dump) {
+#pragma unroll
+            for (int s = 0; s < STAGES; s++)
+                dbg[(((long long) s * sc.numws + wi) * sc.numz + z) * g0.numrs + r] = sums[s];
         }
     }
 }
@@ -680,59 +693,87 @@ cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
                                cudaStream_t st)
 {
     int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
-    dim3 grid((unsigned) (bb.nblk * sc.numws * nzt), (sc.corr_uselen + HS_RC - 1) / HS_RC);
-    size_t smem = (size_t) (sc.nbanks > 1 ? sc.nbanks - 1 : 1) * HS_RC * sizeof(unsigned short);
-    cudaFuncSetAttribute(k_harmsum_std, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    k_harmsum_std<<<grid, 256, smem, st>>>(banks_dev, sc, bb, planes, plane_per_block, hb, dbg, dbg_bi);
+    dim3 grid((unsigned) (bb.nblk * sc.numws * nzt), (sc.corr_uselen + HS_RT - 1) / HS_RT);
+    switch (sc.stages) {
+#define AB_HS_CASE(S)                                                                          \
+    case S:                                                                                    \
+        k_harmsum_std<S><<<grid, HS_RT, 0, st>>>(banks_dev, sc, bb, planes, plane_per_block, hb, \
+                                                 dbg, dbg_bi);                                  \
+        break;
+        AB_HS_CASE(1)
+        AB_HS_CASE(2)
+        AB_HS_CASE(3)
+        AB_HS_CASE(4)
+        AB_HS_CASE(5)
+        AB_HS_CASE(6)
+#undef AB_HS_CASE
+        default:
+            return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
-// In-memory mode: the fundamental block and its subharmonics are read from
-// the full f-fdot plane.  CTA = (block, z tile, r chunk).
+// In-memory mode: fundamental and subharmonic powers come from the full
+// f-fdot plane (inmem_add_ffdotpows).  CTA = (block, z tile, r cells).
+template <int STAGES>
 __global__ void __launch_bounds__(256) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
                                                        const float *plane, HitBuf hb, float *dbg,
                                                        int dbg_bi)
 {
-    extern __shared__ int ism[];                        // [nsub][HS_RC]
-    __shared__ int s_zind[32][HS_ZT];
+    constexpr int NSUB = (1 << (STAGES - 1)) - 1;
+    __shared__ int s_zrow[NSUB > 0 ? NSUB : 1][HS_ZT];
     const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
     const int zt = blockIdx.x % nzt, bi = blockIdx.x / nzt;
-    const int r0 = blockIdx.y * HS_RC, z0 = zt * HS_ZT;
+    const int r = blockIdx.y * HS_RT + threadIdx.x, z0 = zt * HS_ZT;
     const double startr = bb.startr[bi];
     const ab_hgeom g0 = ab_harm_geom(startr, startr + sc.rstep - AB_DR, 1, 1, sc.obs_zlo,
                                      sc.obs_wlo, sc.corr_uselen);
+    const bool ok = r < g0.numrs;
     const int rlo = (int) g0.rlo;
-    int h = 0;
-    for (int s = 1; s < sc.stages; s++)
-        for (int hn = 1; hn < (1 << s); hn += 2, h++) {
-            const double f = (double) hn / (double) (1 << s);
-            for (int c = threadIdx.x; c < HS_RC; c += blockDim.x)
-                ism[h * HS_RC + c] = (r0 + c < g0.numrs)
-                    ? (int) min(max((long long) ab_inmem_rind(rlo, r0 + c, f), 0ll), sc.rlen - 1) : 0;
-            if (threadIdx.x < HS_ZT) {
-                int z = z0 + threadIdx.x;
-                s_zind[h][threadIdx.x] = (z < sc.numz) ? min(max(ab_inmem_zind(g0.zlo, z, f), 0), sc.numz - 1) : 0;
+    int rind[NSUB > 0 ? NSUB : 1];
+    {
+        int h = 0;
+#pragma unroll
+        for (int s = 1; s < STAGES; s++)
+#pragma unroll
+            for (int j = 0; j < (1 << (s - 1)); j++, h++) {
+                const double f = (double) (2 * j + 1) / (double) (1 << s);
+                long long ri = ok ? ab_inmem_rind(rlo, r, f) : 0;
+                rind[h] = (int) min(max(ri, 0ll), sc.rlen - 1);
+                for (int zz = threadIdx.x; zz < HS_ZT; zz += blockDim.x) {
+                    int z = z0 + zz;
+                    int zi = (z < sc.numz) ? ab_inmem_zind(g0.zlo, z, f) : 0;
+                    s_zrow[h][zz] = min(max(zi, 0), sc.numz - 1);
+                }
             }
-        }
+    }
     __syncthreads();
+    float pc[STAGES];
+#pragma unroll
+    for (int s = 0; s < STAGES; s++) pc[s] = sc.powcut[s];
     const long long block = bb.block0 + bi;
     const int zend = min(z0 + HS_ZT, sc.numz);
+    const bool dump = dbg && bi == dbg_bi && ok;
     for (int z = z0; z < zend; z++) {
-        const float *frow = plane + (long long) z * sc.rlen + (long long) rlo * AB_RDR;
-        for (int c = threadIdx.x; c < HS_RC; c += blockDim.x) {
-            const int r = r0 + c;
-            const bool ok = r < g0.numrs;
-            float sum = ok ? frow[r] : 0.f;
-            emit_hit(ok && !(sum <= sc.powcut[0]), make_key(block, 0, 0, z, r), sum, hb);
-            if (dbg && bi == dbg_bi && ok) dbg[((long long) 0 * sc.numz + z) * g0.numrs + r] = sum;
-            int hh = 0;
-            for (int s = 1; s < sc.stages; s++) {
-                const int nh = 1 << (s - 1);
-                for (int j = 0; j < nh; j++, hh++)
-                    if (ok) sum += plane[(long long) s_zind[hh][z - z0] * sc.rlen + ism[hh * HS_RC + c]];
-                emit_hit(ok && !(sum <= sc.powcut[s]), make_key(block, s, 0, z, r), sum, hb);
-                if (dbg && bi == dbg_bi && ok) dbg[((long long) s * sc.numz + z) * g0.numrs + r] = sum;
-            }
+        const int zz = z - z0;
+        float sums[STAGES];
+        float sum = ok ? plane[(long long) z * sc.rlen + (long long) rlo * AB_RDR + r] : 0.f;
+        sums[0] = sum;
+        unsigned mask = (ok && !(sum <= pc[0])) ? 1u : 0u;
+        int h = 0;
+#pragma unroll
+        for (int s = 1; s < STAGES; s++) {
+#pragma unroll
+            for (int j = 0; j < (1 << (s - 1)); j++, h++)
+                if (ok) sum += plane[(long long) s_zrow[h][zz] * sc.rlen + rind[h]];
+            sums[s] = sum;
+            if (ok && !(sum <= pc[s])) mask |= 1u << s;
+        }
+        flush_hits<STAGES>(mask, sums, block, 0, z, r, hb);
+        if (dump) {
+#pragma unroll
+            for (int s = 0; s < STAGES; s++)
+                dbg[((long long) s * sc.numz + z) * g0.numrs + r] = sums[s];
         }
     }
 }
@@ -742,11 +783,106 @@ cudaError_t launch_harmsum_inmem(const SearchConsts &sc, const BlockBatch &bb,
                                  cudaStream_t st)
 {
     int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
-    int nsub = (1 << (sc.stages - 1)) - 1;
-    dim3 grid((unsigned) (bb.nblk * nzt), (sc.corr_uselen + HS_RC - 1) / HS_RC);
-    size_t smem = (size_t) (nsub > 0 ? nsub : 1) * HS_RC * sizeof(int);
-    cudaFuncSetAttribute(k_harmsum_inmem, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    k_harmsum_inmem<<<grid, 256, smem, st>>>(sc, bb, fullplane, hb, dbg, dbg_bi);
+    dim3 grid((unsigned) (bb.nblk * nzt), (sc.corr_uselen + HS_RT - 1) / HS_RT);
+    switch (sc.stages) {
+#define AB_HI_CASE(S)                                                                          \
+    case S:                                                                                    \
+        k_harmsum_inmem<S><<<grid, HS_RT, 0, st>>>(sc, bb, fullplane, hb, dbg, dbg_bi);        \
+        break;
+        AB_HI_CASE(1)
+        AB_HI_CASE(2)
+        AB_HI_CASE(3)
+        AB_HI_CASE(4)
+        AB_HI_CASE(5)
+        AB_HI_CASE(6)
+#undef AB_HI_CASE
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ======================================================================
+// (d) candidate_sigma of every threshold crossing, FP64 on the device
+// (src/characteristics.c:459-546).  The chi-square tail of dof = 2 numsum
+// is the finite Poisson sum exp(-x) sum_{j<numsum} x^j / j!; the
+// reference's asymptotic branch (A&S 6.5.32 / 6.1.41) is kept as is.
+// ======================================================================
+__device__ double d_log_asym_inc_gamma(double a, double z)
+{
+    double x = 1.0, part = 1.0, term = 1.0;
+    for (int i = 1; fabs(part) > 1e-15 && i < 1000; i++) {
+        term *= (a - i);
+        part = term / pow(z, (double) i);
+        x += part;
+    }
+    return (a - 1.0) * log(z) - z + log(x);
+}
+
+__device__ double d_log_asym_gamma(double z)
+{
+    double x = (z - 0.5) * log(z) - z + 0.91893853320467267;
+    double y = 1.0 / (z * z);
+    x += (((-5.9523809523809529e-4 * y + 7.9365079365079365079365e-4) * y -
+           2.7777777777777777777778e-3) * y + 8.3333333333333333333333e-2) / z;
+    return x;
+}
+
+// x with Q(x) = q (standard normal upper tail): erfcinv start, two Newton
+// steps on log Q.
+__device__ double d_gauss_qinv(double q)
+{
+    bool flip = q > 0.5;
+    double qq = flip ? 1.0 - q : q;
+    double x = M_SQRT2 * erfcinv(2.0 * qq);
+    double lq = log(qq);
+    for (int it = 0; it < 2; it++) {
+        double Q = 0.5 * erfc(x * M_SQRT1_2);
+        double pdf = exp(-0.5 * x * x) * 0.39894228040143267794;
+        x += (log(Q) - lq) * Q / pdf;
+    }
+    return flip ? -x : x;
+}
+
+__device__ float d_candidate_sigma(double power, int numsum, double numtrials)
+{
+    if (power <= 0.0) return 0.f;
+    double chi2 = 2.0 * power, dof = 2.0 * numsum, logp;
+    if (chi2 > 1200.0 || (dof > 30 && chi2 > 100.0)) {
+        logp = d_log_asym_inc_gamma(0.5 * dof, 0.5 * chi2) - d_log_asym_gamma(0.5 * dof);
+    } else {
+        double x = 0.5 * chi2, term = 1.0, sum = 1.0;
+        for (int j = 1; j < numsum; j++) {
+            term *= x / j;
+            sum += term;
+        }
+        logp = -x + log(sum);
+    }
+    logp += log(numtrials);
+    double sig;
+    if (logp < -600.0) {
+        double t = sqrt(-2.0 * logp);
+        sig = t - (2.515517 + t * (0.802853 + t * 0.010328)) /
+                  (1.0 + t * (1.432788 + t * (0.189269 + t * 0.001308)));
+    } else {
+        sig = d_gauss_qinv(exp(logp));
+    }
+    return (float) (sig < 0.0 ? 0.0 : sig);
+}
+
+__global__ void k_sigma(const unsigned long long *keys, const float *pows, const unsigned *count,
+                        unsigned cap, float *sig, SigmaConsts c)
+{
+    unsigned n = min(*count, cap);
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int stage = (int) ((keys[i] >> (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS)) & 0x7);
+        sig[i] = d_candidate_sigma((double) pows[i], 1 << stage, c.numindep[stage]);
+    }
+}
+
+cudaError_t launch_sigma(HitBuf hb, float *sig, const SigmaConsts &c, cudaStream_t st)
+{
+    k_sigma<<<296, 256, 0, st>>>(hb.keys, hb.pows, hb.count, hb.cap, sig, c);
     return cudaGetLastError();
 }
 
@@ -820,6 +956,28 @@ cudaError_t launch_threshold(const float *pw, int numws, int numzs, int numrs, f
                              int stage, HitBuf hb, cudaStream_t st)
 {
     k_threshold<<<296, 256, 0, st>>>(pw, numws, numzs, numrs, powcut, stage, hb);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) k_fma_peak(float *out, int iters)
+{
+    float a[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = (threadIdx.x + j) * 1e-7f;
+    const float b = 0.9999999f, c = 1e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) a[j] = fmaf(a[j], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) s += a[j];
+    if (s == 1234.5f) out[0] = s;
+}
+
+cudaError_t launch_fma_peak(float *out, int iters, int sms, cudaStream_t st)
+{
+    k_fma_peak<<<sms * 8, 256, 0, st>>>(out, iters);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,10 @@ struct CorrItem {              // one CTA of the correlation kernel
     int bi, bank, t0, nt;
 };
 
+struct SigmaConsts {
+    double numindep[AB_MAX_STAGES];
+};
+
 struct HitBuf {
     unsigned long long *keys;
     float *pows;
@@ -66,6 +70,8 @@ cudaError_t launch_harmsum_inmem(const SearchConsts &sc, const BlockBatch &bb,
                                  const float *fullplane, HitBuf hb, float *dbg, int dbg_bi,
                                  cudaStream_t st);
 
+cudaError_t launch_sigma(HitBuf hb, float *sig, const SigmaConsts &c, cudaStream_t st);
+
 // per-function drop-in helpers
 cudaError_t launch_add_ffdot(float *fund, const float *sub, int numws, int numzs, int numrs,
                              int sub_numzs, int sub_numrs, double f, int fund_wlo, int sub_wlo,
@@ -75,5 +81,7 @@ cudaError_t launch_inmem_add(float *fund, const float *plane, long long rlen, in
                              int numrs, int fund_rlo, int fund_zlo, double f, cudaStream_t st);
 cudaError_t launch_threshold(const float *pw, int numws, int numzs, int numrs, float powcut,
                              int stage, HitBuf hb, cudaStream_t st);
+
+cudaError_t launch_fma_peak(float *out, int iters, int sms, cudaStream_t st);
 
 }  // namespace ab
