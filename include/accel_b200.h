@@ -171,6 +171,34 @@ int ab_gen_response(ab_ctx *ctx, double roffset, int numbetween, double z, doubl
 int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int wi, int zi,
                    ab_fcomplex *out, int maxlen, int *fftlen_dev);
 
+/* Plane generation for one block and one harmonic that allocates no memory.
+ * No counterpart in the reference: it is ab_subharm_fderivs_vol for callers
+ * that cannot call cudaMalloc (pipelines that reserve all device memory at
+ * start-up, hosts whose device memory belongs to another allocator, or
+ * stream-ordered code where an allocation would synchronise the device).
+ * Inputs and outputs are device pointers owned by the caller: d_fft holds
+ * obs->numbins bins; d_templates the bank of harmonic harmnum/numharm as
+ * [numkern_wdim][numkern_zdim][L] FFT'd templates (L and the dimensions from
+ * ab_bank_geometry, each template as ab_bank_kernel returns it); d_powers
+ * receives powers[numws][numzs][numrs] (capacity in floats).  The block
+ * starts at fullrlo and ends at fullrlo + rstep - 0.5.  Work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream) of the calling
+ * thread's current device; the call does not wait for it.
+ * The engine's intermediates live in one static device array of 160 KiB
+ * that every GPU loading the library keeps until exit, so the bank must need
+ * at most 8192 correlation work items and a data spectrum of at most 2048
+ * points; larger banks return AB_ERR_BUDGET (and a line on stderr).  The
+ * array is shared by all calls and keeps the last call's contents; every
+ * word a call reads is written earlier in the same call, so nothing needs
+ * clearing, but calls whose GPU work overlaps (different streams, threads)
+ * race on it.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress): make that first call before any stream capture.
+ * meta_out (optional) receives the plane's rlo, zlo, wlo and sizes. */
+int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnum, double fullrlo,
+                           const ab_fcomplex *d_fft, const ab_fcomplex *d_templates,
+                           float *d_powers, size_t powers_capacity, void *stream,
+                           ab_ffdotpows *meta_out);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -29,6 +29,7 @@ EXPORTS = [
     "ab_equivalent_gaussian_sigma", "ab_sort_cands", "ab_eliminate_harmonics",
     "ab_ctx_set_profiling", "ab_ctx_kernel_times", "ab_ctx_reset_kernel_times",
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
+    "ab_fderivs_vol_noalloc",
 ]
 
 
@@ -128,6 +129,8 @@ def lib():
     L.ab_num_blocks_main.restype = ll
     L.ab_num_blocks_main.argtypes = [C.POINTER(Obs)]
     L.ab_measure_fp32_peak.argtypes = [vp, C.POINTER(d)]
+    L.ab_fderivs_vol_noalloc.argtypes = [C.POINTER(Obs), i, i, d, vp, vp, vp, C.c_size_t, vp,
+                                         C.POINTER(FFDotPows)]
     L.ab_ctx_launch_count.restype = ll
     L.ab_ctx_launch_count.argtypes = [vp]
     _lib = L

@@ -1,0 +1,152 @@
+// ab_noalloc.cu -- plane generation for one block and one harmonic that
+// allocates no memory.
+//
+// For callers that cannot call cudaMalloc: real-time pipelines that reserve
+// all device memory at start-up and forbid allocation in their processing
+// loop, hosts whose device memory belongs to another allocator (a framework's
+// caching pool), and stream-ordered code where an allocation would
+// synchronise the device.  The caller passes every input and output as a
+// device pointer; the engine's own intermediates (the block's data spectrum,
+// the bank descriptor, the block start and the correlation work list) live
+// in a file-scope static device array instead of context memory.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+
+#include "ab_host.h"
+#include "ab_index.h"
+#include "ab_kernels.h"
+
+using namespace ab;
+
+namespace {
+
+// Static scratch: 160 KiB, held by every GPU that loads the library until exit.
+constexpr size_t kScratchBytes = 160u << 10;
+constexpr size_t kDescOff = 0;          // ab_bank
+constexpr size_t kStartOff = 1024;      // double
+constexpr size_t kItemsOff = 2048;      // CorrItem[kMaxItems]
+constexpr int kMaxItems = 8192;
+constexpr size_t kXhatOff = kItemsOff + sizeof(CorrItem) * kMaxItems;   // float2[L/2]
+
+static_assert(sizeof(ab_bank) <= kStartOff - kDescOff, "descriptor slot");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void *g_scratch_addr[kMaxDevices];
+
+// Address of the static array on the current device; the first call on a
+// device looks it up (cudaGetSymbolAddress) with that device current.
+cudaError_t scratch_address(int dev, unsigned char **out)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+    return cudaSuccess;
+}
+
+__global__ void k_noalloc_setup(ab_bank desc, double startr, int ntmpl, int tile, int nitems,
+                                ab_bank *d_desc, double *d_start, CorrItem *d_items)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *d_desc = desc;
+        *d_start = startr;
+    }
+    if (i < nitems) {
+        int t0 = i * tile;
+        d_items[i] = CorrItem{0, 0, t0, min(tile, ntmpl - t0)};
+    }
+}
+
+}  // namespace
+
+extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnum,
+                                      double fullrlo, const ab_fcomplex *d_fft,
+                                      const ab_fcomplex *d_templates, float *d_powers,
+                                      size_t powers_capacity, void *stream,
+                                      ab_ffdotpows *meta_out)
+{
+    if (!obs || !d_fft || !d_templates || !d_powers) return AB_ERR_ARG;
+    ab_bankset bs;
+    if (ab_bankset_init(obs, &bs) != AB_OK) return AB_ERR_ARG;
+    int k = -1;
+    for (int i = 0; i < bs.nbanks; i++)
+        if (bs.b[i].numharm == numharm && bs.b[i].harmnum == harmnum) k = i;
+    if (k < 0) return AB_ERR_ARG;
+    ab_bank b = bs.b[k];
+    const double fullrhi = fullrlo + obs->rstep - AB_DR;
+    const ab_hgeom g = ab_harm_geom(fullrlo, fullrhi, numharm, harmnum, obs->zlo, obs->wlo,
+                                    obs->corr_uselen);
+    const size_t need = (size_t) b.nw * b.nz * g.numrs;
+    if (meta_out) {
+        meta_out->rlo = g.rlo;
+        meta_out->zlo = g.zlo;
+        meta_out->wlo = g.wlo;
+        meta_out->numrs = g.numrs;
+        meta_out->numzs = b.nz;
+        meta_out->numws = b.nw;
+    }
+    if (powers_capacity < need) return AB_ERR_OVERFLOW;
+    if (g.numrs > b.numrs_max) return AB_ERR_ARG;
+    const int G = 4096 / b.L, tile = 16 * G;
+    const int nitems = (b.ntmpl + tile - 1) / tile;
+    if (nitems > kMaxItems || kXhatOff + sizeof(float2) * (size_t) (b.L / 2) > kScratchBytes) {
+        fprintf(stderr, "ab_fderivs_vol_noalloc: bank %d/%d needs %d work items and a %d-point "
+                        "spectrum; the static scratch holds %d items and %zu bytes\n",
+                harmnum, numharm, nitems, b.L / 2, kMaxItems, kScratchBytes);
+        return AB_ERR_BUDGET;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AB_ERR_CUDA;
+    unsigned char *scr = nullptr;
+    if (scratch_address(dev, &scr) != cudaSuccess) return AB_ERR_CUDA;
+    ab_bank *d_desc = reinterpret_cast<ab_bank *>(scr + kDescOff);
+    double *d_start = reinterpret_cast<double *>(scr + kStartOff);
+    CorrItem *d_items = reinterpret_cast<CorrItem *>(scr + kItemsOff);
+    float2 *d_xhat = reinterpret_cast<float2 *>(scr + kXhatOff);
+
+    // The caller's arrays: templates [nw][nz][L] at offset 0, powers
+    // [nw][nz][numrs] (row stride numrs), data spectrum at scratch offset 0.
+    b.tmpl_off = 0;
+    b.plane_off = 0;
+    b.xhat_off = 0;
+    b.numrs_max = g.numrs;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_noalloc_setup<<<(nitems + 255) / 256, 256, 0, st>>>(b, fullrlo, b.ntmpl, tile, nitems,
+                                                           d_desc, d_start, d_items);
+    if (cudaGetLastError() != cudaSuccess) return AB_ERR_CUDA;
+
+    SearchConsts sc{};
+    sc.obs_zlo = obs->zlo;
+    sc.obs_wlo = obs->wlo;
+    sc.obs_rlo = obs->rlo;
+    sc.obs_lobin = obs->lobin;
+    sc.numbins = obs->numbins;
+    sc.rlen = (obs->highestbin + obs->corr_uselen) * (long long) AB_RDR;
+    sc.corr_uselen = obs->corr_uselen;
+    sc.rstep = obs->rstep;
+    sc.numz = obs->numz;
+    sc.numws = obs->numw > 0 ? obs->numw : 1;
+    sc.stages = obs->numharmstages;
+    sc.inmem = 0;
+    sc.nbanks = 1;
+    sc.nph = obs->nph;
+    BlockBatch bb{d_start, 0, 1, 0};
+    if (launch_prep(d_desc, &b, 1, sc, bb, reinterpret_cast<const float2 *>(d_fft), d_xhat,
+                    b.L / 2, st) != cudaSuccess)
+        return AB_ERR_CUDA;
+    if (launch_corr(b.L, d_desc, sc, bb, d_items, nitems, d_xhat, b.L / 2,
+                    reinterpret_cast<const float2 *>(d_templates), d_powers, 0, nullptr,
+                    st) != cudaSuccess)
+        return AB_ERR_CUDA;
+    return AB_OK;
+}
