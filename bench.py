@@ -305,6 +305,8 @@ def run_ours(args):
                                  "kernel_ms_per_search": harm_ms},
             "kernel_ms_per_search": {"templates": kms[0] / args.steps, "prep": kms[1] / args.steps,
                                      "corr": corr_ms_per_search, "harmsum": harm_ms},
+            "host_ms_per_search": {"outside_replay": kms[4] / args.steps,
+                                   "sort_and_replay_overlapped": kms[5] / args.steps},
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu:

@@ -125,6 +125,9 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
               long long first_block, long long max_blocks,
               ab_cand *cands, long long maxcands, long long *numcands);
 
+/* Candidate list of the last ab_search (all of it, whatever maxcands was). */
+int ab_last_cands(ab_ctx *ctx, ab_cand *out, long long maxout, long long *numcands);
+
 /* Raw threshold crossings of the last ab_search, in reference visit order
  * (block, stage, w, z, r): block ordinal, stage, w index, z index, r index,
  * power.  Returns the count through *numhits. */
@@ -208,7 +211,9 @@ int  ab_sort_cands(ab_cand *cands, long long n);
 long long ab_eliminate_harmonics(ab_cand *cands, long long n);
 
 /* Kernel timing (CUDA events around each launch on the context stream).
- * kinds: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search. */
+ * kinds: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search (device
+ * ms); 4 host work until the last launch is queued, 5 host sort + replay,
+ * 6 wait for the device and hit read-back (host wall ms, ab_search only). */
 int ab_ctx_set_profiling(ab_ctx *ctx, int on);
 int ab_ctx_kernel_times(ab_ctx *ctx, double *ms, long long *launches, int nkinds);
 int ab_ctx_reset_kernel_times(ab_ctx *ctx);

@@ -22,7 +22,7 @@ ERRORS = {-1: "AB_ERR_ARG", -2: "AB_ERR_CUDA", -3: "AB_ERR_NOMEM", -4: "AB_ERR_O
 EXPORTS = [
     "ab_params_default", "ab_ctx_create", "ab_ctx_destroy", "ab_ctx_last_error",
     "ab_ctx_stream", "ab_ctx_set_hbm_budget", "ab_obs_init", "ab_prepare", "ab_search",
-    "ab_last_hits", "ab_set_spectrum", "ab_subharm_fderivs_vol", "ab_add_ffdotpows",
+    "ab_last_hits", "ab_last_cands", "ab_set_spectrum", "ab_subharm_fderivs_vol", "ab_add_ffdotpows",
     "ab_fund_to_ffdotplane", "ab_inmem_add_ffdotpows", "ab_candlist_new", "ab_candlist_free",
     "ab_candlist_get", "ab_candlist_insert", "ab_search_ffdotpows", "ab_block_stage_sums", "ab_gen_response",
     "ab_bank_kernel", "ab_candidate_sigma", "ab_power_for_sigma", "ab_chi2_logp",
@@ -95,6 +95,7 @@ def lib():
     L.ab_prepare.argtypes = [vp, C.POINTER(Obs)]
     L.ab_search.argtypes = [vp, C.POINTER(Obs), vp, i, ll, ll, C.POINTER(Cand), ll,
                             C.POINTER(ll)]
+    L.ab_last_cands.argtypes = [vp, C.POINTER(Cand), ll, C.POINTER(ll)]
     L.ab_last_hits.argtypes = [vp, C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i),
                                C.POINTER(i), C.POINTER(C.c_float), ll, C.POINTER(ll)]
     L.ab_set_spectrum.argtypes = [vp, C.POINTER(Obs), vp]
@@ -244,11 +245,10 @@ class Context:
     def prepare(self, obs):
         self._check(self.L.ab_prepare(self.ptr, C.byref(obs)), "ab_prepare")
 
-    def search(self, obs, fft, first_block=0, max_blocks=-1, maxcands=1 << 20, device_ptr=None):
+    def search(self, obs, fft, first_block=0, max_blocks=-1, device_ptr=None):
         """All blocks and stages of the main search loop; returns the
         candidate list in the reference's order as a list of tuples
         (power, sigma, numharm, r, z, w)."""
-        cands = (Cand * maxcands)()
         n = C.c_longlong()
         if device_ptr is not None:
             src, on_dev = C.c_void_p(device_ptr), 1
@@ -258,7 +258,9 @@ class Context:
                 raise AccelError("spectrum shorter than obs.numbins")
             src, on_dev = C.c_void_p(fft.ctypes.data), 0
         self._check(self.L.ab_search(self.ptr, C.byref(obs), src, on_dev, int(first_block),
-                                     int(max_blocks), cands, maxcands, C.byref(n)), "ab_search")
+                                     int(max_blocks), None, 0, C.byref(n)), "ab_search")
+        cands = (Cand * max(n.value, 1))()
+        self._check(self.L.ab_last_cands(self.ptr, cands, n.value, C.byref(n)), "ab_last_cands")
         return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in cands[:n.value]]
 
     def last_hits(self):
@@ -358,9 +360,12 @@ class Context:
         self.L.ab_ctx_set_profiling(self.ptr, int(on))
 
     def kernel_times(self):
-        ms = (C.c_double * 4)()
-        n = (C.c_longlong * 4)()
-        self.L.ab_ctx_kernel_times(self.ptr, ms, n, 4)
+        """Per kind: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search
+        (device ms); 4 host setup until the last launch is queued, 5 host sort +
+        replay, 6 wait for the device and hit read-back (host wall ms)."""
+        ms = (C.c_double * 7)()
+        n = (C.c_longlong * 7)()
+        self.L.ab_ctx_kernel_times(self.ptr, ms, n, 7)
         return list(ms), list(n)
 
     def reset_kernel_times(self):

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,7 +21,11 @@ using namespace ab;
 namespace {
 
 constexpr int kTwLog2 = 14;                 // FP64 twiddle table for FFTs up to 16384
-constexpr int kNumKinds = 4;                // templates, prep, corr, harmsum
+constexpr int kNumKinds = 7;   // templates, prep, corr, harmsum (device); host setup, host replay, hit fetch
+double now_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 template <typename T> struct DevBuf {
     T *p = nullptr;
@@ -72,22 +77,30 @@ struct ab_ctx {
     DevBuf<CorrItem> items;
     DevBuf<float> dbg;
     DevBuf<float> tmpa, tmpb;
+    DevBuf<unsigned> errw;                   // device error word
 
-    // hits
-    DevBuf<unsigned long long> keys;
-    DevBuf<float> pows;
-    DevBuf<unsigned int> count;
-    DevBuf<float> sigs;
+    // hits: two sets so that the host replays one batch while the device
+    // fills the other
+    DevBuf<unsigned long long> keys, keys2;
+    DevBuf<float> pows, pows2;
+    DevBuf<unsigned int> count, count2;
+    DevBuf<float> sigs, sigs2;
     std::vector<float> hsigs;
-    unsigned int hit_cap = 1u << 23;
+    unsigned *hcount = nullptr;              // pinned [2]
+    cudaEvent_t batch_done[2] = {nullptr, nullptr};
+    cudaStream_t cstream = nullptr;          // device->host copies of hits
+    unsigned int hit_cap = 1u << 22;
     std::vector<unsigned long long> hkeys;
     std::vector<float> hpows;
     std::vector<double> hstart;
+    std::vector<ab_cand> last_cands;
+    unsigned overflow_need = 0;              // hits one batch wanted beyond hit_cap
+    bool hits_truncated = false;             // host copy holds only the latest batches
 
     // timing
     bool prof = false;
-    double kms[kNumKinds] = {0, 0, 0, 0};
-    long long kn[kNumKinds] = {0, 0, 0, 0};
+    double kms[kNumKinds] = {0, 0, 0, 0, 0, 0, 0};
+    long long kn[kNumKinds] = {0, 0, 0, 0, 0, 0, 0};
     long long launches = 0;
     std::vector<cudaEvent_t> evpool;
     std::vector<std::pair<int, int>> evpending;   // (kind, event index)
@@ -203,6 +216,7 @@ static SearchConsts make_consts(const ab_obs *obs, const ab_bankset &bs)
     sc.nbanks = bs.nbanks;
     sc.nph = obs->nph;
     for (int i = 0; i < AB_MAX_STAGES; i++) sc.powcut[i] = i < obs->numharmstages ? obs->powcut[i] : 0.f;
+    sc.err = nullptr;
     return sc;
 }
 
@@ -267,13 +281,108 @@ static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
     return AB_OK;
 }
 
-// Core search over main-loop blocks [first, first+count).  Hits accumulate in
-// the context's hit buffer (reset here).  dbg_block >= 0 dumps its stage sums.
+// Hit set i of the context (0 or 1).
+struct HitSet {
+    unsigned long long *keys;
+    float *pows, *sigs;
+    unsigned *count;
+};
+
+static int ensure_hitsets(ab_ctx *ctx)
+{
+    CK(ctx->keys.ensure(ctx->hit_cap));
+    CK(ctx->pows.ensure(ctx->hit_cap));
+    CK(ctx->sigs.ensure(ctx->hit_cap));
+    CK(ctx->count.ensure(1));
+    CK(ctx->keys2.ensure(ctx->hit_cap));
+    CK(ctx->pows2.ensure(ctx->hit_cap));
+    CK(ctx->sigs2.ensure(ctx->hit_cap));
+    CK(ctx->count2.ensure(1));
+    if (!ctx->hcount) CK(cudaHostAlloc((void **) &ctx->hcount, 2 * sizeof(unsigned), cudaHostAllocDefault));
+    for (int i = 0; i < 2; i++)
+        if (!ctx->batch_done[i]) CK(cudaEventCreateWithFlags(&ctx->batch_done[i], cudaEventDisableTiming));
+    if (!ctx->cstream) CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+    return AB_OK;
+}
+
+static HitSet hitset(ab_ctx *ctx, int i)
+{
+    return i == 0 ? HitSet{ctx->keys.p, ctx->pows.p, ctx->sigs.p, ctx->count.p}
+                  : HitSet{ctx->keys2.p, ctx->pows2.p, ctx->sigs2.p, ctx->count2.p};
+}
+
+// After the launches that fill hit set i: sigma of every hit, the count to
+// pinned host memory, and an event marking the set complete.
+static int close_hitset(ab_ctx *ctx, const ab_obs *obs, int i)
+{
+    HitSet h = hitset(ctx, i);
+    SigmaConsts c{};
+    for (int k = 0; k < AB_MAX_STAGES; k++)
+        c.numindep[k] = k < obs->numharmstages ? (double) obs->numindep[k] : 1.0;
+    HitBuf hb{h.keys, h.pows, h.count, ctx->hit_cap};
+    CK(launch_sigma(hb, h.sigs, c, ctx->stream));
+    ctx->launches++;
+    CK(cudaMemcpyAsync(ctx->hcount + i, h.count, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaEventRecord(ctx->batch_done[i], ctx->stream));
+    return AB_OK;
+}
+
+// Waits for hit set i, appends its hits to the context's host copy and, if
+// list is given, replays them (they all belong to blocks after those of any
+// earlier set, so set-by-set replay is the reference's visit order).
+static int drain_hitset(ab_ctx *ctx, const ab_obs *obs, int i, ab_list *list, double *replay_ms)
+{
+    CK(cudaEventSynchronize(ctx->batch_done[i]));
+    unsigned n = ctx->hcount[i];
+    if (n > ctx->hit_cap) {
+        ctx->overflow_need = n;
+        return fail(ctx, AB_ERR_OVERFLOW, "%u threshold crossings in one batch exceed the hit "
+                                          "buffer (%u)", n, ctx->hit_cap);
+    }
+    if (n == 0) return AB_OK;
+    HitSet h = hitset(ctx, i);
+    if (ctx->hkeys.size() + n > (size_t) 1 << 24) {
+        // keep host memory bounded: the replay only needs this batch
+        ctx->hkeys.clear();
+        ctx->hpows.clear();
+        ctx->hsigs.clear();
+        ctx->hits_truncated = true;
+    }
+    size_t old = ctx->hkeys.size();
+    ctx->hkeys.resize(old + n);
+    ctx->hpows.resize(old + n);
+    ctx->hsigs.resize(old + n);
+    CK(cudaMemcpyAsync(ctx->hkeys.data() + old, h.keys, sizeof(unsigned long long) * n,
+                       cudaMemcpyDeviceToHost, ctx->cstream));
+    CK(cudaMemcpyAsync(ctx->hpows.data() + old, h.pows, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                       ctx->cstream));
+    CK(cudaMemcpyAsync(ctx->hsigs.data() + old, h.sigs, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                       ctx->cstream));
+    CK(cudaStreamSynchronize(ctx->cstream));
+    if (list) {
+        double t0 = now_ms();
+        int rc = ab_replay_hits(obs, ctx->hkeys.data() + old, ctx->hpows.data() + old,
+                                ctx->hsigs.data() + old, n, ctx->hstart.data(),
+                                ab_num_blocks(obs), list);
+        if (replay_ms) *replay_ms += now_ms() - t0;
+        if (rc) return fail(ctx, rc, "hit replay failed");
+    }
+    return AB_OK;
+}
+
+// Core search over main-loop blocks [first, first+count).  All hits are kept
+// in ctx->hkeys/hpows/hsigs; with list != NULL they are also replayed into
+// the candidate list, batch by batch while the device computes the next
+// batch.  dbg_block >= 0 dumps that block's stage sums into ctx->dbg.
 static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long long first,
-                       long long count, long long dbg_block)
+                       long long count, long long dbg_block, ab_list *list,
+                       double *replay_ms = nullptr)
 {
     const ab_bankset &bs = ctx->bs;
     SearchConsts sc = make_consts(obs, bs);
+    CK(ctx->errw.ensure(1));
+    CK(cudaMemsetAsync(ctx->errw.p, 0, sizeof(unsigned), ctx->stream));
+    sc.err = ctx->errw.p;
     long long nmain = ab_num_blocks(obs), npre = ab_num_preblocks(obs);
     if (first < 0) first = 0;
     if (count < 0 || first + count > nmain) count = nmain - first;
@@ -287,11 +396,12 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     CK(ctx->startr.ensure(ctx->hstart.size()));
     CK(cudaMemcpyAsync(ctx->startr.p, ctx->hstart.data(), sizeof(double) * (nmain + npre),
                        cudaMemcpyHostToDevice, ctx->stream));
-    CK(ctx->keys.ensure(ctx->hit_cap));
-    CK(ctx->pows.ensure(ctx->hit_cap));
-    CK(ctx->count.ensure(1));
-    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned), ctx->stream));
-    HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
+    int rc = ensure_hitsets(ctx);
+    if (rc) return rc;
+    ctx->hkeys.clear();
+    ctx->hpows.clear();
+    ctx->hsigs.clear();
+    ctx->hits_truncated = false;
     const int nstage = obs->numharmstages;
     const size_t dbg_floats = (size_t) nstage * sc.numws * sc.numz * obs->corr_uselen;
     if (dbg_block >= 0) CK(ctx->dbg.ensure(dbg_floats));
@@ -309,12 +419,11 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
                                  sizeof(float) * first_col, sc.numz, ctx->stream));
         CK(ctx->xhat.ensure((size_t) std::max<long long>(nall, 1) * bs.xhat_per_block));
         CorrPlan plan;
-        // item arrays are built per launch size
         for (int pass = 0; pass < 2; pass++) {
             long long nb = pass == 0 ? npre : nmain;
             if (nb == 0) continue;
             BlockBatch bb{ctx->startr.p + (pass == 0 ? nmain : 0), 0, (int) nb, pass == 0};
-            int rc = run_prep(ctx, sc, bb, dfft, 0, 1);
+            rc = run_prep(ctx, sc, bb, dfft, 0, 1);
             if (rc) return rc;
             build_corr_plan(bs, (int) nb, 0, 1, plan);
             CK(ctx->items.ensure(plan.items.size()));
@@ -325,8 +434,10 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             // the item upload is reused by the next pass: wait before overwriting
             CK(cudaStreamSynchronize(ctx->stream));
         }
+        CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned), ctx->stream));
         if (count > 0) {
             BlockBatch bb{ctx->startr.p + first, first, (int) count, 0};
+            HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
             tick(ctx, 3, true);
             cudaError_t e = launch_harmsum_inmem(sc, bb, ctx->fullplane.p, hb,
                                                  dbg_block >= 0 ? ctx->dbg.p : nullptr,
@@ -336,15 +447,20 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             if (e != cudaSuccess)
                 return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
         }
-        return AB_OK;
+        rc = close_hitset(ctx, obs, 0);
+        if (rc) return rc;
+        return drain_hitset(ctx, obs, 0, list, replay_ms);
     }
 
-    // standard mode: batches of blocks, each correlated for every bank, then summed
+    // standard mode: batches of blocks, each correlated for every bank, then
+    // summed; hit sets alternate so the host replays batch k-1 meanwhile
     const size_t per_block = (size_t) bs.plane_per_block * sizeof(float) +
                              (size_t) bs.xhat_per_block * sizeof(float2);
     long long B = (long long) (ctx->scratch_budget / std::max<size_t>(per_block, 1));
     if (B < 1) B = 1;
     if (B > 512) B = 512;
+    // several batches per search let the replay overlap the device work
+    if (count >= 8 && B > (count + 7) / 8) B = (count + 7) / 8;
     if (B > count) B = std::max<long long>(count, 1);
     CK(ctx->planes.ensure((size_t) B * bs.plane_per_block));
     CK(ctx->xhat.ensure((size_t) B * bs.xhat_per_block));
@@ -358,16 +474,21 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     if (rem)
         CK(cudaMemcpyAsync(ctx->items.p + full.items.size(), tail.items.data(),
                            sizeof(CorrItem) * tail.items.size(), cudaMemcpyHostToDevice, ctx->stream));
-    for (long long b0 = first; b0 < first + count; b0 += B) {
+    int k = 0;
+    for (long long b0 = first; b0 < first + count; b0 += B, k++) {
         int nb = (int) std::min<long long>(B, first + count - b0);
+        const int set = k & 1;
+        HitSet h = hitset(ctx, set);
+        CK(cudaMemsetAsync(h.count, 0, sizeof(unsigned), ctx->stream));
         BlockBatch bb{ctx->startr.p + b0, b0, nb, 0};
-        int rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
+        rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
         if (rc) return rc;
         const CorrPlan &p = (nb == B) ? full : tail;
         const CorrItem *di = ctx->items.p + ((nb == B) ? 0 : full.items.size());
         rc = run_corr(ctx, sc, bb, p, di, ctx->planes.p, bs.plane_per_block, nullptr);
         if (rc) return rc;
         int dbi = (dbg_block >= b0 && dbg_block < b0 + nb) ? (int) (dbg_block - b0) : -1;
+        HitBuf hb{h.keys, h.pows, h.count, ctx->hit_cap};
         tick(ctx, 3, true);
         cudaError_t e = launch_harmsum_std(ctx->dbanks.p, sc, bb, ctx->planes.p, bs.plane_per_block,
                                            hb, dbi >= 0 ? ctx->dbg.p : nullptr, dbi, ctx->stream);
@@ -375,21 +496,19 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         ctx->launches++;
         if (e != cudaSuccess)
             return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
+        rc = close_hitset(ctx, obs, set);
+        if (rc) return rc;
+        if (k > 0) {
+            rc = drain_hitset(ctx, obs, set ^ 1, list, replay_ms);
+            if (rc) return rc;
+        }
     }
+    if (k > 0) return drain_hitset(ctx, obs, (k - 1) & 1, list, replay_ms);
     return AB_OK;
 }
 
-static int fetch_hits(ab_ctx *ctx, long long *nhits, const ab_obs *obs = nullptr)
+static int fetch_hits(ab_ctx *ctx, long long *nhits)
 {
-    if (obs) {
-        SigmaConsts c{};
-        for (int i = 0; i < AB_MAX_STAGES; i++)
-            c.numindep[i] = i < obs->numharmstages ? (double) obs->numindep[i] : 1.0;
-        CK(ctx->sigs.ensure(ctx->hit_cap));
-        HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
-        CK(launch_sigma(hb, ctx->sigs.p, c, ctx->stream));
-        ctx->launches++;
-    }
     unsigned n = 0;
     CK(cudaMemcpyAsync(&n, ctx->count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -406,14 +525,21 @@ static int fetch_hits(ab_ctx *ctx, long long *nhits, const ab_obs *obs = nullptr
                            cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaMemcpyAsync(ctx->hpows.data(), ctx->pows.p, sizeof(float) * n, cudaMemcpyDeviceToHost,
                            ctx->stream));
-        if (obs) {
-            ctx->hsigs.resize(n);
-            CK(cudaMemcpyAsync(ctx->hsigs.data(), ctx->sigs.p, sizeof(float) * n,
-                               cudaMemcpyDeviceToHost, ctx->stream));
-        }
         CK(cudaStreamSynchronize(ctx->stream));
     }
     *nhits = n;
+    return AB_OK;
+}
+
+// Device-side failures that do not abort a kernel (a bounded wait that ran
+// out) are reported through the context's error word.
+static int check_device_error(ab_ctx *ctx)
+{
+    unsigned e = 0;
+    if (!ctx->errw.p) return AB_OK;
+    CK(cudaMemcpyAsync(&e, ctx->errw.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e) return fail(ctx, AB_ERR_CUDA, "device wait timed out (error word 0x%x)", e);
     return AB_OK;
 }
 
@@ -468,9 +594,19 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->dbg.release();
     ctx->tmpa.release();
     ctx->tmpb.release();
+    ctx->errw.release();
     ctx->keys.release();
     ctx->pows.release();
     ctx->count.release();
+    ctx->sigs.release();
+    ctx->keys2.release();
+    ctx->pows2.release();
+    ctx->count2.release();
+    ctx->sigs2.release();
+    if (ctx->hcount) cudaFreeHost(ctx->hcount);
+    for (int i = 0; i < 2; i++)
+        if (ctx->batch_done[i]) cudaEventDestroy(ctx->batch_done[i]);
+    if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
     for (auto e : ctx->evpool) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -515,6 +651,7 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
               long long *numcands)
 {
     if (!ctx || !obs || !fft) return fail(ctx, AB_ERR_ARG, "null argument");
+    const double t_start = now_ms();
     int rc = use_device(ctx);
     if (rc) return rc;
     rc = ensure_banks(ctx, obs);
@@ -527,31 +664,63 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
         if (rc) return rc;
         dfft = ctx->fft.p;
     }
-    rc = search_core(ctx, obs, dfft, first_block, max_blocks, -1);
-    if (rc) return rc;
-    long long nh = 0;
-    rc = fetch_hits(ctx, &nh, obs);
+    double replay_ms = 0.0;
+    ab_list *l = nullptr;
+    for (int attempt = 0;; attempt++) {
+        l = ab_list_new();
+        ctx->overflow_need = 0;
+        rc = search_core(ctx, obs, dfft, first_block, max_blocks, -1, l, &replay_ms);
+        if (!rc) rc = check_device_error(ctx);
+        if (rc == AB_ERR_OVERFLOW && ctx->overflow_need > ctx->hit_cap && attempt < 3) {
+            // a batch crossed the threshold more often than the hit buffer
+            // holds: grow it and search again
+            CK(cudaStreamSynchronize(ctx->stream));
+            unsigned want = ctx->hit_cap;
+            while (want < ctx->overflow_need + ctx->overflow_need / 4) want *= 2;
+            ctx->hit_cap = want;
+            ab_list_free(l);
+            continue;
+        }
+        break;
+    }
+    const double t_done = now_ms();
     harvest(ctx);
-    if (rc) return rc;
-    ab_list *l = ab_list_new();
-    long long nmain = ab_num_blocks(obs);
-    rc = ab_replay_hits(obs, ctx->hkeys.data(), ctx->hpows.data(), ctx->hsigs.data(), nh,
-                        ctx->hstart.data(), nmain, l);
+    if (ctx->prof) {
+        ctx->kms[4] += t_done - t_start - replay_ms;   // host wall time outside the replay
+        ctx->kms[5] += replay_ms;                      // sort + replay (overlaps the device)
+        ctx->kn[4]++; ctx->kn[5]++;
+    }
     if (rc) {
         ab_list_free(l);
-        return fail(ctx, rc, "hit replay failed");
+        return rc;
     }
-    long long n = ab_list_get(l, cands, maxcands);
+    long long n = ab_list_get(l, nullptr, 0);
+    ctx->last_cands.resize((size_t) n);
+    ab_list_get(l, ctx->last_cands.data(), n);
     ab_list_free(l);
+    if (cands)
+        for (long long i = 0; i < n && i < maxcands; i++) cands[i] = ctx->last_cands[i];
     if (numcands) *numcands = n;
     if (cands && n > maxcands) return fail(ctx, AB_ERR_OVERFLOW, "%lld candidates > maxcands", n);
     return AB_OK;
+}
+
+int ab_last_cands(ab_ctx *ctx, ab_cand *out, long long maxout, long long *numcands)
+{
+    if (!ctx) return AB_ERR_ARG;
+    long long n = (long long) ctx->last_cands.size();
+    if (out)
+        for (long long i = 0; i < n && i < maxout; i++) out[i] = ctx->last_cands[i];
+    if (numcands) *numcands = n;
+    return (out && n > maxout) ? AB_ERR_OVERFLOW : AB_OK;
 }
 
 int ab_last_hits(ab_ctx *ctx, long long *block, int *stage, int *wi, int *zi, int *ri, float *power,
                  long long maxhits, long long *numhits)
 {
     if (!ctx) return AB_ERR_ARG;
+    if (ctx->hits_truncated)
+        return fail(ctx, AB_ERR_STATE, "the last search kept only its latest batches of hits");
     long long n = (long long) ctx->hkeys.size();
     std::vector<size_t> order(n);
     for (long long i = 0; i < n; i++) order[i] = i;
@@ -587,13 +756,13 @@ int ab_block_stage_sums(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_h
     if (capacity < need) return fail(ctx, AB_ERR_OVERFLOW, "need %zu floats", need);
     rc = upload_spectrum(ctx, obs, fft_host);
     if (rc) return rc;
-    rc = search_core(ctx, obs, ctx->fft.p, block, 1, block);
+    rc = search_core(ctx, obs, ctx->fft.p, block, 1, block, nullptr);
+    if (!rc) rc = check_device_error(ctx);
     if (rc) return rc;
     CK(cudaMemcpyAsync(out, ctx->dbg.p, sizeof(float) * need, cudaMemcpyDeviceToHost, ctx->stream));
-    long long nh;
-    rc = fetch_hits(ctx, &nh);
+    CK(cudaStreamSynchronize(ctx->stream));
     harvest(ctx);
-    return rc;
+    return AB_OK;
 }
 
 int ab_set_spectrum(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host)
@@ -644,6 +813,9 @@ int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harm
         return fail(ctx, AB_ERR_OVERFLOW, "plane needs %zu floats", need);
     SearchConsts sc = make_consts(obs, ctx->bs);
     sc.inmem = 0;                              // the block plane, not the full plane
+    CK(ctx->errw.ensure(1));
+    CK(cudaMemsetAsync(ctx->errw.p, 0, sizeof(unsigned), ctx->stream));
+    sc.err = ctx->errw.p;
     CK(ctx->startr.ensure(1));
     CK(cudaMemcpyAsync(ctx->startr.p, &fullrlo, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(ctx->xhat.ensure((size_t) ctx->bs.xhat_per_block));
@@ -663,7 +835,7 @@ int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harm
                          cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     harvest(ctx);
-    return AB_OK;
+    return check_device_error(ctx);
 }
 
 int ab_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund, const ab_ffdotpows *sub,

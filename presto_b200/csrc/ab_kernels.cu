@@ -477,6 +477,9 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
 // ======================================================================
 // (b) correlation
 // ======================================================================
+// Correlation of one (block, bank) data spectrum with a tile of templates:
+// the data spectrum is staged in shared memory once, templates stream from
+// L2 (each template row is read by every block of the batch).
 template <int L>
 __global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
                                               const CorrItem *items, const float2 *xhat,
@@ -624,7 +627,10 @@ __global__ void __launch_bounds__(256) k_harmsum_std(const ab_bank *banks, Searc
                                                      float *dbg, int dbg_bi)
 {
     constexpr int NSUB = (1 << (STAGES - 1)) - 1;
-    __shared__ int s_row[NSUB > 0 ? NSUB : 1][HS_ZT];
+    constexpr int NS1 = NSUB > 0 ? NSUB : 1;
+    __shared__ const float *s_row[HS_ZT][NS1 + 1];      // [z][0] fundamental, [z][1+h] subharmonic h
+    __shared__ long long s_rlo[NS1];
+    __shared__ int s_zlo[NS1], s_wind[NS1];
     const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
     int x = blockIdx.x;
     const int zt = x % nzt;
@@ -638,46 +644,57 @@ __global__ void __launch_bounds__(256) k_harmsum_std(const ab_bank *banks, Searc
     const ab_hgeom g0 = ab_harm_geom(startr, lastr, 1, 1, sc.obs_zlo, sc.obs_wlo, sc.corr_uselen);
     const bool ok = r < g0.numrs;
     const float *pb = planes + (long long) bi * plane_per_block;
-    int rind[NSUB > 0 ? NSUB : 1];
-#pragma unroll
-    for (int h = 0; h < NSUB; h++) {
+    // per-bank plane geometry of this block, once per CTA
+    if (NSUB > 0 && threadIdx.x < NSUB) {
+        const int h = threadIdx.x;
         const ab_bank &bh = banks[h + 1];
         const ab_hgeom gh = ab_harm_geom(startr, lastr, bh.numharm, bh.harmnum, sc.obs_zlo,
                                          sc.obs_wlo, sc.corr_uselen);
-        int ri = ok ? ab_rind(startr, r, bh.f, gh.rlo) : 0;
-        rind[h] = min(max(ri, 0), bh.numrs_max - 1);
-        const int wind = min(max(ab_wind(g0.wlo, wi, bh.f, gh.wlo), 0), bh.nw - 1);
-        for (int zz = threadIdx.x; zz < HS_ZT; zz += blockDim.x) {
-            int z = z0 + zz;
-            int zi = (z < sc.numz) ? ab_zind(sc.obs_zlo, z, bh.f, gh.zlo) : 0;
-            zi = min(max(zi, 0), bh.nz - 1);
-            s_row[h][zz] = (int) (bh.plane_off + ((long long) wind * bh.nz + zi) * bh.numrs_max);
+        s_rlo[h] = gh.rlo;
+        s_zlo[h] = gh.zlo;
+        s_wind[h] = min(max(ab_wind(g0.wlo, wi, bh.f, gh.wlo), 0), bh.nw - 1);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (NSUB + 1) * HS_ZT; e += blockDim.x) {
+        const int h = e / HS_ZT - 1, zz = e % HS_ZT;
+        const int z = min(z0 + zz, sc.numz - 1);
+        if (h < 0) {
+            s_row[zz][0] = pb + banks[0].plane_off +
+                           ((long long) wi * sc.numz + z) * banks[0].numrs_max;
+        } else {
+            const ab_bank &bh = banks[h + 1];
+            int zi = min(max(ab_zind(sc.obs_zlo, z, bh.f, s_zlo[h]), 0), bh.nz - 1);
+            s_row[zz][h + 1] = pb + bh.plane_off + ((long long) s_wind[h] * bh.nz + zi) * bh.numrs_max;
         }
     }
+    // subharmonic r indices of this thread's cell (clamped, so every load is in bounds)
+    int rind[NS1];
+    const int rc = ok ? r : 0;
+#pragma unroll
+    for (int h = 0; h < NSUB; h++)
+        rind[h] = min(max(ab_rind(startr, rc, banks[h + 1].f, s_rlo[h]), 0), banks[h + 1].numrs_max - 1);
     __syncthreads();
     float pc[STAGES];
 #pragma unroll
-    for (int s = 0; s < STAGES; s++) pc[s] = sc.powcut[s];
-    const long long f_off = banks[0].plane_off + (long long) wi * sc.numz * banks[0].numrs_max;
-    const int f_stride = banks[0].numrs_max;
+    for (int s = 0; s < STAGES; s++) pc[s] = ok ? sc.powcut[s] : INFINITY;
     const long long block = bb.block0 + bi;
     const int zend = min(z0 + HS_ZT, sc.numz);
     const bool dump = dbg && bi == dbg_bi && ok;
     for (int z = z0; z < zend; z++) {
         const int zz = z - z0;
         float sums[STAGES];
-        float sum = ok ? pb[f_off + (long long) z * f_stride + r] : 0.f;
+        float sum = __ldg(s_row[zz][0] + rc);
         sums[0] = sum;
-        unsigned mask = (ok && !(sum <= pc[0])) ? 1u : 0u;
+        unsigned mask = (sum > pc[0] || sum != sum) ? 1u : 0u;
         int h = 0;
 #pragma unroll
         for (int s = 1; s < STAGES; s++) {
 #pragma unroll
-            for (int j = 0; j < (1 << (s - 1)); j++, h++)
-                if (ok) sum += pb[s_row[h][zz] + rind[h]];
+            for (int j = 0; j < (1 << (s - 1)); j++, h++) sum += __ldg(s_row[zz][h + 1] + rind[h]);
             sums[s] = sum;
-            if (ok && !(sum <= pc[s])) mask |= 1u << s;
+            if (sum > pc[s] || sum != sum) mask |= 1u << s;
         }
+        if (!ok) mask = 0u;
         flush_hits<STAGES>(mask, sums, block, wi, z, r, hb);
         if (dump) {
 #pragma unroll

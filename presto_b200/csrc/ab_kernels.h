@@ -17,6 +17,7 @@ struct SearchConsts {
     int corr_uselen, rstep, numz, numws, stages, inmem, nbanks;
     float nph;
     float powcut[AB_MAX_STAGES];
+    unsigned *err;             // device error word for bounded waits; may be null
 };
 
 // Blocks of one launch: global ordinal block0 + i, start frequency startr[i].
