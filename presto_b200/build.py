@@ -19,7 +19,8 @@ CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu"]
 C_SOURCES = ["ab_host.c"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
-CC_FLAGS = ["-O2", "-g", "-fPIC", "-std=c11", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
+CC_FLAGS = ["-O2", "-g", "-fPIC", "-std=gnu11", "-pthread", "-ffp-contract=off", "-Wall",
+            "-Wno-unused-function"]
 
 
 def _cc():
@@ -70,7 +71,7 @@ def build(force=False, verbose=False, ptxas_info=False):
         objs.append(o)
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), "-ccbin", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++",
-           "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lm"]
+           "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lm", "-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -201,11 +201,18 @@ __device__ __forceinline__ void apply_tw(float2 *x, const float2 *bs)
     }
 }
 
+template <int L, int S, int PASS>
+__device__ __forceinline__ void apply_tw_pass(float2 *x, int b, int t, const FftTw<L, S> &tw)
+{
+    if constexpr (PASS == 2) apply_tw<16>(x, tw.b2);
+    if constexpr (PASS == 3) apply_tw<FftShape<L>::R3>(x, tw.b3[b]);
+}
+
 // One Stockham pass.  v holds x[t + NT m]; results of a non-final pass go
 // through shared memory and come back in the same strided layout.
-// PASS: 1, 2 or 3 (selects the twiddle bases).
-template <int L, int R, int LS, int S, bool LAST, int PASS>
-__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const FftTw<L, S> &tw)
+// PASS: 1, 2 or 3 (selects the twiddles).  TW: FftTw (register bases).
+template <int L, int R, int LS, int S, bool LAST, int PASS, class TW>
+__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const TW &tw)
 {
     constexpr int NT = L / 16, NB = 16 / R;
 #pragma unroll
@@ -213,8 +220,7 @@ __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, con
         float2 x[R];
 #pragma unroll
         for (int q = 0; q < R; q++) x[q] = v[b + q * NB];
-        if constexpr (PASS == 2) apply_tw<R>(x, tw.b2);
-        if constexpr (PASS == 3) apply_tw<R>(x, tw.b3[b]);
+        if constexpr (PASS > 1) apply_tw_pass<L, S, PASS>(x, b, t, tw);
         dft<R, S>(x);
         if constexpr (LAST) {
 #pragma unroll
@@ -237,8 +243,8 @@ __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, con
 
 // Full transform of the group's data, in place in v.  Must be called by all
 // threads of the CTA (it contains __syncthreads).
-template <int L, int S>
-__device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const FftTw<L, S> &tw)
+template <int L, int S, class TW>
+__device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const TW &tw)
 {
     using SH = FftShape<L>;
     if constexpr (SH::R3 > 1) {

@@ -10,6 +10,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <unistd.h>
 
 #include "ab_host.h"
 #include "ab_index.h"
@@ -394,19 +396,25 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
 /* The reference keeps an r-ordered singly linked list and walks it from
  * the head for every threshold crossing.  Here the list is an array: the
  * walk's stopping node ("first node with r >= rr, else the last node") is
- * found by binary search while the array is ordered, and by the same
- * linear walk otherwise (the reference can place a new candidate before
- * a last node exactly 15 bins lower, which breaks the ordering). */
+ * found by a galloping binary search from the previous stop while the array
+ * is ordered, and by the same linear walk as the reference while it is not
+ * (replacing the second-to-last node with a higher r, or placing a new
+ * candidate before a last node exactly 15 bins lower, can put two adjacent
+ * nodes out of order).  ninv counts adjacent inversions exactly. */
 struct ab_list {
     ab_cand *c;
     long long n, cap;
-    int ordered;
+    long long ninv;                     /* adjacent pairs with r[i] > r[i+1] */
+    long long last;                     /* stop node of the previous insert */
+    double *seg;                        /* max-of-r segment tree (unordered walks) */
+    long long segsz;
+    int seg_dirty;
 };
 
 ab_list *ab_list_new(void)
 {
     ab_list *l = (ab_list *) calloc(1, sizeof(ab_list));
-    if (l) l->ordered = 1;
+    if (l) l->seg_dirty = 1;
     return l;
 }
 
@@ -414,7 +422,47 @@ void ab_list_free(ab_list *l)
 {
     if (!l) return;
     free(l->c);
+    free(l->seg);
     free(l);
+}
+
+/* Segment tree over the array positions holding max(r); answers "first
+ * position in [0, lim) with r >= rr" in O(log n) whatever the ordering. */
+static int seg_rebuild(ab_list *l)
+{
+    long long sz = 1;
+    while (sz < l->n) sz <<= 1;
+    if (sz != l->segsz || !l->seg) {
+        double *p = (double *) realloc(l->seg, sizeof(double) * 2 * (size_t) sz);
+        if (!p) return -1;
+        l->seg = p;
+        l->segsz = sz;
+    }
+    for (long long i = 0; i < sz; i++) l->seg[sz + i] = i < l->n ? l->c[i].r : -INFINITY;
+    for (long long i = sz - 1; i >= 1; i--)
+        l->seg[i] = l->seg[2 * i] > l->seg[2 * i + 1] ? l->seg[2 * i] : l->seg[2 * i + 1];
+    l->seg_dirty = 0;
+    return 0;
+}
+
+static void seg_set(ab_list *l, long long i)
+{
+    if (l->seg_dirty) return;
+    long long pos = l->segsz + i;
+    l->seg[pos] = l->c[i].r;
+    for (pos >>= 1; pos >= 1; pos >>= 1)
+        l->seg[pos] = l->seg[2 * pos] > l->seg[2 * pos + 1] ? l->seg[2 * pos] : l->seg[2 * pos + 1];
+}
+
+static long long seg_first_ge(const ab_list *l, long long node, long long lo, long long hi,
+                              long long lim, double rr)
+{
+    if (lo >= lim || l->seg[node] < rr) return -1;
+    if (hi - lo == 1) return lo;
+    long long mid = (lo + hi) / 2;
+    long long r = seg_first_ge(l, 2 * node, lo, mid, lim, rr);
+    if (r >= 0) return r;
+    return seg_first_ge(l, 2 * node + 1, mid, hi, lim, rr);
 }
 
 static int list_reserve(ab_list *l, long long want)
@@ -436,67 +484,111 @@ static void set_cand(ab_cand *c, float power, float sigma, int numharm, double r
     c->r = rr; c->z = zz; c->w = ww;
 }
 
-static void list_check_order(ab_list *l, long long i)
+static int inv_at(const ab_list *l, long long a)  /* pair (a, a+1) inverted? */
 {
-    if (i > 0 && l->c[i - 1].r > l->c[i].r) l->ordered = 0;
-    if (i + 1 < l->n && l->c[i].r > l->c[i + 1].r) l->ordered = 0;
+    return a >= 0 && a + 1 < l->n && l->c[a].r > l->c[a + 1].r;
+}
+
+static void replace_at(ab_list *l, long long i, float power, float sigma, int numharm,
+                       double rr, double zz, double ww)
+{
+    l->ninv -= inv_at(l, i - 1) + inv_at(l, i);
+    set_cand(&l->c[i], power, sigma, numharm, rr, zz, ww);
+    l->ninv += inv_at(l, i - 1) + inv_at(l, i);
+    seg_set(l, i);
+}
+
+static void insert_at(ab_list *l, long long at, float power, float sigma, int numharm,
+                      double rr, double zz, double ww)
+{
+    l->ninv -= inv_at(l, at - 1);
+    memmove(&l->c[at + 1], &l->c[at], sizeof(ab_cand) * (size_t) (l->n - at));
+    set_cand(&l->c[at], power, sigma, numharm, rr, zz, ww);
+    l->n++;
+    l->ninv += inv_at(l, at - 1) + inv_at(l, at);
+    l->seg_dirty = 1;
+}
+
+static void remove_at(ab_list *l, long long t)
+{
+    l->ninv -= inv_at(l, t - 1) + inv_at(l, t);
+    memmove(&l->c[t], &l->c[t + 1], sizeof(ab_cand) * (size_t) (l->n - t - 1));
+    l->n--;
+    l->ninv += inv_at(l, t - 1);
+    l->seg_dirty = 1;
+}
+
+/* first i in [0, n-1) with c[i].r >= rr, else n-1 (the reference's walk) */
+static long long find_stop(ab_list *l, double rr)
+{
+    const ab_cand *c = l->c;
+    const long long n1 = l->n - 1;
+    if (n1 <= 0) return 0;
+    if (l->ninv) {
+        if (l->seg_dirty && seg_rebuild(l)) {        /* no memory: plain walk */
+            long long t = 0;
+            while (t < n1 && c[t].r < rr) t++;
+            return t;
+        }
+        long long t = seg_first_ge(l, 1, 0, l->segsz, n1, rr);
+        return t < 0 ? n1 : t;
+    }
+    long long s0 = l->last < 0 ? 0 : (l->last >= n1 ? n1 - 1 : l->last);
+    long long lo, hi, step = 1;
+    if (c[s0].r >= rr) {
+        hi = s0;
+        while (hi - step >= 0 && c[hi - step].r >= rr) { hi -= step; step <<= 1; }
+        lo = hi - step < -1 ? -1 : hi - step;
+    } else {
+        lo = s0;
+        while (lo + step < n1 && c[lo + step].r < rr) { lo += step; step <<= 1; }
+        hi = lo + step > n1 ? n1 : lo + step;
+    }
+    while (hi - lo > 1) {
+        long long mid = lo + (hi - lo) / 2;
+        if (c[mid].r >= rr) hi = mid; else lo = mid;
+    }
+    l->last = hi;
+    return hi;
 }
 
 int ab_list_insert(ab_list *l, float power, float sigma, int numharm,
                    double rr, double zz, double ww)
 {
     if (list_reserve(l, l->n + 1)) return -1;
-    ab_cand *c = l->c;
     if (l->n == 0) {
-        set_cand(&c[0], power, sigma, numharm, rr, zz, ww);
+        set_cand(&l->c[0], power, sigma, numharm, rr, zz, ww);
         l->n = 1;
         return 1;
     }
-    long long t;                       /* the walk's stopping node */
-    if (l->ordered) {
-        long long lo = 0, hi = l->n - 1;          /* search [0, n-1) */
-        while (lo < hi) {
-            long long mid = (lo + hi) / 2;
-            if (c[mid].r < rr) lo = mid + 1; else hi = mid;
-        }
-        t = lo;
-    } else {
-        t = 0;
-        while (t < l->n - 1 && c[t].r < rr) t++;
-    }
+    long long t = find_stop(l, rr);
     long long p = t - 1;
+    ab_cand *c = l->c;
     int added = 0;
     double next_diff = fabs(rr - c[t].r);
     double prev_diff = p >= 0 ? fabs(rr - c[p].r) : AB_CLOSEST_R + 1.0;
     if (prev_diff < AB_CLOSEST_R) {
         if (c[p].sigma < sigma) {
-            set_cand(&c[p], power, sigma, numharm, rr, zz, ww);
-            list_check_order(l, p);
+            replace_at(l, p, power, sigma, numharm, rr, zz, ww);
             added = 1;
         }
         if (next_diff < AB_CLOSEST_R && c[t].sigma < sigma) {
             if (added) {              /* the new candidate already replaced prev */
-                memmove(&c[t], &c[t + 1], sizeof(ab_cand) * (size_t) (l->n - t - 1));
-                l->n--;
+                remove_at(l, t);
             } else {
-                set_cand(&c[t], power, sigma, numharm, rr, zz, ww);
-                list_check_order(l, t);
+                replace_at(l, t, power, sigma, numharm, rr, zz, ww);
                 added = 1;
             }
         }
     } else if (next_diff < AB_CLOSEST_R) {
         if (c[t].sigma < sigma) {
-            set_cand(&c[t], power, sigma, numharm, rr, zz, ww);
-            list_check_order(l, t);
+            replace_at(l, t, power, sigma, numharm, rr, zz, ww);
             added = 1;
         }
     } else {
         added = 1;
         long long at = (t == l->n - 1 && c[t].r < rr - AB_CLOSEST_R) ? l->n : t;
-        memmove(&c[at + 1], &c[at], sizeof(ab_cand) * (size_t) (l->n - at));
-        set_cand(&c[at], power, sigma, numharm, rr, zz, ww);
-        l->n++;
-        list_check_order(l, at);
+        insert_at(l, at, power, sigma, numharm, rr, zz, ww);
     }
     return added;
 }
@@ -508,58 +600,188 @@ long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout)
     return l->n;
 }
 
-/* LSD radix sort of (key, index) by the 62-bit key, 16 bits per pass. */
-static int radix_order(const unsigned long long *keys, long long n, unsigned *order)
+/* Parallel LSD radix sort of hit indices by key.  Keys are taken relative
+ * to the smallest block present, so a batch's keys fit in 48 bits: four
+ * passes of 12-bit digits, each pass a per-thread histogram, an exclusive
+ * scan over (digit, thread) and a stable scatter. */
+#define RS_BITS 12
+#define RS_BINS (1 << RS_BITS)
+#define RS_MAXT 16
+
+typedef struct {
+    const unsigned long long *k0;
+    unsigned long long *k1;
+    const unsigned long long *o0;       /* payload: power and sigma bits */
+    unsigned long long *o1;
+    size_t lo, hi;
+    int shift;
+    size_t *hist;                       /* [RS_BINS] of this thread */
+} rs_job;
+
+typedef struct {
+    rs_job job[RS_MAXT];
+    int nt, phase;
+    pthread_barrier_t bar;
+    size_t (*hist)[RS_BINS];
+    int npasses;
+    unsigned long long *ka, *kb;
+    unsigned long long *oa, *ob;
+    size_t n;
+} rs_ctx;
+
+typedef struct { rs_ctx *c; int id; } rs_arg;
+
+static void rs_count(rs_job *j)
 {
-    unsigned *tmp = (unsigned *) malloc(sizeof(unsigned) * (size_t) n);
-    unsigned long long *k0 = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
-    unsigned long long *k1 = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
-    size_t *cnt = (size_t *) malloc(sizeof(size_t) * 65536);
-    if (!tmp || !k0 || !k1 || !cnt) {
-        free(tmp); free(k0); free(k1); free(cnt);
+    memset(j->hist, 0, sizeof(size_t) * RS_BINS);
+    for (size_t i = j->lo; i < j->hi; i++) j->hist[(j->k0[i] >> j->shift) & (RS_BINS - 1)]++;
+}
+
+static void rs_scatter(rs_job *j)
+{
+    for (size_t i = j->lo; i < j->hi; i++) {
+        size_t pos = j->hist[(j->k0[i] >> j->shift) & (RS_BINS - 1)]++;
+        j->k1[pos] = j->k0[i];
+        j->o1[pos] = j->o0[i];
+    }
+}
+
+static void rs_scan(rs_ctx *c)
+{
+    size_t sum = 0;
+    for (int d = 0; d < RS_BINS; d++)
+        for (int t = 0; t < c->nt; t++) {
+            size_t v = c->hist[t][d];
+            c->hist[t][d] = sum;
+            sum += v;
+        }
+}
+
+static void rs_setup_pass(rs_ctx *c, int pass)
+{
+    unsigned long long *k0 = (pass & 1) ? c->kb : c->ka, *k1 = (pass & 1) ? c->ka : c->kb;
+    unsigned long long *o0 = (pass & 1) ? c->ob : c->oa, *o1 = (pass & 1) ? c->oa : c->ob;
+    for (int t = 0; t < c->nt; t++) {
+        rs_job *j = &c->job[t];
+        j->k0 = k0; j->k1 = k1; j->o0 = o0; j->o1 = o1;
+        j->shift = RS_BITS * pass;
+    }
+}
+
+static void *rs_worker(void *p)
+{
+    rs_arg *a = (rs_arg *) p;
+    rs_ctx *c = a->c;
+    for (int pass = 0; pass < c->npasses; pass++) {
+        if (a->id == 0) rs_setup_pass(c, pass);
+        pthread_barrier_wait(&c->bar);
+        rs_count(&c->job[a->id]);
+        pthread_barrier_wait(&c->bar);
+        if (a->id == 0) rs_scan(c);
+        pthread_barrier_wait(&c->bar);
+        rs_scatter(&c->job[a->id]);
+        pthread_barrier_wait(&c->bar);
+    }
+    return NULL;
+}
+
+/* Sorts keys[] (and the payload pl[] with it) in place by key. */
+static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long long n)
+{
+    unsigned long long kmin = ~0ull, kmax = 0;
+    for (long long i = 0; i < n; i++) {
+        if (keys[i] < kmin) kmin = keys[i];
+        if (keys[i] > kmax) kmax = keys[i];
+    }
+    int bits = 0;
+    while (bits < 64 && ((kmax - kmin) >> bits)) bits++;
+    int npasses = (bits + RS_BITS - 1) / RS_BITS;
+    if (npasses == 0) return AB_OK;
+    rs_ctx c;
+    memset(&c, 0, sizeof(c));
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    c.nt = n < (1 << 16) ? 1 : (int) (ncpu > RS_MAXT ? RS_MAXT : (ncpu < 1 ? 1 : ncpu));
+    c.n = (size_t) n;
+    c.npasses = npasses;
+    c.ka = keys;
+    c.oa = pl;
+    c.kb = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
+    c.ob = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
+    c.hist = malloc(sizeof(size_t) * RS_BINS * (size_t) c.nt);
+    if (!c.kb || !c.ob || !c.hist) {
+        free(c.kb); free(c.ob); free(c.hist);
         return AB_ERR_NOMEM;
     }
-    for (long long i = 0; i < n; i++) { order[i] = (unsigned) i; k0[i] = keys[i]; }
-    for (int pass = 0; pass < 4; pass++) {
-        int sh = 16 * pass;
-        memset(cnt, 0, sizeof(size_t) * 65536);
-        for (long long i = 0; i < n; i++) cnt[(k0[i] >> sh) & 0xFFFF]++;
-        size_t sum = 0;
-        for (int d = 0; d < 65536; d++) { size_t c = cnt[d]; cnt[d] = sum; sum += c; }
-        for (long long i = 0; i < n; i++) {
-            size_t pos = cnt[(k0[i] >> sh) & 0xFFFF]++;
-            k1[pos] = k0[i];
-            tmp[pos] = order[i];
-        }
-        unsigned long long *kt = k0; k0 = k1; k1 = kt;
-        memcpy(order, tmp, sizeof(unsigned) * (size_t) n);
+    for (long long i = 0; i < n; i++) keys[i] -= kmin;
+    for (int t = 0; t < c.nt; t++) {
+        c.job[t].lo = (size_t) n * t / c.nt;
+        c.job[t].hi = (size_t) n * (t + 1) / c.nt;
+        c.job[t].hist = c.hist[t];
     }
-    free(tmp); free(k0); free(k1); free(cnt);
+    if (c.nt == 1) {
+        for (int pass = 0; pass < npasses; pass++) {
+            rs_setup_pass(&c, pass);
+            rs_count(&c.job[0]);
+            rs_scan(&c);
+            rs_scatter(&c.job[0]);
+        }
+    } else {
+        pthread_t th[RS_MAXT];
+        rs_arg args[RS_MAXT];
+        pthread_barrier_init(&c.bar, NULL, (unsigned) c.nt);
+        for (int t = 1; t < c.nt; t++) {
+            args[t].c = &c; args[t].id = t;
+            pthread_create(&th[t], NULL, rs_worker, &args[t]);
+        }
+        args[0].c = &c; args[0].id = 0;
+        rs_worker(&args[0]);
+        for (int t = 1; t < c.nt; t++) pthread_join(th[t], NULL);
+        pthread_barrier_destroy(&c.bar);
+    }
+    if (npasses & 1) {
+        memcpy(keys, c.kb, sizeof(unsigned long long) * (size_t) n);
+        memcpy(pl, c.ob, sizeof(unsigned long long) * (size_t) n);
+    }
+    for (long long i = 0; i < n; i++) keys[i] += kmin;
+    free(c.kb); free(c.ob); free(c.hist);
     return AB_OK;
 }
 
 /* Device hits carry (key, power, sigma); the key orders them as the
- * reference visits them (block, stage, w, z, r).  Replays search_ffdotpows'
- * per-hit work (src/accel_utils.c:1430-1442).  sigs may be NULL, in which
- * case candidate_sigma is evaluated here. */
-int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows, const float *sigs,
+ * reference visits them (block, stage, w, z, r).  Sorts them (keys, pows and
+ * sigs are reordered in place) and replays search_ffdotpows' per-hit work
+ * (src/accel_utils.c:1430-1442).  sigs may be NULL, in which case
+ * candidate_sigma is evaluated here. */
+int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows, float *sigs,
                    long long nhits, const double *startr_tab, long long ntab, ab_list *l)
 {
     if (nhits <= 0) return AB_OK;
-    unsigned *order = (unsigned *) malloc(sizeof(unsigned) * (size_t) nhits);
-    if (!order) return AB_ERR_NOMEM;
-    int rc = radix_order(keys, nhits, order);
-    if (rc) { free(order); return rc; }
+    unsigned long long *pl = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) nhits);
+    if (!pl) return AB_ERR_NOMEM;
+    for (long long i = 0; i < nhits; i++) {
+        unsigned pb, sb = 0;
+        memcpy(&pb, &pows[i], 4);
+        if (sigs) memcpy(&sb, &sigs[i], 4);
+        pl[i] = ((unsigned long long) pb << 32) | sb;
+    }
+    int rc = radix_sort_kv(keys, pl, nhits);
+    if (rc) { free(pl); return rc; }
     long long cur_block = -1;
     ab_hgeom g = {0, 0, 0, 0};
     for (long long i = 0; i < nhits; i++) {
-        unsigned long long k = keys[order[i]];
+        unsigned long long k = keys[i];
+        unsigned pb = (unsigned) (pl[i] >> 32), sb = (unsigned) pl[i];
+        float pw, sg;
+        memcpy(&pw, &pb, 4);
+        memcpy(&sg, &sb, 4);
+        pows[i] = pw;
+        if (sigs) sigs[i] = sg;
         int ri = (int) (k & 0xFFFF); k >>= AB_KEY_RBITS;
         int zi = (int) (k & 0xFFF); k >>= AB_KEY_ZBITS;
         int wi = (int) (k & 0x7F); k >>= AB_KEY_WBITS;
         int stage = (int) (k & 0x7); k >>= AB_KEY_SBITS;
         long long block = (long long) k;
-        if (block >= ntab) { free(order); return AB_ERR_ARG; }
+        if (block >= ntab) { free(pl); return AB_ERR_ARG; }
         if (block != cur_block) {
             /* the fundamental plane of the block (src/accel_utils.c:1034-1039) */
             double startr = startr_tab[block];
@@ -568,15 +790,13 @@ int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows, con
             cur_block = block;
         }
         int numharm = 1 << stage;
-        float pw = pows[order[i]];
-        float sig = sigs ? sigs[order[i]]
-                         : (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
+        float sig = sigs ? sg : (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
         double rr = (g.rlo + ri * (double) AB_DR) / (double) numharm;
         double zz = (g.zlo + zi * (double) AB_DZ) / (double) numharm;
         double ww = (g.wlo + wi * (double) AB_DW) / (double) numharm;
-        if (ab_list_insert(l, pw, sig, numharm, rr, zz, ww) < 0) { free(order); return AB_ERR_NOMEM; }
+        if (ab_list_insert(l, pw, sig, numharm, rr, zz, ww) < 0) { free(pl); return AB_ERR_NOMEM; }
     }
-    free(order);
+    free(pl);
     return AB_OK;
 }
 

@@ -67,7 +67,7 @@ int       ab_list_insert(ab_list *l, float power, float sigma, int numharm,
                          double rr, double zz, double ww);
 long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout);
 int       ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows,
-                         const float *sigs, long long nhits, const double *startr_tab,
+                         float *sigs, long long nhits, const double *startr_tab,
                          long long ntab, ab_list *l);
 /* Start frequencies of the main-loop blocks, accumulated exactly as the
  * reference's driver does (startr += rstep). */

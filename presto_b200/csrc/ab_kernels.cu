@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts
     const int offset = 2 * b.hw0;
     const int numrs = g.numrs;
     const float invL2 = 1.0f / ((float) L * (float) L);
-    FftTw<L, 1> tw;
+    FftTw<L, 1> tw;                                     // twiddle bases in registers
     tw.init(t);
     __syncthreads();
     const int iters = (it.nt + SH::G - 1) / SH::G;
