@@ -184,6 +184,7 @@ def _cells_per_search(name):
 def run_ours(args):
     import torch
     import presto_b200 as pb
+    from presto_b200 import replicas
 
     rank, world, local = dist_env()
     dist = None
@@ -234,10 +235,7 @@ def run_ours(args):
     launches = ctx.launch_count() - launches0
     kms, kn = ctx.kernel_times()
     ctx.set_profiling(False)
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = replicas.max_over_ranks(ms, dist, device=f"cuda:{local}")
     total_cells = counts["cells"] * args.steps * world
     value = total_cells / (ms_max / 1e3)
 
@@ -255,10 +253,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device=f"cuda:{local}")
     nhits = len(ctx.last_hits()[0])
 
     # ---- roofline of the dominant kernel (correlation) ----
