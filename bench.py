@@ -323,6 +323,114 @@ def measured_fp32_peak(ctx):
     return v.value if rc == 0 else None
 
 
+class SpectrumCache:
+    """Seeded synthetic spectra by (N, injected) so a long request mix does not
+    spend minutes generating time series; the mix itself is seeded."""
+
+    def __init__(self, dt, seed):
+        self.dt, self.seed, self.cache = dt, seed, {}
+
+    def get(self, N, inject, rng):
+        key = (N, inject)
+        if key not in self.cache:
+            from presto_b200 import synth
+            ps = []
+            if inject:
+                T = N * self.dt
+                f = float(np.exp(rng.uniform(np.log(5.0), np.log(300.0))))
+                ps = [dict(r=f * T, z=float(rng.uniform(-200, 200)),
+                           harms=[(0.02, float(rng.uniform(0, 6.28))) for _ in range(8)])]
+            self.cache[key] = synth.spectrum(synth.time_series(N, self.seed + len(self.cache), ps))
+        return self.cache[key]
+
+
+def batched_requests(n, seed):
+    """cfg4 recipe: lengths uniform in {2^20..2^23}, zmax in {50, 200, 600},
+    numharm 8, wmax 0 (not given), 5 % with an injected 8-harmonic pulsar."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        N = int(1 << int(rng.integers(20, 24)))
+        out.append(dict(N=N, inject=bool(rng.random() < 0.05),
+                        opts=dict(zmax=int(rng.choice([50, 200, 600])), numharm=8)))
+    return out, rng
+
+
+def served_requests(n, seed, rate):
+    """cfg5 recipe: Poisson arrivals, N log-uniform in 2^19..2^23 (on a
+    half-octave grid), zmax in {0,100,300,600}, wmax in {0,0,0,200},
+    numharm in {4,8,16}, noise and injection as in the batched mix."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    for _ in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        N = int(round(2 ** (19 + 0.5 * int(rng.integers(0, 9))) / 2)) * 2
+        opts = dict(zmax=int(rng.choice([0, 100, 300, 600])), numharm=int(rng.choice([4, 8, 16])))
+        w = int(rng.choice([0, 0, 0, 200]))
+        if w:
+            opts["wmax"] = w
+        out.append(dict(t=t, N=N, inject=bool(rng.random() < 0.05), opts=opts))
+    return out, rng
+
+
+def run_pool_mode(args):
+    """--mode batched | served: the pool (ab_pool) against the plain
+    single-request path on the same requests and GPU."""
+    import presto_b200 as pb
+    from presto_b200 import serve
+    dt = 64e-6
+    if args.mode == "batched":
+        reqs, rng = batched_requests(args.requests, 4000)
+    else:
+        reqs, rng = served_requests(args.requests, 5000, args.rate)
+    cache = SpectrumCache(dt, 4100)
+    ffts = [cache.get(r["N"], r["inject"], rng) for r in reqs]
+    cells = 0
+    for r, f in zip(reqs, ffts):
+        o = pb.obs_init(pb.make_params(r["N"], dt, f.size, **r["opts"]))
+        cells += pb.algorithmic_counts(o)["cells"]
+    # plain single-request path: one context, one request at a time
+    ctx = pb.Context(0)
+    for r, f in zip(reqs[:3], ffts[:3]):                       # warm-up (templates)
+        ctx.search(pb.obs_init(pb.make_params(r["N"], dt, f.size, **r["opts"])), f)
+    t0 = time.perf_counter()
+    plain = [ctx.search(pb.obs_init(pb.make_params(r["N"], dt, f.size, **r["opts"])), f)
+             for r, f in zip(reqs, ffts)]
+    t_plain = time.perf_counter() - t0
+    ctx.close()
+    pool = serve.SearchPool(0, nworkers=args.workers)
+    for r, f in zip(reqs[:args.workers], ffts[:args.workers]):   # warm-up
+        pool.wait(pool.submit(f, r["N"], dt, **r["opts"]))
+    pool.reset_stats()
+    t0 = time.perf_counter()
+    tickets = []
+    for r, f in zip(reqs, ffts):
+        if args.mode == "served":
+            delay = r["t"] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+        tickets.append(pool.submit(f, r["N"], dt, **r["opts"]))
+    got = [pool.wait(t)[0] for t in tickets]
+    t_pool = time.perf_counter() - t0
+    st = pool.stats()
+    pool.close()
+    same = all(a == b for a, b in zip(got, plain))
+    line = {"metric": "DM-trial searches/s", "value": len(reqs) / t_pool, "unit": "searches/s",
+            "n_gpus": 1, "mode": args.mode, "requests": len(reqs), "workers": args.workers,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "plain_searches_per_s": len(reqs) / t_plain,
+            "speedup_vs_plain": t_plain / t_pool,
+            "cells_per_s": cells / t_pool, "plain_cells_per_s": cells / t_plain,
+            "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"]},
+            "results_identical_to_plain": same,
+            "config": {"recipe": "cfg4 (batched DM trials)" if args.mode == "batched"
+                       else f"cfg5 (Poisson arrivals at {args.rate}/s)",
+                       "spectra": "seeded synthetic, one noise and one injected spectrum "
+                                  "per length reused across requests"}}
+    print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,9 +442,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scratch-mb", type=int, default=0,
                     help="cap the engine's block scratch (profiling runs)")
+    ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
+                    help="batched/served: the request pool vs the plain path (one GPU)")
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--rate", type=float, default=20.0, help="served: arrivals per second")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.mode != "plain" and args.impl == "ours":
+        return run_pool_mode(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -202,6 +202,29 @@ int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnum, double f
                            float *d_powers, size_t powers_capacity, void *stream,
                            ab_ffdotpows *meta_out);
 
+/* Batched and served searches (no counterpart in the reference, whose
+ * accelsearch searches one spectrum per process: src/accelsearch.c:44-316).
+ * A pool of nworkers engine contexts on one device, each on its own host
+ * thread and stream.  Requests queue in arrival order; a free worker takes
+ * the head request once its device-memory footprint (in-memory plane plus
+ * spectrum, on top of every worker's fixed scratch) fits hbm_budget (0: 80 %
+ * of the free memory), so requests arriving while others run are admitted as
+ * workers and memory free up, and their kernels overlap on the GPU.  Each
+ * result equals ab_search of that request alone.  ab_pool_submit copies the
+ * spectrum (p->numbins bins); ab_pool_wait blocks for the result (out NULL:
+ * count only, the result is kept), then frees it; latency = submit to done. */
+typedef struct ab_pool ab_pool;
+int  ab_pool_create(int device, int nworkers, size_t hbm_budget, ab_pool **out);
+void ab_pool_destroy(ab_pool *pool);
+const char *ab_pool_last_error(const ab_pool *pool);
+int  ab_pool_submit(ab_pool *pool, const ab_params *p, const ab_fcomplex *fft, long long *ticket);
+int  ab_pool_wait(ab_pool *pool, long long ticket, ab_cand *out, long long maxout,
+                  long long *numcands, double *latency_ms);
+/* completed requests, p50/p99 latency (ms) and first start to last finish. */
+int  ab_pool_stats(ab_pool *pool, long long *completed, double *p50_ms, double *p99_ms,
+                   double *busy_ms);
+int  ab_pool_reset_stats(ab_pool *pool);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -29,7 +29,8 @@ EXPORTS = [
     "ab_equivalent_gaussian_sigma", "ab_sort_cands", "ab_eliminate_harmonics",
     "ab_ctx_set_profiling", "ab_ctx_kernel_times", "ab_ctx_reset_kernel_times",
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
-    "ab_fderivs_vol_noalloc",
+    "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
+    "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats",
 ]
 
 
@@ -130,6 +131,14 @@ def lib():
     L.ab_num_blocks_main.restype = ll
     L.ab_num_blocks_main.argtypes = [C.POINTER(Obs)]
     L.ab_measure_fp32_peak.argtypes = [vp, C.POINTER(d)]
+    L.ab_pool_create.argtypes = [i, i, C.c_size_t, C.POINTER(vp)]
+    L.ab_pool_destroy.argtypes = [vp]
+    L.ab_pool_last_error.restype = C.c_char_p
+    L.ab_pool_last_error.argtypes = [vp]
+    L.ab_pool_submit.argtypes = [vp, C.POINTER(Params), vp, C.POINTER(ll)]
+    L.ab_pool_wait.argtypes = [vp, ll, C.POINTER(Cand), ll, C.POINTER(ll), C.POINTER(d)]
+    L.ab_pool_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
+    L.ab_pool_reset_stats.argtypes = [vp]
     L.ab_fderivs_vol_noalloc.argtypes = [C.POINTER(Obs), i, i, d, vp, vp, vp, C.c_size_t, vp,
                                          C.POINTER(FFDotPows)]
     L.ab_ctx_launch_count.restype = ll

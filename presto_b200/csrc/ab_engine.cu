@@ -60,8 +60,16 @@ struct ab_ctx {
     // template banks
     ab_bankset bs{};
     bool have_banks = false;
-    int bank_inmem = -1;
-    DevBuf<float2> tmpl;
+    // template banks of recently used search geometries, least recently used
+    // evicted beyond kBankCache entries; tmpl points into the current one
+    struct BankEntry {
+        ab_bankset bs;
+        DevBuf<float2> tmpl;
+        unsigned long long used;
+    };
+    std::vector<BankEntry *> bank_cache;
+    unsigned long long bank_clock = 0;
+    float2 *tmpl_p = nullptr;
     DevBuf<ab_bank> dbanks;
     DevBuf<double2> tw64;
     DevBuf<float2> resp;
@@ -155,45 +163,70 @@ static void harvest(ab_ctx *ctx)
 }
 
 // ---- banks ----------------------------------------------------------------
+constexpr int kBankCache = 4;
+
+static bool same_templates(const ab_bankset &a, const ab_bankset &b)
+{
+    if (a.nbanks != b.nbanks) return false;
+    for (int i = 0; i < a.nbanks; i++) {
+        const ab_bank &x = a.b[i], &y = b.b[i];
+        if (x.numharm != y.numharm || x.harmnum != y.harmnum || x.zmax != y.zmax ||
+            x.wmax != y.wmax || x.L != y.L)
+            return false;
+    }
+    return true;
+}
+
+// Makes the template banks of obs current: from the cache when a search with
+// the same template geometry ran before, else generated on the device.
 static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
 {
     ab_bankset nb;
     int rc = ab_bankset_init(obs, &nb);
     if (rc) return fail(ctx, rc, "unsupported search geometry (FFT span above 4096 or "
                                  "circular wrap into valid cells)");
-    bool same = ctx->have_banks && nb.nbanks == ctx->bs.nbanks;
-    for (int i = 0; same && i < nb.nbanks; i++) {
-        const ab_bank &a = nb.b[i], &b = ctx->bs.b[i];
-        same = a.numharm == b.numharm && a.harmnum == b.harmnum && a.zmax == b.zmax &&
-               a.wmax == b.wmax && a.L == b.L;
-    }
-    if (same) {
-        // strides (numrs_max) may change with the spectrum length; templates do not
-        ctx->bs = nb;
-        CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks,
-                           cudaMemcpyHostToDevice, ctx->stream));
-        return AB_OK;
-    }
-    if (ctx->tw64.n == 0) {
-        CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
-        launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
-        CK(cudaGetLastError());
-    }
-    CK(ctx->tmpl.ensure((size_t) nb.tmpl_total));
     CK(ctx->dbanks.ensure(AB_MAX_BANKS));
-    CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks, cudaMemcpyHostToDevice,
-                       ctx->stream));
-    for (int i = 0; i < nb.nbanks; i++) {
-        tick(ctx, 0, true);
-        cudaError_t e = launch_templates(&nb.b[i], ctx->tmpl.p + nb.b[i].tmpl_off, nullptr,
-                                         ctx->tw64.p, kTwLog2, nullptr, 0, ctx->stream);
-        tick(ctx, 0, false);
-        ctx->launches++;
-        if (e != cudaSuccess)
-            return fail(ctx, AB_ERR_CUDA, "template generation failed: %s", cudaGetErrorString(e));
+    ab_ctx::BankEntry *hit = nullptr;
+    for (auto *e : ctx->bank_cache)
+        if (same_templates(e->bs, nb)) hit = e;
+    if (!hit) {
+        if (ctx->tw64.n == 0) {
+            CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
+            launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
+            CK(cudaGetLastError());
+        }
+        if ((int) ctx->bank_cache.size() >= kBankCache) {
+            auto lru = std::min_element(ctx->bank_cache.begin(), ctx->bank_cache.end(),
+                                        [](ab_ctx::BankEntry *x, ab_ctx::BankEntry *y) {
+                                            return x->used < y->used;
+                                        });
+            // the evicted buffer may still be read by queued kernels
+            CK(cudaStreamSynchronize(ctx->stream));
+            hit = *lru;
+        } else {
+            hit = new ab_ctx::BankEntry();
+            ctx->bank_cache.push_back(hit);
+        }
+        hit->bs.nbanks = 0;
+        CK(hit->tmpl.ensure((size_t) nb.tmpl_total));
+        for (int i = 0; i < nb.nbanks; i++) {
+            tick(ctx, 0, true);
+            cudaError_t e = launch_templates(&nb.b[i], hit->tmpl.p + nb.b[i].tmpl_off, nullptr,
+                                             ctx->tw64.p, kTwLog2, nullptr, 0, ctx->stream);
+            tick(ctx, 0, false);
+            ctx->launches++;
+            if (e != cudaSuccess)
+                return fail(ctx, AB_ERR_CUDA, "template generation failed: %s", cudaGetErrorString(e));
+        }
     }
+    // strides (numrs_max) follow the spectrum length; templates do not
+    hit->bs = nb;
+    hit->used = ++ctx->bank_clock;
+    ctx->tmpl_p = hit->tmpl.p;
     ctx->bs = nb;
     ctx->have_banks = true;
+    CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks, cudaMemcpyHostToDevice,
+                       ctx->stream));
     return AB_OK;
 }
 
@@ -258,7 +291,7 @@ static int run_corr(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
     for (int i = 0; i < p.nL; i++) {
         tick(ctx, 2, true);
         cudaError_t e = launch_corr(p.Ls[i], ctx->dbanks.p, sc, bb, ditems + p.off[i], p.cnt[i],
-                                    ctx->xhat.p, ctx->bs.xhat_per_block, ctx->tmpl.p, planes,
+                                    ctx->xhat.p, ctx->bs.xhat_per_block, ctx->tmpl_p, planes,
                                     ppb, fullplane, ctx->stream);
         tick(ctx, 2, false);
         ctx->launches++;
@@ -581,7 +614,11 @@ void ab_ctx_destroy(ab_ctx *ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    ctx->tmpl.release();
+    for (auto *e : ctx->bank_cache) {
+        e->tmpl.release();
+        delete e;
+    }
+    ctx->bank_cache.clear();
     ctx->dbanks.release();
     ctx->tw64.release();
     ctx->resp.release();
@@ -995,7 +1032,7 @@ int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int
     if (wi < 0 || wi >= b.nw || zi < 0 || zi >= b.nz) return fail(ctx, AB_ERR_ARG, "template index");
     if (!out) return AB_OK;
     if (maxlen < b.L) return fail(ctx, AB_ERR_OVERFLOW, "need %d", b.L);
-    CK(cudaMemcpyAsync(out, ctx->tmpl.p + b.tmpl_off + (long long) (wi * b.nz + zi) * b.L,
+    CK(cudaMemcpyAsync(out, ctx->tmpl_p + b.tmpl_off + (long long) (wi * b.nz + zi) * b.L,
                        sizeof(float2) * b.L, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     harvest(ctx);

@@ -366,11 +366,12 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
         if (npre > 0 && obs->corr_uselen > nrmax) nrmax = obs->corr_uselen;
         if (nrmax == 0) nrmax = obs->corr_uselen;
         b->numrs_max = nrmax;
-        /* Valid cells use spread-data samples [0, 4*hw0 + numrs - 1); the
-         * reference's circular FFT of fftlen_ref must not wrap into them,
-         * which makes any transform length >= that span equivalent. */
+        /* Valid cells read spread-data samples [0, 4*hw0 + numrs - 1).  The
+         * device transforms the reference's window extended periodically
+         * (period fftlen_ref), so any length >= that span gives the
+         * reference's circular correlation on the valid cells, including
+         * the cases where the reference's own FFT wraps into them. */
         int need = 4 * b->hw0 + nrmax - 1;
-        if (need > b->fftlen_ref) return AB_ERR_ARG;
         int L = (int) next_pow2(need);
         if (L < 512) L = 512;
         if (L > 4096) return AB_ERR_ARG;

@@ -411,9 +411,11 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
     }
     __syncthreads();
     const double norm = s_norm;
-    // spread data d[i] = norm * x[i] (i < numdata) at even samples; the
-    // L-point transform of the spread data is the L/2-point transform of d,
-    // repeated twice, so only that half is computed and stored.
+    // spread data d[i] = norm * x[i mod numdata] at even samples: the
+    // reference's window of numdata bins repeated with period fftlen_ref, so
+    // that a device transform longer than the reference's reproduces its
+    // circular correlation.  The L-point transform of the spread data is the
+    // L/2-point transform of d, repeated twice; only that half is computed.
     const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
     float2 *sm = fsm + grp * SH::SMEM;
     FftTw<LH, -1> tw;
@@ -421,9 +423,9 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
     float2 v[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-        int i = t + SH::NT * m;
+        const int i = (t + SH::NT * m) % numdata;
         float2 x = make_float2(0.f, 0.f);
-        if (i < numdata) {
+        {
             long long bin = lobin + i - sc.obs_lobin;
             if (bin >= 0 && bin < sc.numbins) {
                 float2 a = fft[bin];

@@ -279,3 +279,26 @@ def test_injected_signal_recovered(ctx, ablib):
     T = N * DT
     assert abs(best[3] * best[2] - 123.4 * T) < 1.0 or abs(best[3] - 123.4 * T) < 1.0
     assert abs(best[4] * best[2] - 40.0) <= 2.0 or abs(best[4] - 40.0) <= 2.0
+
+
+def test_wrapping_bank_matches_oracle(ctx, ablib, oracle):
+    """zmax=100, wmax=200, numharm=16: the reference's 192-point FFT for the
+    1/16 harmonic is one sample shorter than the span its valid cells read, so
+    its own circular correlation wraps; the device must reproduce that."""
+    N = 1 << 16
+    fft = _spec(N, 17, [dict(r=600.2, z=5.0, w=30.0, harms=[(0.1, 0.3)] * 4)])
+    kw = dict(zmax=100, wmax=200, numharm=16)
+    obs = ablib.obs_init(ablib.make_params(N, DT, fft.size, **kw))
+    oobs = oracle.obs_init(oracle.make_params(N, DT, fft.size, **kw))
+    geo = {(g["numharm"], g["harmnum"]): g for g in ablib.bank_geometry(obs)}
+    g = geo[(16, 1)]
+    assert 4 * g["hw"] + g["numrs_max"] - 1 > g["fftlen_ref"]      # the wrap is real
+    ctx.set_spectrum(obs, fft)
+    bank = oracle.Bank(oobs, 16, 1)
+    for b in (1, 7, 20):
+        lo = obs.rlo + b * obs.rstep
+        meta, dev = ctx.subharm_fderivs_vol(obs, 16, 1, lo, lo + obs.rstep - 0.5)
+        ometa, orc, _, _ = oracle.subharm_fderivs_vol(oobs, fft, 16, 1, lo, lo + obs.rstep - 0.5, bank)
+        assert meta == ometa
+        ok, worst = _close(dev, orc)
+        assert ok, (b, worst)
