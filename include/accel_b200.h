@@ -225,6 +225,13 @@ int  ab_pool_stats(ab_pool *pool, long long *completed, double *p50_ms, double *
                    double *busy_ms);
 int  ab_pool_reset_stats(ab_pool *pool);
 
+/* Tensor-core self-test (no counterpart in the reference): C[128][N] =
+ * A[128][K] . B[N][K]^T through tcgen05 BF16 MMAs with FP32 accumulation in
+ * tensor memory, operands split into hi + lo BF16 parts when split != 0 (the
+ * arithmetic of the split-precision correlation).  Host arrays; K % 16 == 0,
+ * K <= 256, N % 16 == 0, 16 <= N <= 256. */
+int ab_tc_gemm(ab_ctx *ctx, const float *A, const float *B, float *C, int N, int K, int split);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -30,7 +30,7 @@ EXPORTS = [
     "ab_ctx_set_profiling", "ab_ctx_kernel_times", "ab_ctx_reset_kernel_times",
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
     "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
-    "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats",
+    "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats", "ab_tc_gemm",
 ]
 
 
@@ -131,6 +131,7 @@ def lib():
     L.ab_num_blocks_main.restype = ll
     L.ab_num_blocks_main.argtypes = [C.POINTER(Obs)]
     L.ab_measure_fp32_peak.argtypes = [vp, C.POINTER(d)]
+    L.ab_tc_gemm.argtypes = [vp, vp, vp, vp, i, i, i]
     L.ab_pool_create.argtypes = [i, i, C.c_size_t, C.POINTER(vp)]
     L.ab_pool_destroy.argtypes = [vp]
     L.ab_pool_last_error.restype = C.c_char_p

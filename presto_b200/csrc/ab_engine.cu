@@ -1069,6 +1069,29 @@ int ab_ctx_reset_kernel_times(ab_ctx *ctx)
 
 long long ab_ctx_launch_count(ab_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
+int ab_tc_gemm(ab_ctx *ctx, const float *A, const float *B, float *C, int N, int K, int split)
+{
+    if (!ctx || !A || !B || !C) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    DevBuf<float> a, b, c;
+    CK(a.ensure((size_t) 128 * K));
+    CK(b.ensure((size_t) N * K));
+    CK(c.ensure((size_t) 128 * N));
+    CK(ctx->errw.ensure(1));
+    CK(cudaMemsetAsync(ctx->errw.p, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemcpyAsync(a.p, A, sizeof(float) * 128 * K, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.p, B, sizeof(float) * N * K, cudaMemcpyHostToDevice, ctx->stream));
+    cudaError_t e = launch_tc_gemm(a.p, b.p, c.p, N, K, split, ctx->errw.p, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, AB_ERR_ARG, "tc gemm: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(C, c.p, sizeof(float) * 128 * N, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    a.release();
+    b.release();
+    c.release();
+    return check_device_error(ctx);
+}
+
 int ab_measure_fp32_peak(ab_ctx *ctx, double *tflops)
 {
     if (!ctx || !tflops) return AB_ERR_ARG;

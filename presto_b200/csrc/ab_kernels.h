@@ -84,5 +84,7 @@ cudaError_t launch_threshold(const float *pw, int numws, int numzs, int numrs, f
                              int stage, HitBuf hb, cudaStream_t st);
 
 cudaError_t launch_fma_peak(float *out, int iters, int sms, cudaStream_t st);
+cudaError_t launch_tc_gemm(const float *A, const float *B, float *C, int N, int K, int split,
+                           unsigned *err, cudaStream_t st);
 
 }  // namespace ab
