@@ -102,6 +102,19 @@ const char *ab_ctx_last_error(const ab_ctx *ctx);
 void *ab_ctx_stream(ab_ctx *ctx);                 /* cudaStream_t of the context */
 int  ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes);
 
+/* Correlation path of the context's searches and drop-ins (replaces the
+ * FFTW multiply / inverse transform of subharm_fderivs_vol,
+ * src/accel_utils.c:1140-1193, by one of two device evaluations):
+ *   AB_CORR_FFT            FP32 radix-16 FFTs fused with the template
+ *                          multiply and power (default);
+ *   AB_CORR_TC_SPLIT_BF16  the banded template product as a complex
+ *                          contraction on the tensor cores, operands split
+ *                          into BF16 hi + lo parts, FP32 accumulation.
+ * The reference has no counterpart (it has one path). */
+#define AB_CORR_FFT            0
+#define AB_CORR_TC_SPLIT_BF16  1
+int  ab_ctx_set_corr_path(ab_ctx *ctx, int path);
+
 /* Geometry + thresholds (create_accelobs).  Host only. */
 int ab_obs_init(const ab_params *p, ab_obs *obs);
 

@@ -31,7 +31,12 @@ EXPORTS = [
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
     "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
     "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats", "ab_tc_gemm",
+    "ab_ctx_set_corr_path",
 ]
+
+# correlation paths (ab_ctx_set_corr_path)
+CORR_FFT = 0
+CORR_TC_SPLIT_BF16 = 1
 
 
 class AccelError(RuntimeError):
@@ -92,6 +97,7 @@ def lib():
     L.ab_ctx_stream.restype = vp
     L.ab_ctx_stream.argtypes = [vp]
     L.ab_ctx_set_hbm_budget.argtypes = [vp, C.c_size_t]
+    L.ab_ctx_set_corr_path.argtypes = [vp, i]
     L.ab_obs_init.argtypes = [C.POINTER(Params), C.POINTER(Obs)]
     L.ab_prepare.argtypes = [vp, C.POINTER(Obs)]
     L.ab_search.argtypes = [vp, C.POINTER(Obs), vp, i, ll, ll, C.POINTER(Cand), ll,
@@ -364,6 +370,11 @@ class Context:
         self._check(self.L.ab_bank_kernel(self.ptr, C.byref(obs), numharm, harmnum, wi, zi,
                                           out.ctypes.data, L.value, C.byref(L)), "ab_bank_kernel")
         return out
+
+    def set_corr_path(self, path):
+        """CORR_FFT (FP32 FFT correlation, default) or CORR_TC_SPLIT_BF16
+        (tensor-core banded contraction, split BF16 operands)."""
+        self._check(self.L.ab_ctx_set_corr_path(self.ptr, int(path)), "ab_ctx_set_corr_path")
 
     # ---- timing -------------------------------------------------------------
     def set_profiling(self, on):

@@ -62,11 +62,27 @@ struct ab_ctx {
     bool have_banks = false;
     // template banks of recently used search geometries, least recently used
     // evicted beyond kBankCache entries; tmpl points into the current one
+    // operands of the tensor-core correlation for one bank set: templates
+    // sorted by half-width into tiles, packed split-BF16 taps per tile
+    struct TcBank {
+        bool ready = false;
+        std::vector<TcTile> tiles;          // bank-major
+        std::vector<int> tile_lo;           // first tile of each bank, nbanks + 1 entries
+        DevBuf<TcTile> dtiles;
+        DevBuf<int> dperm;
+        DevBuf<unsigned char> pack;
+        int nks_max = 0;
+    };
     struct BankEntry {
         ab_bankset bs;
         DevBuf<float2> tmpl;
         unsigned long long used;
+        TcBank tc;
     };
+    BankEntry *cur_bank = nullptr;
+    int corr_path = AB_CORR_FFT;            // correlation path of searches and drop-ins
+    DevBuf<float2> dtime;                   // normalised block data (tensor-core path)
+    DevBuf<TcItem> titems;
     std::vector<BankEntry *> bank_cache;
     unsigned long long bank_clock = 0;
     float2 *tmpl_p = nullptr;
@@ -208,6 +224,7 @@ static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
             ctx->bank_cache.push_back(hit);
         }
         hit->bs.nbanks = 0;
+        hit->tc.ready = false;
         CK(hit->tmpl.ensure((size_t) nb.tmpl_total));
         for (int i = 0; i < nb.nbanks; i++) {
             tick(ctx, 0, true);
@@ -223,6 +240,7 @@ static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
     hit->bs = nb;
     hit->used = ++ctx->bank_clock;
     ctx->tmpl_p = hit->tmpl.p;
+    ctx->cur_bank = hit;
     ctx->bs = nb;
     ctx->have_banks = true;
     CK(cudaMemcpyAsync(ctx->dbanks.p, nb.b, sizeof(ab_bank) * nb.nbanks, cudaMemcpyHostToDevice,
@@ -311,6 +329,133 @@ static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
     ctx->launches += bank_hi - bank_lo;
     if (e != cudaSuccess)
         return fail(ctx, AB_ERR_CUDA, "prep launch failed: %s", cudaGetErrorString(e));
+    return AB_OK;
+}
+
+// ---- tensor-core correlation ---------------------------------------------
+// Tiles of the current bank set: per bank, templates sorted by half-width
+// (widest first, then by index) in groups of TC_TILE_T, each covering the taps
+// [hw0 - hwmax, hw0 + hwmax) of its widest member rounded out to 8; then the
+// raw responses and the packed split-BF16 operand, built once per bank set.
+static int ensure_tc(ab_ctx *ctx)
+{
+    ab_ctx::TcBank &tb = ctx->cur_bank->tc;
+    if (tb.ready) return AB_OK;
+    const ab_bankset &bs = ctx->bs;
+    tb.tiles.clear();
+    tb.tile_lo.assign(1, 0);
+    std::vector<int> perm;
+    long long off = 0;
+    int nks_max = 0, stride_max = 0;
+    for (int k = 0; k < bs.nbanks; k++) {
+        const ab_bank &b = bs.b[k];
+        std::vector<int> hw(b.ntmpl), order(b.ntmpl);
+        for (int t = 0; t < b.ntmpl; t++) {
+            int wi = t / b.nz, zi = t - wi * b.nz;
+            hw[t] = ab_w_resp_halfwidth((double) (-b.zmax + zi * AB_DZ), (double) (-b.wmax + wi * AB_DW));
+            order[t] = t;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return hw[x] > hw[y]; });
+        const int pbase = (int) perm.size();
+        perm.insert(perm.end(), order.begin(), order.end());
+        for (int i0 = 0; i0 < b.ntmpl; i0 += TC_TILE_T) {
+            TcTile t{};
+            t.bank = k;
+            t.t0 = pbase + i0;
+            t.nt = std::min(TC_TILE_T, b.ntmpl - i0);
+            t.n = (2 * t.nt + 15) / 16 * 16;
+            const int hwmax = hw[order[i0]];
+            t.c_lo = (b.hw0 - hwmax) / 8 * 8;
+            const int c_hi = (b.hw0 + hwmax + 7) / 8 * 8;
+            t.nks = (c_hi - t.c_lo) / 8;
+            t.off = off;
+            off += 2LL * t.nks * 64 * t.n;
+            nks_max = std::max(nks_max, t.nks);
+            tb.tiles.push_back(t);
+        }
+        tb.tile_lo.push_back((int) tb.tiles.size());
+        stride_max = std::max(stride_max, 4 * b.hw0);
+    }
+    if (tc_corr_smem(nks_max) > 227 * 1024)
+        return fail(ctx, AB_ERR_ARG, "template responses too wide for the tensor-core path");
+    CK(tb.dtiles.ensure(tb.tiles.size()));
+    CK(tb.dperm.ensure(perm.size()));
+    CK(tb.pack.ensure((size_t) off));
+    CK(cudaMemcpyAsync(tb.dtiles.p, tb.tiles.data(), sizeof(TcTile) * tb.tiles.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(tb.dperm.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    DevBuf<float2> raw;
+    int ntmax = 0;
+    for (int k = 0; k < bs.nbanks; k++) ntmax = std::max(ntmax, bs.b[k].ntmpl);
+    CK(raw.ensure((size_t) ntmax * stride_max));
+    int rc = AB_OK;
+    for (int k = 0; k < bs.nbanks && rc == AB_OK; k++) {
+        const ab_bank &b = bs.b[k];
+        const int lo = tb.tile_lo[k], nt = tb.tile_lo[k + 1] - lo;
+        int nks_k = 0;
+        for (int i = lo; i < lo + nt; i++) nks_k = std::max(nks_k, tb.tiles[i].nks);
+        tick(ctx, 0, true);
+        cudaError_t e = launch_tc_raw(&b, 4 * b.hw0, raw.p, ctx->tw64.p, kTwLog2, ctx->stream);
+        if (e == cudaSuccess)
+            e = launch_tc_pack(&b, tb.dtiles.p + lo, nt, nks_k, tb.dperm.p, raw.p, 4 * b.hw0,
+                               tb.pack.p, ctx->stream);
+        tick(ctx, 0, false);
+        ctx->launches += 2;
+        if (e != cudaSuccess)
+            rc = fail(ctx, AB_ERR_CUDA, "tensor-core operand packing failed: %s", cudaGetErrorString(e));
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    raw.release();
+    if (rc) return rc;
+    if (e != cudaSuccess)
+        return fail(ctx, AB_ERR_CUDA, "tensor-core operand packing failed: %s", cudaGetErrorString(e));
+    tb.nks_max = nks_max;
+    tb.ready = true;
+    return AB_OK;
+}
+
+// Work items of one batch of nblk blocks over banks [bank_lo, bank_hi):
+// longest tiles first; the blocks of one (tile, parity, positions) are
+// adjacent so that they share the tile's operand in L2.
+static void build_tc_plan(const ab_ctx::TcBank &tb, const ab_bankset &bs, int nblk, int bank_lo,
+                          int bank_hi, std::vector<TcItem> &items)
+{
+    items.clear();
+    std::vector<int> order;
+    for (int i = tb.tile_lo[bank_lo]; i < tb.tile_lo[bank_hi]; i++) order.push_back(i);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return tb.tiles[x].nks > tb.tiles[y].nks; });
+    for (int i : order) {
+        const ab_bank &b = bs.b[tb.tiles[i].bank];
+        for (int p = 0; p < 2; p++) {
+            const int na = (b.numrs_max - p + 1) / 2;
+            for (int a0 = 0; a0 < na; a0 += 2 * TC_ATILE)
+                for (int bi = 0; bi < nblk; bi++) items.push_back(TcItem{bi, i, p, a0});
+        }
+    }
+}
+
+// Normalised data and tensor-core correlation of one batch.
+static int run_tc(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                  int bank_lo, int bank_hi, const TcItem *ditems, int nitems, float *planes,
+                  long long ppb, float *fullplane)
+{
+    const ab_ctx::TcBank &tb = ctx->cur_bank->tc;
+    tick(ctx, 1, true);
+    cudaError_t e = launch_prep_time(ctx->dbanks.p + bank_lo, ctx->bs.b + bank_lo, bank_hi - bank_lo,
+                                     sc, bb, fft, ctx->dtime.p, ctx->bs.dtime_per_block, ctx->stream);
+    tick(ctx, 1, false);
+    ctx->launches++;
+    if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "data preparation failed: %s", cudaGetErrorString(e));
+    tick(ctx, 2, true);
+    e = launch_corr_tc(ctx->dbanks.p, sc, bb, ditems, nitems, tb.dtiles.p, tb.dperm.p, ctx->dtime.p,
+                       ctx->bs.dtime_per_block, tb.pack.p, tb.nks_max, planes, ppb, fullplane,
+                       ctx->stream);
+    tick(ctx, 2, false);
+    ctx->launches++;
+    if (e != cudaSuccess)
+        return fail(ctx, AB_ERR_CUDA, "tensor-core correlation launch failed: %s", cudaGetErrorString(e));
     return AB_OK;
 }
 
@@ -450,12 +595,32 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         if (first_col > 0)
             CK(cudaMemset2DAsync(ctx->fullplane.p, sizeof(float) * sc.rlen, 0,
                                  sizeof(float) * first_col, sc.numz, ctx->stream));
-        CK(ctx->xhat.ensure((size_t) std::max<long long>(nall, 1) * bs.xhat_per_block));
+        const bool tcp = ctx->corr_path == AB_CORR_TC_SPLIT_BF16;
+        if (tcp) {
+            rc = ensure_tc(ctx);
+            if (rc) return rc;
+            CK(ctx->dtime.ensure((size_t) std::max<long long>(std::max(npre, nmain), 1) *
+                                 bs.dtime_per_block));
+        } else {
+            CK(ctx->xhat.ensure((size_t) std::max<long long>(nall, 1) * bs.xhat_per_block));
+        }
         CorrPlan plan;
+        std::vector<TcItem> tplan;
         for (int pass = 0; pass < 2; pass++) {
             long long nb = pass == 0 ? npre : nmain;
             if (nb == 0) continue;
             BlockBatch bb{ctx->startr.p + (pass == 0 ? nmain : 0), 0, (int) nb, pass == 0};
+            if (tcp) {
+                build_tc_plan(ctx->cur_bank->tc, bs, (int) nb, 0, 1, tplan);
+                CK(ctx->titems.ensure(tplan.size()));
+                CK(cudaMemcpyAsync(ctx->titems.p, tplan.data(), sizeof(TcItem) * tplan.size(),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+                rc = run_tc(ctx, sc, bb, dfft, 0, 1, ctx->titems.p, (int) tplan.size(), nullptr, 0,
+                            ctx->fullplane.p);
+                if (rc) return rc;
+                CK(cudaStreamSynchronize(ctx->stream));
+                continue;
+            }
             rc = run_prep(ctx, sc, bb, dfft, 0, 1);
             if (rc) return rc;
             build_corr_plan(bs, (int) nb, 0, 1, plan);
@@ -487,8 +652,13 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
 
     // standard mode: batches of blocks, each correlated for every bank, then
     // summed; hit sets alternate so the host replays batch k-1 meanwhile
+    const bool tcp = ctx->corr_path == AB_CORR_TC_SPLIT_BF16;
+    if (tcp) {
+        rc = ensure_tc(ctx);
+        if (rc) return rc;
+    }
     const size_t per_block = (size_t) bs.plane_per_block * sizeof(float) +
-                             (size_t) bs.xhat_per_block * sizeof(float2);
+                             (size_t) (tcp ? bs.dtime_per_block : bs.xhat_per_block) * sizeof(float2);
     long long B = (long long) (ctx->scratch_budget / std::max<size_t>(per_block, 1));
     if (B < 1) B = 1;
     if (B > 512) B = 512;
@@ -496,17 +666,30 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     if (count >= 8 && B > (count + 7) / 8) B = (count + 7) / 8;
     if (B > count) B = std::max<long long>(count, 1);
     CK(ctx->planes.ensure((size_t) B * bs.plane_per_block));
-    CK(ctx->xhat.ensure((size_t) B * bs.xhat_per_block));
     CorrPlan full, tail;
-    build_corr_plan(bs, (int) B, 0, bs.nbanks, full);
+    std::vector<TcItem> tfull, ttail;
     long long rem = count % B;
-    if (rem) build_corr_plan(bs, (int) rem, 0, bs.nbanks, tail);
-    CK(ctx->items.ensure(full.items.size() + tail.items.size()));
-    CK(cudaMemcpyAsync(ctx->items.p, full.items.data(), sizeof(CorrItem) * full.items.size(),
-                       cudaMemcpyHostToDevice, ctx->stream));
-    if (rem)
-        CK(cudaMemcpyAsync(ctx->items.p + full.items.size(), tail.items.data(),
-                           sizeof(CorrItem) * tail.items.size(), cudaMemcpyHostToDevice, ctx->stream));
+    if (tcp) {
+        CK(ctx->dtime.ensure((size_t) B * bs.dtime_per_block));
+        build_tc_plan(ctx->cur_bank->tc, bs, (int) B, 0, bs.nbanks, tfull);
+        if (rem) build_tc_plan(ctx->cur_bank->tc, bs, (int) rem, 0, bs.nbanks, ttail);
+        CK(ctx->titems.ensure(tfull.size() + ttail.size()));
+        CK(cudaMemcpyAsync(ctx->titems.p, tfull.data(), sizeof(TcItem) * tfull.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        if (rem)
+            CK(cudaMemcpyAsync(ctx->titems.p + tfull.size(), ttail.data(), sizeof(TcItem) * ttail.size(),
+                               cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        CK(ctx->xhat.ensure((size_t) B * bs.xhat_per_block));
+        build_corr_plan(bs, (int) B, 0, bs.nbanks, full);
+        if (rem) build_corr_plan(bs, (int) rem, 0, bs.nbanks, tail);
+        CK(ctx->items.ensure(full.items.size() + tail.items.size()));
+        CK(cudaMemcpyAsync(ctx->items.p, full.items.data(), sizeof(CorrItem) * full.items.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        if (rem)
+            CK(cudaMemcpyAsync(ctx->items.p + full.items.size(), tail.items.data(),
+                               sizeof(CorrItem) * tail.items.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
     int k = 0;
     for (long long b0 = first; b0 < first + count; b0 += B, k++) {
         int nb = (int) std::min<long long>(B, first + count - b0);
@@ -514,12 +697,20 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         HitSet h = hitset(ctx, set);
         CK(cudaMemsetAsync(h.count, 0, sizeof(unsigned), ctx->stream));
         BlockBatch bb{ctx->startr.p + b0, b0, nb, 0};
-        rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
-        if (rc) return rc;
-        const CorrPlan &p = (nb == B) ? full : tail;
-        const CorrItem *di = ctx->items.p + ((nb == B) ? 0 : full.items.size());
-        rc = run_corr(ctx, sc, bb, p, di, ctx->planes.p, bs.plane_per_block, nullptr);
-        if (rc) return rc;
+        if (tcp) {
+            const TcItem *di = ctx->titems.p + ((nb == B) ? 0 : tfull.size());
+            const int ni = (int) ((nb == B) ? tfull.size() : ttail.size());
+            rc = run_tc(ctx, sc, bb, dfft, 0, bs.nbanks, di, ni, ctx->planes.p, bs.plane_per_block,
+                        nullptr);
+            if (rc) return rc;
+        } else {
+            rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
+            if (rc) return rc;
+            const CorrPlan &p = (nb == B) ? full : tail;
+            const CorrItem *di = ctx->items.p + ((nb == B) ? 0 : full.items.size());
+            rc = run_corr(ctx, sc, bb, p, di, ctx->planes.p, bs.plane_per_block, nullptr);
+            if (rc) return rc;
+        }
         int dbi = (dbg_block >= b0 && dbg_block < b0 + nb) ? (int) (dbg_block - b0) : -1;
         HitBuf hb{h.keys, h.pows, h.count, ctx->hit_cap};
         tick(ctx, 3, true);
@@ -616,6 +807,9 @@ void ab_ctx_destroy(ab_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto *e : ctx->bank_cache) {
         e->tmpl.release();
+        e->tc.dtiles.release();
+        e->tc.dperm.release();
+        e->tc.pack.release();
         delete e;
     }
     ctx->bank_cache.clear();
@@ -632,6 +826,8 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->tmpa.release();
     ctx->tmpb.release();
     ctx->errw.release();
+    ctx->dtime.release();
+    ctx->titems.release();
     ctx->keys.release();
     ctx->pows.release();
     ctx->count.release();
@@ -652,6 +848,13 @@ void ab_ctx_destroy(ab_ctx *ctx)
 const char *ab_ctx_last_error(const ab_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
 void *ab_ctx_stream(ab_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+int ab_ctx_set_corr_path(ab_ctx *ctx, int path)
+{
+    if (!ctx || (path != AB_CORR_FFT && path != AB_CORR_TC_SPLIT_BF16)) return AB_ERR_ARG;
+    ctx->corr_path = path;
+    return AB_OK;
+}
 
 int ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes)
 {
@@ -855,18 +1058,32 @@ int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harm
     sc.err = ctx->errw.p;
     CK(ctx->startr.ensure(1));
     CK(cudaMemcpyAsync(ctx->startr.p, &fullrlo, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(ctx->xhat.ensure((size_t) ctx->bs.xhat_per_block));
     CK(ctx->planes.ensure((size_t) ctx->bs.plane_per_block));
     BlockBatch bb{ctx->startr.p, 0, 1, 0};
-    rc = run_prep(ctx, sc, bb, ctx->fft.p, k, k + 1);
-    if (rc) return rc;
-    CorrPlan plan;
-    build_corr_plan(ctx->bs, 1, k, k + 1, plan);
-    CK(ctx->items.ensure(plan.items.size()));
-    CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
-                       cudaMemcpyHostToDevice, ctx->stream));
-    rc = run_corr(ctx, sc, bb, plan, ctx->items.p, ctx->planes.p, ctx->bs.plane_per_block, nullptr);
-    if (rc) return rc;
+    if (ctx->corr_path == AB_CORR_TC_SPLIT_BF16) {
+        rc = ensure_tc(ctx);
+        if (rc) return rc;
+        CK(ctx->dtime.ensure((size_t) ctx->bs.dtime_per_block));
+        std::vector<TcItem> tplan;
+        build_tc_plan(ctx->cur_bank->tc, ctx->bs, 1, k, k + 1, tplan);
+        CK(ctx->titems.ensure(tplan.size()));
+        CK(cudaMemcpyAsync(ctx->titems.p, tplan.data(), sizeof(TcItem) * tplan.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        rc = run_tc(ctx, sc, bb, ctx->fft.p, k, k + 1, ctx->titems.p, (int) tplan.size(), ctx->planes.p,
+                    ctx->bs.plane_per_block, nullptr);
+        if (rc) return rc;
+    } else {
+        CK(ctx->xhat.ensure((size_t) ctx->bs.xhat_per_block));
+        rc = run_prep(ctx, sc, bb, ctx->fft.p, k, k + 1);
+        if (rc) return rc;
+        CorrPlan plan;
+        build_corr_plan(ctx->bs, 1, k, k + 1, plan);
+        CK(ctx->items.ensure(plan.items.size()));
+        CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        rc = run_corr(ctx, sc, bb, plan, ctx->items.p, ctx->planes.p, ctx->bs.plane_per_block, nullptr);
+        if (rc) return rc;
+    }
     CK(cudaMemcpy2DAsync(out->powers, sizeof(float) * g.numrs, ctx->planes.p + b.plane_off,
                          sizeof(float) * b.numrs_max, sizeof(float) * g.numrs, (size_t) b.nw * b.nz,
                          cudaMemcpyDeviceToHost, ctx->stream));

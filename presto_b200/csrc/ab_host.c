@@ -336,7 +336,7 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
                 pairs[n][0] = 1 << s; pairs[n][1] = h; n++;
             }
     long long nblocks = ab_num_blocks(obs), npre = ab_num_preblocks(obs);
-    long long tmpl = 0, plane = 0, xhat = 0;
+    long long tmpl = 0, plane = 0, xhat = 0, dtime = 0;
     for (int i = 0; i < n; i++) {
         ab_bank *b = &bs->b[i];
         b->numharm = pairs[i][0];
@@ -381,6 +381,8 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
         tmpl += (long long) b->ntmpl * L;
         b->xhat_off = xhat;
         xhat += L / 2;
+        b->dtime_off = dtime;
+        dtime += b->fftlen_ref / AB_NUMBETWEEN;
         b->plane_off = plane;
         plane += (long long) b->nw * b->nz * b->numrs_max;
     }
@@ -388,6 +390,7 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
     bs->tmpl_total = tmpl;
     bs->plane_per_block = plane;
     bs->xhat_per_block = xhat;
+    bs->dtime_per_block = dtime;
     return AB_OK;
 }
 

@@ -28,6 +28,8 @@ typedef struct {
     long long tmpl_off;           /* complex offset of the bank's templates */
     long long plane_off;          /* float offset inside one block's plane scratch */
     long long xhat_off;           /* complex offset inside one block's spectrum scratch */
+    long long dtime_off;          /* complex offset of the block's normalised data
+                                     (tensor-core correlation) */
 } ab_bank;
 
 typedef struct {
@@ -36,6 +38,7 @@ typedef struct {
     long long tmpl_total;         /* complex elements over all banks */
     long long plane_per_block;    /* floats of plane scratch per block */
     long long xhat_per_block;     /* complex elements of spectrum scratch per block */
+    long long dtime_per_block;    /* complex elements of normalised data per block */
 } ab_bankset;
 
 /* Template-bank geometry for obs, in the reference's harmonic order:

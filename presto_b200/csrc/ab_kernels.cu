@@ -183,7 +183,9 @@ __device__ void fft64_tab(double2 *x, int n, const double2 *tw, int nmax)
 }
 
 // One CTA per template.  mode 0: bank template (placed, FFT'd, FP32 into
-// out + t*L).  mode 1: raw response of numkern points into out.
+// out + t*L).  mode 1: raw response of numkern points into out.  mode 2:
+// raw response of bank template t (numkern = 4 halfwidth points) into
+// out + t*L, L being the row stride (taps of the tensor-core path).
 // Dynamic shared memory: (L + nfft_max) double2.
 struct TmplArgs {
     int mode, zmax, wmax, nz, L, t_base;
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(256) k_templates(TmplArgs a)
     int t = a.t_base + blockIdx.x;
     double z, w;
     int numbetween, numkern;
-    if (a.mode == 0) {
+    if (a.mode != 1) {
         int wi = t / a.nz, zi = t - wi * a.nz;
         z = -a.zmax + zi * AB_DZ;
         w = -a.wmax + wi * AB_DW;
@@ -212,18 +214,19 @@ __global__ void __launch_bounds__(256) k_templates(TmplArgs a)
         numbetween = a.numbetween;
         numkern = a.numkern1;
     }
-    const double roffset = (a.mode == 0) ? 0.0 : a.roffset;
-    if (a.mode == 0 && numkern > a.L) return;       // host validates; keeps stores in range
+    const double roffset = (a.mode == 1) ? a.roffset : 0.0;
+    if (a.mode != 1 && numkern > a.L) return;       // host validates; keeps stores in range
+    float2 *raw = (a.mode == 2) ? a.out + (size_t) t * a.L : a.out;
     const int L = a.L, half = numkern / 2;
     double2 *placed = dsm;              // [L]   (mode 0)
-    double2 *chirp = dsm + L;           // [nfft]
+    double2 *chirp = dsm + (a.mode == 0 ? L : 0);   // [nfft]
     if (a.mode == 0)
         for (int i = threadIdx.x; i < L; i += blockDim.x) placed[i] = make_double2(0.0, 0.0);
     if (fabs(w) < 1E-4) {
         for (int c = threadIdx.x; c < numkern; c += blockDim.x) {
             double2 v = z_resp_point(roffset, numbetween, z, numkern, c);
             if (a.mode == 0) placed[c >= half ? c - half : L - half + c] = v;
-            else a.out[c] = make_float2((float) v.x, (float) v.y);
+            else raw[c] = make_float2((float) v.x, (float) v.y);
         }
         __syncthreads();
     } else {
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(256) k_templates(TmplArgs a)
         for (int c = threadIdx.x; c < numkern; c += blockDim.x) {
             double2 v = chirp[first + c];
             if (a.mode == 0) placed[c >= half ? c - half : L - half + c] = v;
-            else a.out[c] = make_float2((float) v.x, (float) v.y);
+            else raw[c] = make_float2((float) v.x, (float) v.y);
         }
         __syncthreads();
     }
@@ -337,6 +340,42 @@ cudaError_t launch_response(double roffset, int numbetween, double z, double w, 
     return cudaGetLastError();
 }
 
+cudaError_t launch_tc_raw(const ab_bank *b, int stride, float2 *out, const double2 *tw_all,
+                          int max_log2, cudaStream_t st)
+{
+    int nfft_max = 0;
+    for (int wi = 0; wi < b->nw; wi++) {
+        double w = -b->wmax + wi * AB_DW;
+        for (int zi = 0; zi < b->nz; zi++) {
+            double z = -b->zmax + zi * AB_DZ;
+            int nk = 2 * AB_NUMBETWEEN * ab_resp_halfwidth(z, w);
+            if (nk > stride) return cudaErrorInvalidValue;
+            int n = chirp_len(z, w, nk, AB_NUMBETWEEN);
+            if (n > nfft_max) nfft_max = n;
+        }
+    }
+    if (nfft_max > (1 << max_log2)) return cudaErrorInvalidValue;
+    size_t smem = (size_t) (nfft_max > 0 ? nfft_max : 1) * sizeof(double2);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_templates, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    TmplArgs a{};
+    a.mode = 2;
+    a.zmax = b->zmax;
+    a.wmax = b->wmax;
+    a.nz = b->nz;
+    a.L = stride;
+    a.tw = tw_all;
+    a.nmax = 1 << max_log2;
+    a.out = out;
+    const int chunk = 65535;
+    for (int t0 = 0; t0 < b->ntmpl; t0 += chunk) {
+        a.t_base = t0;
+        int n = b->ntmpl - t0 < chunk ? b->ntmpl - t0 : chunk;
+        k_templates<<<n, 256, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 // ======================================================================
 // (b) spectrum preparation
 // ======================================================================
@@ -368,26 +407,19 @@ __device__ void bitonic_sort(float *a, int n2)
     }
 }
 
-template <int LH>
-__global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
-                                              const float2 *fft, float2 *xhat,
-                                              long long xhat_per_block)
+// Block normalisation 1/sqrt(median(|X|^2)/ln 2) of the numdata bins from
+// lobin (zero outside the spectrum), or 1/sqrt(nph) when nph is given
+// (src/accel_utils.c:1079-1099).  The median is taken over float POWER()
+// values without FMA, sorted exactly; even counts average the two central
+// values (GSL semantics).  pw: shared scratch of nextpow2(numdata) floats.
+// Called by every thread of the CTA.
+__device__ double block_norm(const SearchConsts &sc, long long lobin, int numdata, const float2 *fft,
+                             float *pw, double *s_norm)
 {
-    using SH = FftShape<LH>;
-    extern __shared__ float2 fsm[];
-    __shared__ double s_norm;
-    const int bank = blockIdx.x, bi = blockIdx.y;
-    const ab_bank b = banks[bank];
-    ab_hgeom g;
-    block_geom(sc, b, bb.startr[bi], &g);
-    const long long lobin = g.rlo - b.hw0;
-    const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
-
     if (sc.nph > 0.0f) {
-        if (threadIdx.x == 0) s_norm = 1.0 / sqrt((double) sc.nph);
+        if (threadIdx.x == 0) *s_norm = 1.0 / sqrt((double) sc.nph);
     } else {
         // block median of |X|^2 in float (POWER(), no FMA), src/accel_utils.c:1087-1099
-        float *pw = reinterpret_cast<float *>(fsm);
         int n2 = 1;
         while (n2 < numdata) n2 <<= 1;
         for (int i = threadIdx.x; i < n2; i += blockDim.x) {
@@ -406,11 +438,28 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
             if (numdata & 1) m = pw[numdata / 2];
             else m = 0.5 * ((double) pw[(numdata - 1) / 2] + (double) pw[numdata / 2]);
             float med = (float) m;
-            s_norm = 1.0 / sqrt((double) med / 0.69314718055994530942);
+            *s_norm = 1.0 / sqrt((double) med / 0.69314718055994530942);
         }
     }
     __syncthreads();
-    const double norm = s_norm;
+    return *s_norm;
+}
+
+template <int LH>
+__global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+                                              const float2 *fft, float2 *xhat,
+                                              long long xhat_per_block)
+{
+    using SH = FftShape<LH>;
+    extern __shared__ float2 fsm[];
+    __shared__ double s_norm;
+    const int bank = blockIdx.x, bi = blockIdx.y;
+    const ab_bank b = banks[bank];
+    ab_hgeom g;
+    block_geom(sc, b, bb.startr[bi], &g);
+    const long long lobin = g.rlo - b.hw0;
+    const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
+    const double norm = block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
     // spread data d[i] = norm * x[i mod numdata] at even samples: the
     // reference's window of numdata bins repeated with period fftlen_ref, so
     // that a device transform longer than the reference's reproduces its
@@ -473,6 +522,54 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
                 return cudaErrorInvalidValue;
         }
     }
+    return cudaGetLastError();
+}
+
+// Normalised block data for the tensor-core correlation: d[i] = norm *
+// X[lobin + i] for i < numdata = fftlen_ref / 2, zero outside the spectrum
+// (get_fourier_amplitudes, src/accel_utils.c:993-1022, and the normalisation
+// of :1079-1115).  The correlation reads it periodically (period numdata),
+// which is the reference's circular correlation over fftlen_ref.
+__global__ void __launch_bounds__(256) k_prep_time(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+                                                   const float2 *fft, float2 *dtime,
+                                                   long long dt_per_block)
+{
+    extern __shared__ float2 fsm[];
+    __shared__ double s_norm;
+    const int bank = blockIdx.x, bi = blockIdx.y;
+    const ab_bank b = banks[bank];
+    ab_hgeom g;
+    block_geom(sc, b, bb.startr[bi], &g);
+    const long long lobin = g.rlo - b.hw0;
+    const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
+    const double norm = block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
+    float2 *o = dtime + (long long) bi * dt_per_block + b.dtime_off;
+    for (int i = threadIdx.x; i < numdata; i += blockDim.x) {
+        long long bin = lobin + i - sc.obs_lobin;
+        float2 x = make_float2(0.f, 0.f);
+        if (bin >= 0 && bin < sc.numbins) {
+            float2 v = fft[bin];
+            x = make_float2((float) ((double) v.x * norm), (float) ((double) v.y * norm));
+        }
+        o[i] = x;
+    }
+}
+
+cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                             const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                             float2 *dtime, long long dt_per_block, cudaStream_t st)
+{
+    int n2max = 1;
+    for (int k = 0; k < nbanks; k++) {
+        int numdata = banks_host[k].fftlen_ref / AB_NUMBETWEEN, n2 = 1;
+        while (n2 < numdata) n2 <<= 1;
+        if (n2 > n2max) n2max = n2;
+    }
+    size_t smem = (size_t) n2max * sizeof(float);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_prep_time, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    dim3 grid(nbanks, bb.nblk);
+    k_prep_time<<<grid, 256, smem, st>>>(banks_dev, sc, bb, fft, dtime, dt_per_block);
     return cudaGetLastError();
 }
 

@@ -87,4 +87,36 @@ cudaError_t launch_fma_peak(float *out, int iters, int sms, cudaStream_t st);
 cudaError_t launch_tc_gemm(const float *A, const float *B, float *C, int N, int K, int split,
                            unsigned *err, cudaStream_t st);
 
+// kernel set (b'), tensor-core correlation: the banded template product as a
+// complex contraction in split BF16 (hi + lo) with FP32 accumulation.
+constexpr int TC_TILE_T = 128;          // templates per tile (MMA N = 2 per template)
+constexpr int TC_ATILE = 128;           // output positions per accumulator (MMA M)
+constexpr int TC_STAGES = 4;            // template K-step ring
+constexpr int TC_CHUNK = 64 * 2 * TC_TILE_T;   // bytes of one K step (hi + lo) at N = 256
+
+struct TcTile {                 // templates perm[t0 .. t0+nt) of one bank
+    int bank, t0, nt, n;        // n = MMA N = 2 nt rounded up to 16
+    int c_lo, nks;              // first tap (multiple of 8) and K steps of 8 taps
+    long long off;              // byte offset of the packed operand (parity 0;
+                                // parity 1 follows after nks * 64 n bytes)
+};
+struct TcItem {                 // one CTA: positions a0 .. a0+255 of one parity
+    int bi, tile, parity, a0;
+};
+
+cudaError_t launch_tc_raw(const ab_bank *b, int stride, float2 *out, const double2 *tw_all,
+                          int max_log2, cudaStream_t st);
+cudaError_t launch_tc_pack(const ab_bank *b, const TcTile *tiles_dev, int ntiles, int nks_max,
+                           const int *perm_dev, const float2 *raw, int stride,
+                           unsigned char *pack, cudaStream_t st);
+cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                             const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                             float2 *dtime, long long dt_per_block, cudaStream_t st);
+cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, const BlockBatch &bb,
+                           const TcItem *items, int nitems, const TcTile *tiles, const int *perm,
+                           const float2 *dtime, long long dt_per_block, const unsigned char *pack,
+                           int nks_max, float *planes, long long plane_per_block, float *fullplane,
+                           cudaStream_t st);
+size_t tc_corr_smem(int nks_max);
+
 }  // namespace ab

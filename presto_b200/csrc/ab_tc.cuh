@@ -80,6 +80,23 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Arrive on bar (count 1) announcing `bytes` of asynchronous transactions.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Contiguous global -> shared copy by the bulk-copy engine, completing
+// `bytes` of transactions on bar.  No multicast.  dst and src 16-byte
+// aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
+
 // Bounded wait on an mbarrier phase: false (and *err |= flag) if it did not
 // complete within ~2^22 polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned *err, unsigned flag)
