@@ -198,6 +198,9 @@ def run_ours(args):
     w = WORKLOADS[name]
     fft = make_spectrum(name, seed_offset=rank)
     ctx = pb.Context(local)
+    tc = args.corr == "tc"
+    if tc:
+        ctx.set_corr_path(pb.CORR_TC_SPLIT_BF16)
     if args.scratch_mb:
         ctx.L.ab_ctx_set_hbm_budget(ctx.ptr, int(args.scratch_mb) * 4 << 20)
     obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
@@ -258,8 +261,6 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel (correlation) ----
     corr_ms_per_search = kms[2] / args.steps
-    achieved = counts["corr_flops"] / (corr_ms_per_search / 1e3) / 1e12
-    fp32_peak = measured_fp32_peak(ctx)
     harm_ms = kms[3] / args.steps
     peaks = {}
     try:
@@ -267,16 +268,39 @@ def run_ours(args):
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
+    if tc:
+        # split-BF16 contraction, timed inside a long step: sustained BF16 peak
+        tflops = counts["tc_flops"] / (corr_ms_per_search / 1e3) / 1e12
+        bf16 = peaks.get("bf16_tflops_sustained")
+        src = "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
+        if bf16 is None:
+            bf16, src = 1400.0, "fallback sustained BF16 1.4 PFLOP/s (of fallback)"
+        roof = {"bound": "tensor", "kernel": "k_corr_tc (split-BF16 banded contraction)",
+                "achieved": tflops, "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16,
+                "traffic": None, "flops_per_search": counts["tc_flops"],
+                "kernel_ms_per_search": corr_ms_per_search, "peak_source": src}
+    else:
+        achieved = counts["corr_flops"] / (corr_ms_per_search / 1e3) / 1e12
+        fp32_peak = measured_fp32_peak(ctx)
+        roof = {"bound": "fp32", "kernel": "k_corr (template correlation)",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "flops_per_search": counts["corr_flops"],
+                "kernel_ms_per_search": corr_ms_per_search,
+                "peak_source": "measured in-run FP32 FMA loop (MEASURED_PEAKS.json "
+                               "holds no FP32 CUDA-core figure)"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 hi+lo products, f32 accumulate" if tc else "f32",
             "data": "synthetic",
             "config": {"workload": name, "desc": w["desc"], "N": w["N"], "zmax": w["zmax"],
                        "wmax": w["wmax"], "numharm": w["numharm"], "blocks": counts["blocks"],
                        "cells_per_search": counts["cells"],
+                       "corr": "tc_split_bf16" if tc else "fft_f32",
                        "l2": "256 MiB buffer written between timed steps",
                        "parallelism": f"replicas x{world} (independent spectra per GPU)"},
             "searches_per_s": value / counts["cells"],
@@ -286,13 +310,7 @@ def run_ours(args):
                     "h2d_bytes_per_step": int(fft.nbytes),
                     "d2h_bytes_per_step": int(4 + 12 * nhits),
                     "searches_per_s": args.steps * world / (e2e_ms / 1e3)},
-            "roofline": {"bound": "fp32", "kernel": "k_corr (template correlation)",
-                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak, "traffic": None,
-                         "flops_per_search": counts["corr_flops"],
-                         "kernel_ms_per_search": corr_ms_per_search,
-                         "peak_source": "measured in-run FP32 FMA loop (MEASURED_PEAKS.json "
-                                        "holds no FP32 CUDA-core figure)"},
+            "roofline": roof,
             "roofline_harmsum": {"bound": "hbm", "kernel": "k_harmsum (sum + search)",
                                  "achieved": counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9,
                                  "peak": hbm, "unit": "GB/s",
@@ -442,6 +460,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scratch-mb", type=int, default=0,
                     help="cap the engine's block scratch (profiling runs)")
+    ap.add_argument("--corr", choices=["fft", "tc"], default="fft",
+                    help="correlation path: FP32 FFTs, or the split-BF16 tensor-core contraction")
     ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
                     help="batched/served: the request pool vs the plain path (one GPU)")
     ap.add_argument("--requests", type=int, default=48)

@@ -252,6 +252,9 @@ double ab_chi2_logp(double chi2, double dof);
 double ab_equivalent_gaussian_sigma(double logp);
 int  ab_sort_cands(ab_cand *cands, long long n);
 long long ab_eliminate_harmonics(ab_cand *cands, long long n);
+/* Half-width in bins of the (z, w) response, w_resp_halfwidth with LOWACC
+ * (src/responses.c:49-84; z_resp_halfwidth :27-47 when w = 0). */
+int  ab_w_resp_halfwidth(double z, double w);
 
 /* Kernel timing (CUDA events around each launch on the context stream).
  * kinds: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search (device

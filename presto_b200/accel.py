@@ -31,7 +31,7 @@ EXPORTS = [
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
     "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
     "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats", "ab_tc_gemm",
-    "ab_ctx_set_corr_path",
+    "ab_ctx_set_corr_path", "ab_w_resp_halfwidth",
 ]
 
 # correlation paths (ab_ctx_set_corr_path)
@@ -98,6 +98,7 @@ def lib():
     L.ab_ctx_stream.argtypes = [vp]
     L.ab_ctx_set_hbm_budget.argtypes = [vp, C.c_size_t]
     L.ab_ctx_set_corr_path.argtypes = [vp, i]
+    L.ab_w_resp_halfwidth.argtypes = [C.c_double, C.c_double]
     L.ab_obs_init.argtypes = [C.POINTER(Params), C.POINTER(Obs)]
     L.ab_prepare.argtypes = [vp, C.POINTER(Obs)]
     L.ab_search.argtypes = [vp, C.POINTER(Obs), vp, i, ll, ll, C.POINTER(Cand), ll,
@@ -225,7 +226,17 @@ def algorithmic_counts(obs):
     flops *= nb
     sum_bytes = 4.0 * fund_cells * obs.numharmstages + 4.0 * fund_cells * (numharm - 1) + \
         8.0 * fund_cells * (obs.numharmstages - 1)
-    return dict(blocks=nb, cells=cells, corr_flops=flops, harmsum_bytes=sum_bytes)
+    # tensor-core path: 8 FLOPs per complex tap, numkern / 2 = 2 hw taps per
+    # output cell, 3 products (hi.hi, hi.lo, lo.hi), numrs_max cells per row
+    tc = 0.0
+    hwf = lib().ab_w_resp_halfwidth
+    for b in bank_geometry(obs):
+        zmax, wmax = b["nz"] - 1, (b["nw"] - 1) * 10
+        taps = sum(2 * hwf(float(-zmax + 2 * zi), float(-wmax + 20 * wi))
+                   for wi in range(b["nw"]) for zi in range(b["nz"]))
+        tc += 8.0 * 3.0 * taps * b["numrs_max"]
+    return dict(blocks=nb, cells=cells, corr_flops=flops, harmsum_bytes=sum_bytes,
+                tc_flops=tc * nb)
 
 
 class Context:
