@@ -119,8 +119,9 @@ int  ab_ctx_set_corr_path(ab_ctx *ctx, int path);
 int ab_obs_init(const ab_params *p, ab_obs *obs);
 
 /* Template-bank geometry of obs in the reference's harmonic order (host
- * only).  info[8*k ..] = numharm, harmnum, numkern_zdim, numkern_wdim,
- * reference fftlen, device FFT length, kernel half width, largest numrs. */
+ * only).  info[9*k ..] = numharm, harmnum, numkern_zdim, numkern_wdim,
+ * reference fftlen, device FFT length, kernel half width, largest numrs,
+ * blocks per device transform in the whole-spectrum search. */
 int ab_bank_geometry(const ab_obs *obs, int *nbanks, int *info, int maxbanks);
 
 /* Number of blocks of the main search loop (src/accelsearch.c:187-224). */

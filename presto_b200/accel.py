@@ -195,15 +195,16 @@ def num_blocks(obs):
 
 
 def bank_geometry(obs):
-    """Per template bank: dict(numharm, harmnum, nz, nw, fftlen_ref, L, hw, numrs_max)."""
+    """Per template bank: dict(numharm, harmnum, nz, nw, fftlen_ref, L, hw, numrs_max,
+    sbm = blocks per device transform in the whole-spectrum search)."""
     n = C.c_int()
     rc = lib().ab_bank_geometry(C.byref(obs), C.byref(n), None, 0)
     if rc:
         raise AccelError(f"ab_bank_geometry: {ERRORS.get(rc, rc)}")
-    info = (C.c_int * (8 * n.value))()
+    info = (C.c_int * (9 * n.value))()
     lib().ab_bank_geometry(C.byref(obs), C.byref(n), info, n.value)
-    keys = ("numharm", "harmnum", "nz", "nw", "fftlen_ref", "L", "hw", "numrs_max")
-    return [dict(zip(keys, info[8 * k:8 * k + 8])) for k in range(n.value)]
+    keys = ("numharm", "harmnum", "nz", "nw", "fftlen_ref", "L", "hw", "numrs_max", "sbm")
+    return [dict(zip(keys, info[9 * k:9 * k + 9])) for k in range(n.value)]
 
 
 def algorithmic_counts(obs):

@@ -95,6 +95,7 @@ struct ab_ctx {
     long long fft_bins = 0;
     bool fft_valid = false;
     DevBuf<float2> xhat;
+    DevBuf<double> norms;                    // [block][bank] of superblock banks
     DevBuf<float> planes;
     DevBuf<float> fullplane;
     DevBuf<double> startr;
@@ -279,7 +280,10 @@ struct CorrPlan {
     int nL = 0;
 };
 
-static void build_corr_plan(const ab_bankset &bs, int nblk, int bank_lo, int bank_hi, CorrPlan &p)
+// With sc.superblocks, a bank of superblock height m > 1 has one transform
+// unit per m consecutive blocks of the batch (CorrItem.bi is the unit).
+static void build_corr_plan(const ab_bankset &bs, const SearchConsts &sc, int nblk, int bank_lo,
+                            int bank_hi, CorrPlan &p)
 {
     p.items.clear();
     p.nL = 0;
@@ -289,8 +293,9 @@ static void build_corr_plan(const ab_bankset &bs, int nblk, int bank_lo, int ban
         for (int k = bank_lo; k < bank_hi; k++) {
             const ab_bank &b = bs.b[k];
             if (b.L != L) continue;
+            const int units = corr_units(b, sc, nblk);
             for (int t0 = 0; t0 < b.ntmpl; t0 += tile)
-                for (int bi = 0; bi < nblk; bi++)
+                for (int bi = 0; bi < units; bi++)
                     p.items.push_back(CorrItem{bi, k, t0, std::min(tile, b.ntmpl - t0)});
         }
         int n = (int) p.items.size() - start;
@@ -623,7 +628,7 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             }
             rc = run_prep(ctx, sc, bb, dfft, 0, 1);
             if (rc) return rc;
-            build_corr_plan(bs, (int) nb, 0, 1, plan);
+            build_corr_plan(bs, sc, (int) nb, 0, 1, plan);
             CK(ctx->items.ensure(plan.items.size()));
             CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
                                cudaMemcpyHostToDevice, ctx->stream));
@@ -681,8 +686,11 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
                                cudaMemcpyHostToDevice, ctx->stream));
     } else {
         CK(ctx->xhat.ensure((size_t) B * bs.xhat_per_block));
-        build_corr_plan(bs, (int) B, 0, bs.nbanks, full);
-        if (rem) build_corr_plan(bs, (int) rem, 0, bs.nbanks, tail);
+        sc.superblocks = 1;
+        CK(ctx->norms.ensure((size_t) B * bs.nbanks));
+        sc.norms = ctx->norms.p;
+        build_corr_plan(bs, sc, (int) B, 0, bs.nbanks, full);
+        if (rem) build_corr_plan(bs, sc, (int) rem, 0, bs.nbanks, tail);
         CK(ctx->items.ensure(full.items.size() + tail.items.size()));
         CK(cudaMemcpyAsync(ctx->items.p, full.items.data(), sizeof(CorrItem) * full.items.size(),
                            cudaMemcpyHostToDevice, ctx->stream));
@@ -704,6 +712,12 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
                         nullptr);
             if (rc) return rc;
         } else {
+            tick(ctx, 1, true);
+            cudaError_t en = launch_norms(ctx->dbanks.p, bs.b, bs.nbanks, sc, bb, dfft, ctx->stream);
+            tick(ctx, 1, false);
+            ctx->launches++;
+            if (en != cudaSuccess)
+                return fail(ctx, AB_ERR_CUDA, "normalisation launch failed: %s", cudaGetErrorString(en));
             rc = run_prep(ctx, sc, bb, dfft, 0, bs.nbanks);
             if (rc) return rc;
             const CorrPlan &p = (nb == B) ? full : tail;
@@ -828,6 +842,7 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->errw.release();
     ctx->dtime.release();
     ctx->titems.release();
+    ctx->norms.release();
     ctx->keys.release();
     ctx->pows.release();
     ctx->count.release();
@@ -1077,7 +1092,7 @@ int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harm
         rc = run_prep(ctx, sc, bb, ctx->fft.p, k, k + 1);
         if (rc) return rc;
         CorrPlan plan;
-        build_corr_plan(ctx->bs, 1, k, k + 1, plan);
+        build_corr_plan(ctx->bs, sc, 1, k, k + 1, plan);
         CK(ctx->items.ensure(plan.items.size()));
         CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
                            cudaMemcpyHostToDevice, ctx->stream));

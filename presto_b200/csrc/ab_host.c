@@ -324,7 +324,21 @@ static int calc_fftlen(int numharm, int harmnum, int zmax, int wmax, const ab_ob
     return ab_next_good_fftlen(bins_needed + end_effects);
 }
 
+/* Device transform cost per template and transform, by log2 L: the
+ * radix-16 work L log2 L unless measured costs are supplied. */
+static double transform_cost(const double *cost_by_log2L, int L)
+{
+    int lg = twon_to_index(L);
+    if (cost_by_log2L && lg < AB_COST_SLOTS && cost_by_log2L[lg] > 0.0) return cost_by_log2L[lg];
+    return (double) L * lg;
+}
+
 int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
+{
+    return ab_bankset_init_tuned(obs, NULL, bs);
+}
+
+int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_bankset *bs)
 {
     memset(bs, 0, sizeof(*bs));
     int pairs[AB_MAX_BANKS][2], n = 0;
@@ -357,15 +371,25 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
                 if (ab_w_resp_halfwidth(-b->zmax + zi * AB_DZ, -b->wmax + wi * AB_DW) > b->hw0)
                     return AB_ERR_ARG;
         int nrmax = 0;
+        long long *rlo = (long long *) malloc(sizeof(long long) * (size_t) (nblocks > 0 ? nblocks : 1));
+        int *nrs = (int *) malloc(sizeof(int) * (size_t) (nblocks > 0 ? nblocks : 1));
+        if (!rlo || !nrs) {
+            free(rlo);
+            free(nrs);
+            return AB_ERR_NOMEM;
+        }
         double startr = obs->rlo;
         for (long long k = 0; k < nblocks; k++, startr += obs->rstep) {
             ab_hgeom g = ab_harm_geom(startr, startr + obs->rstep - AB_DR, b->numharm,
                                       b->harmnum, obs->zlo, obs->wlo, obs->corr_uselen);
             if (g.numrs > nrmax) nrmax = g.numrs;
+            rlo[k] = g.rlo;
+            nrs[k] = g.numrs;
         }
         if (npre > 0 && obs->corr_uselen > nrmax) nrmax = obs->corr_uselen;
         if (nrmax == 0) nrmax = obs->corr_uselen;
         b->numrs_max = nrmax;
+        b->index = i;
         /* Valid cells read spread-data samples [0, 4*hw0 + numrs - 1).  The
          * device transforms the reference's window extended periodically
          * (period fftlen_ref), so any length >= that span gives the
@@ -374,7 +398,42 @@ int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
         int need = 4 * b->hw0 + nrmax - 1;
         int L = (int) next_pow2(need);
         if (L < 512) L = 512;
-        if (L > 4096) return AB_ERR_ARG;
+        if (L > 4096) {
+            free(rlo);
+            free(nrs);
+            return AB_ERR_ARG;
+        }
+        /* Superblocks (standard search only): when the reference's own
+         * transform does not wrap into valid cells, m consecutive blocks can
+         * share one device transform of length L2 over the first block's
+         * window, provided the widest span of m consecutive blocks'
+         * sub-planes, 2 (rlo_last - rlo_first) + numrs_last columns, plus the
+         * 4 hw0 - 1 samples of template reach fits in L2.  (L2, m) minimises
+         * the transform cost per block. */
+        int sbm = 1;
+        if (!obs->inmem && need <= b->fftlen_ref && nblocks > 1) {
+            double best = transform_cost(cost_by_log2L, L);
+            for (int m = 2; m <= AB_MAX_SBM && m <= nblocks; m++) {
+                long long span = 0;
+                for (long long k = 0; k + m - 1 < nblocks; k++) {
+                    long long sp = 2 * (rlo[k + m - 1] - rlo[k]) + nrs[k + m - 1];
+                    if (sp > span) span = sp;
+                }
+                long long need_m = 4LL * b->hw0 + span - 1;
+                for (int L2 = 512; L2 <= 4096; L2 <<= 1) {
+                    if (need_m > L2 || L2 < need) continue;
+                    double c = transform_cost(cost_by_log2L, L2) / m;
+                    if (c < best * 0.98) {
+                        best = c;
+                        L = L2;
+                        sbm = m;
+                    }
+                }
+            }
+        }
+        free(rlo);
+        free(nrs);
+        b->sbm = sbm;
         b->L = L;
         b->log2L = twon_to_index(L);
         b->tmpl_off = tmpl;
@@ -884,9 +943,10 @@ int ab_bank_geometry(const ab_obs *obs, int *nbanks, int *info, int maxbanks)
     if (maxbanks < bs.nbanks) return AB_ERR_OVERFLOW;
     for (int k = 0; k < bs.nbanks; k++) {
         const ab_bank *b = &bs.b[k];
-        int *o = info + 8 * k;
+        int *o = info + 9 * k;
         o[0] = b->numharm; o[1] = b->harmnum; o[2] = b->nz; o[3] = b->nw;
         o[4] = b->fftlen_ref; o[5] = b->L; o[6] = b->hw0; o[7] = b->numrs_max;
+        o[8] = b->sbm;
     }
     return AB_OK;
 }

@@ -30,7 +30,13 @@ typedef struct {
     long long xhat_off;           /* complex offset inside one block's spectrum scratch */
     long long dtime_off;          /* complex offset of the block's normalised data
                                      (tensor-core correlation) */
+    int sbm;                      /* blocks per device transform in the standard
+                                     search (superblock height, >= 1) */
+    int index;                    /* position in the bank set */
 } ab_bank;
+
+#define AB_MAX_SBM 8              /* superblock height limit */
+#define AB_COST_SLOTS 16          /* transform cost table entries (by log2 L) */
 
 typedef struct {
     int nbanks;
@@ -44,6 +50,10 @@ typedef struct {
 /* Template-bank geometry for obs, in the reference's harmonic order:
  * (1,1), (2,1), (4,1), (4,3), (8,1), ... (src/accel_utils.c:240-288). */
 int ab_bankset_init(const ab_obs *obs, ab_bankset *bs);
+/* The same with measured per-template transform costs by log2 L
+ * (AB_COST_SLOTS entries, <= 0 for unknown), which choose each bank's
+ * transform length and superblock height. */
+int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_bankset *bs);
 
 /* Number of blocks of the main loop (src/accelsearch.c:187-224) and of the
  * in-memory low-frequency pre-pass (src/accelsearch.c:166-183). */

@@ -453,13 +453,18 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
     using SH = FftShape<LH>;
     extern __shared__ float2 fsm[];
     __shared__ double s_norm;
-    const int bank = blockIdx.x, bi = blockIdx.y;
+    const int bank = blockIdx.x, bi = blockIdx.y;      // bi: transform unit
     const ab_bank b = banks[bank];
+    // superblock: the window of its first block, the normalisation of that
+    // block (computed by k_norms), the data unrepeated over L/2 bins
+    const bool sb = sc.superblocks && b.sbm > 1;
+    const int blk = sb ? bi * b.sbm : bi;
     ab_hgeom g;
-    block_geom(sc, b, bb.startr[bi], &g);
+    block_geom(sc, b, bb.startr[blk], &g);
     const long long lobin = g.rlo - b.hw0;
-    const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
-    const double norm = block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
+    const int numdata = sb ? LH : b.fftlen_ref / AB_NUMBETWEEN;
+    const double norm = sb ? sc.norms[(long long) blk * sc.nbanks + b.index]
+                           : block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
     // spread data d[i] = norm * x[i mod numdata] at even samples: the
     // reference's window of numdata bins repeated with period fftlen_ref, so
     // that a device transform longer than the reference's reproduces its
@@ -504,7 +509,7 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
         int LH = b.L / 2;
         size_t fftsm = (size_t) 256 * 16 * 17 / 16 * sizeof(float2);  // G * SMEM float2
         size_t smem = fftsm > (size_t) n2 * sizeof(float) ? fftsm : (size_t) n2 * sizeof(float);
-        dim3 grid(1, bb.nblk);
+        dim3 grid(1, corr_units(b, sc, bb.nblk));
         // launch a 1-bank grid by offsetting the bank pointer
         const ab_bank *bp = banks_dev + k;
         switch (LH) {
@@ -521,6 +526,42 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
             default:
                 return cudaErrorInvalidValue;
         }
+    }
+    return cudaGetLastError();
+}
+
+// Block normalisations of one superblock bank: sc.norms[block * nbanks +
+// bank index] = 1/sqrt(median/ln 2) over the block's own window of
+// fftlen_ref / 2 bins (src/accel_utils.c:1079-1099).
+__global__ void __launch_bounds__(256) k_norms(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+                                               const float2 *fft, double *norms)
+{
+    extern __shared__ float2 fsm[];
+    __shared__ double s_norm;
+    const ab_bank b = banks[blockIdx.x];
+    const int bi = blockIdx.y;
+    ab_hgeom g;
+    block_geom(sc, b, bb.startr[bi], &g);
+    const double n = block_norm(sc, g.rlo - b.hw0, b.fftlen_ref / AB_NUMBETWEEN, fft,
+                                reinterpret_cast<float *>(fsm), &s_norm);
+    if (threadIdx.x == 0) norms[(long long) bi * sc.nbanks + b.index] = n;
+}
+
+cudaError_t launch_norms(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                         const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                         cudaStream_t st)
+{
+    if (!sc.superblocks) return cudaSuccess;
+    cudaFuncSetAttribute(k_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    for (int k = 0; k < nbanks; k++) {
+        const ab_bank &b = banks_host[k];
+        if (b.sbm <= 1) continue;
+        int numdata = b.fftlen_ref / AB_NUMBETWEEN, n2 = 1;
+        while (n2 < numdata) n2 <<= 1;
+        size_t smem = (size_t) n2 * sizeof(float);
+        if (smem > 200 * 1024) return cudaErrorInvalidValue;
+        k_norms<<<dim3(1, bb.nblk), 256, smem, st>>>(banks_dev + k, sc, bb, fft,
+                                                       const_cast<double *>(sc.norms));
     }
     return cudaGetLastError();
 }
@@ -588,18 +629,51 @@ __global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts
 {
     using SH = FftShape<L>;
     extern __shared__ float2 fsm[];
+    __shared__ long long s_off[AB_MAX_SBM];
+    __shared__ float s_scale[AB_MAX_SBM];
+    __shared__ int s_c0[AB_MAX_SBM], s_lim[AB_MAX_SBM];
     float2 *xs = fsm;                                   // [L/2]
-    const CorrItem it = items[blockIdx.x];
+    const CorrItem it = items[blockIdx.x];              // it.bi: transform unit
     const ab_bank b = banks[it.bank];
     const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
     float2 *sm = fsm + L / 2 + grp * SH::SMEM;
+    // column -> block map of a superblock: low / high nibble = first / second
+    // block whose sub-plane holds the column (15 = none)
+    unsigned char *cmap = reinterpret_cast<unsigned char *>(fsm + L / 2 + SH::G * SH::SMEM);
     const float2 *xsrc = xhat + (long long) it.bi * xhat_per_block + b.xhat_off;
     for (int i = threadIdx.x; i < L / 2; i += blockDim.x) xs[i] = xsrc[i];
+    const bool sb = !sc.inmem && sc.superblocks && b.sbm > 1;
+    const int b0 = sb ? it.bi * b.sbm : it.bi;
     ab_hgeom g;
-    block_geom(sc, b, bb.startr[it.bi], &g);
+    block_geom(sc, b, bb.startr[b0], &g);
     const int offset = 2 * b.hw0;
     const int numrs = g.numrs;
     const float invL2 = 1.0f / ((float) L * (float) L);
+    if (sb) {
+        // superblock: block j's column kk is transform column 2 (rlo_j - rlo_0) + kk;
+        // its powers scale by (norm_j / norm_0)^2 (the transform used norm_0)
+        const int mb = min(b.sbm, bb.nblk - b0);
+        if ((int) threadIdx.x < mb) {
+            const int j = threadIdx.x;
+            ab_hgeom gj;
+            block_geom(sc, b, bb.startr[b0 + j], &gj);
+            const int c0 = (int) (2 * (gj.rlo - g.rlo));
+            s_c0[j] = c0;
+            s_lim[j] = max(0, min(gj.numrs, b.numrs_max));
+            s_off[j] = (long long) (b0 + j) * plane_per_block + b.plane_off - c0;
+            const double r = sc.norms[(long long) (b0 + j) * sc.nbanks + b.index] /
+                             sc.norms[(long long) b0 * sc.nbanks + b.index];
+            s_scale[j] = (float) (r * r);
+        }
+        __syncthreads();
+        for (int kk = threadIdx.x; kk < L; kk += blockDim.x) {
+            unsigned code = 0xFFu;
+            for (int j = 0; j < mb; j++)
+                if ((unsigned) (kk - s_c0[j]) < (unsigned) s_lim[j])
+                    code = ((code & 0x0Fu) == 0x0Fu) ? ((code & 0xF0u) | j) : ((code & 0x0Fu) | (j << 4));
+            cmap[kk] = (unsigned char) code;
+        }
+    }
     FftTw<L, 1> tw;                                     // twiddle bases in registers
     tw.init(t);
     __syncthreads();
@@ -620,7 +694,21 @@ __global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts
             for (int m = 0; m < 16; m++) v[m] = make_float2(0.f, 0.f);
         }
         fft_run<L, 1>(v, sm, t, tw);
-        if (valid) {
+        if (valid && sb) {
+            const long long row = (long long) tl * b.numrs_max;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int kk = t + SH::NT * m - offset;
+                if (kk >= 0) {
+                    const unsigned code = cmap[kk];
+                    const float pw = fmaf(v[m].x, v[m].x, v[m].y * v[m].y) * invL2;
+                    unsigned j = code & 0x0Fu;
+                    if (j < AB_MAX_SBM) planes[s_off[j] + row + kk] = pw * s_scale[j];
+                    j = code >> 4;
+                    if (j < AB_MAX_SBM) planes[s_off[j] + row + kk] = pw * s_scale[j];
+                }
+            }
+        } else if (valid) {
             float *out;
             long long lim = numrs;
             if (sc.inmem) {
@@ -652,7 +740,7 @@ cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
                         cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    size_t smem = (size_t) (L / 2 + 256 * 17) * sizeof(float2);
+    size_t smem = (size_t) (L / 2 + 256 * 17) * sizeof(float2) + (size_t) L;
     switch (L) {
 #define AB_CORR_CASE(N)                                                                       \
     case N:                                                                                   \
@@ -719,8 +807,12 @@ __device__ __forceinline__ void flush_hits(unsigned mask, const float *sums, lon
 // HS_RT r cells); each thread owns one r cell, keeps its subharmonic r
 // indices (rinds) in registers and walks the z rows.  Plane row offsets of
 // every subharmonic for the tile's rows are staged in shared memory.
+// Latency-bound gathers: the register cap keeps 6 / 4 / 3 CTAs per SM at
+// 3-4 / 5 / 6 stages.
+constexpr int harmsum_min_ctas(int stages) { return stages <= 2 ? 1 : stages <= 4 ? 6 : (stages == 5 ? 4 : 3); }
+
 template <int STAGES>
-__global__ void __launch_bounds__(256) k_harmsum_std(const ab_bank *banks, SearchConsts sc,
+__global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_std(const ab_bank *banks, SearchConsts sc,
                                                      BlockBatch bb, const float *planes,
                                                      long long plane_per_block, HitBuf hb,
                                                      float *dbg, int dbg_bi)
@@ -832,7 +924,7 @@ cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
 // In-memory mode: fundamental and subharmonic powers come from the full
 // f-fdot plane (inmem_add_ffdotpows).  CTA = (block, z tile, r cells).
 template <int STAGES>
-__global__ void __launch_bounds__(256) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
+__global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
                                                        const float *plane, HitBuf hb, float *dbg,
                                                        int dbg_bi)
 {

@@ -18,6 +18,8 @@ struct SearchConsts {
     float nph;
     float powcut[AB_MAX_STAGES];
     unsigned *err;             // device error word for bounded waits; may be null
+    int superblocks;           // standard search: banks with sbm > 1 share transforms
+    const double *norms;       // [block][bank] normalisations (superblock banks)
 };
 
 // Blocks of one launch: global ordinal block0 + i, start frequency startr[i].
@@ -56,6 +58,16 @@ cudaError_t launch_response(double roffset, int numbetween, double z, double w, 
 cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
                         const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
                         float2 *xhat, long long xhat_per_block, cudaStream_t st);
+// per-block normalisations of the superblock banks among banks_host[0..nbanks)
+// into sc.norms[block * sc.nbanks + bank index]
+cudaError_t launch_norms(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                         const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                         cudaStream_t st);
+// transform units (superblocks, or blocks) of a bank in a batch of nblk blocks
+inline int corr_units(const ab_bank &b, const SearchConsts &sc, int nblk)
+{
+    return (sc.superblocks && b.sbm > 1) ? (nblk + b.sbm - 1) / b.sbm : nblk;
+}
 cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
                         const BlockBatch &bb, const CorrItem *items, int nitems,
                         const float2 *xhat, long long xhat_per_block, const float2 *tmpl,
