@@ -115,6 +115,22 @@ int  ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes);
 #define AB_CORR_TC_SPLIT_BF16  1
 int  ab_ctx_set_corr_path(ab_ctx *ctx, int path);
 
+/* Transform schedule (no counterpart in the reference, whose FFT length per
+ * harmonic is calc_fftlen's, src/accel_utils.c:137-150).  The whole-spectrum
+ * search correlates each bank with a device FFT of length L (512..8192) that
+ * serves m consecutive blocks (1..8, only where the reference's own transform
+ * does not wrap); L and m minimise the correlation cost per block under a
+ * process-wide table of costs per template and transform, indexed by log2 L
+ * (AB_COST_SLOTS = 16 entries; a length whose entry is <= 0 is not used for
+ * superblocks).  The library starts with a table measured on B200 for 512 to
+ * 4096 points; ab_autotune re-measures those on the context's device and
+ * installs them (costs_out may be NULL).  Set the table before creating the
+ * banks a search, ab_bank_geometry or ab_fderivs_vol_noalloc rely on: the
+ * template length follows it. */
+int  ab_set_transform_costs(const double *costs, int n);
+int  ab_get_transform_costs(double *costs, int n);
+int  ab_autotune(ab_ctx *ctx, double *costs_out, int n);
+
 /* Geometry + thresholds (create_accelobs).  Host only. */
 int ab_obs_init(const ab_params *p, ab_obs *obs);
 
@@ -201,9 +217,9 @@ int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int
  * starts at fullrlo and ends at fullrlo + rstep - 0.5.  Work is queued on
  * `stream` (a cudaStream_t, NULL for the default stream) of the calling
  * thread's current device; the call does not wait for it.
- * The engine's intermediates live in one static device array of 160 KiB
+ * The engine's intermediates live in one static device array of 192 KiB
  * that every GPU loading the library keeps until exit, so the bank must need
- * at most 8192 correlation work items and a data spectrum of at most 2048
+ * at most 8192 correlation work items and a data spectrum of at most 4096
  * points; larger banks return AB_ERR_BUDGET (and a line on stderr).  The
  * array is shared by all calls and keeps the last call's contents; every
  * word a call reads is written earlier in the same call, so nothing needs

@@ -31,8 +31,11 @@ EXPORTS = [
     "ab_ctx_launch_count", "ab_bank_geometry", "ab_num_blocks_main", "ab_measure_fp32_peak",
     "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
     "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats", "ab_tc_gemm",
-    "ab_ctx_set_corr_path", "ab_w_resp_halfwidth",
+    "ab_ctx_set_corr_path", "ab_w_resp_halfwidth", "ab_set_transform_costs",
+    "ab_get_transform_costs", "ab_autotune",
 ]
+
+COST_SLOTS = 16
 
 # correlation paths (ab_ctx_set_corr_path)
 CORR_FFT = 0
@@ -99,6 +102,9 @@ def lib():
     L.ab_ctx_set_hbm_budget.argtypes = [vp, C.c_size_t]
     L.ab_ctx_set_corr_path.argtypes = [vp, i]
     L.ab_w_resp_halfwidth.argtypes = [C.c_double, C.c_double]
+    L.ab_set_transform_costs.argtypes = [C.POINTER(C.c_double), i]
+    L.ab_get_transform_costs.argtypes = [C.POINTER(C.c_double), i]
+    L.ab_autotune.argtypes = [vp, C.POINTER(C.c_double), i]
     L.ab_obs_init.argtypes = [C.POINTER(Params), C.POINTER(Obs)]
     L.ab_prepare.argtypes = [vp, C.POINTER(Obs)]
     L.ab_search.argtypes = [vp, C.POINTER(Obs), vp, i, ll, ll, C.POINTER(Cand), ll,
@@ -205,6 +211,22 @@ def bank_geometry(obs):
     lib().ab_bank_geometry(C.byref(obs), C.byref(n), info, n.value)
     keys = ("numharm", "harmnum", "nz", "nw", "fftlen_ref", "L", "hw", "numrs_max", "sbm")
     return [dict(zip(keys, info[9 * k:9 * k + 9])) for k in range(n.value)]
+
+
+def get_transform_costs():
+    """Correlation cost per template and transform (ms) by log2 L (0: unknown)."""
+    c = (C.c_double * COST_SLOTS)()
+    lib().ab_get_transform_costs(c, COST_SLOTS)
+    return list(c)
+
+
+def set_transform_costs(costs):
+    """Install a cost table (by log2 L); it chooses transform lengths and
+    superblock heights of banks built afterwards."""
+    c = (C.c_double * COST_SLOTS)(*[float(x) for x in list(costs)[:COST_SLOTS]])
+    rc = lib().ab_set_transform_costs(c, COST_SLOTS)
+    if rc:
+        raise AccelError(f"ab_set_transform_costs: {ERRORS.get(rc, rc)}")
 
 
 def algorithmic_counts(obs):
@@ -382,6 +404,13 @@ class Context:
         self._check(self.L.ab_bank_kernel(self.ptr, C.byref(obs), numharm, harmnum, wi, zi,
                                           out.ctypes.data, L.value, C.byref(L)), "ab_bank_kernel")
         return out
+
+    def autotune(self):
+        """Measure the correlation cost per transform length on this context's
+        device and install it process-wide; returns the table."""
+        c = (C.c_double * COST_SLOTS)()
+        self._check(self.L.ab_autotune(self.ptr, c, COST_SLOTS), "ab_autotune")
+        return list(c)
 
     def set_corr_path(self, path):
         """CORR_FFT (FP32 FFT correlation, default) or CORR_TC_SPLIT_BF16

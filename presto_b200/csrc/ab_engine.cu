@@ -287,9 +287,9 @@ static void build_corr_plan(const ab_bankset &bs, const SearchConsts &sc, int nb
 {
     p.items.clear();
     p.nL = 0;
-    for (int L = 512; L <= 4096; L <<= 1) {
+    for (int L = 512; L <= 8192; L <<= 1) {
         int start = (int) p.items.size();
-        const int G = 4096 / L, tile = 16 * G;
+        const int G = L >= 4096 ? 1 : 4096 / L, tile = 16 * G;
         for (int k = bank_lo; k < bank_hi; k++) {
             const ab_bank &b = bs.b[k];
             if (b.L != L) continue;
@@ -863,6 +863,99 @@ void ab_ctx_destroy(ab_ctx *ctx)
 const char *ab_ctx_last_error(const ab_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
 void *ab_ctx_stream(ab_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+// Correlation cost per template and transform at each device FFT length from
+// 512 to 4096: a fundamental-like bank of 128 templates (half-width L/16,
+// 3L/4 valid columns) over 148 blocks, k_corr timed with CUDA events (best of
+// 3 after a warm-up) on zeroed data.  The table replaces the process-wide one.
+int ab_autotune(ab_ctx *ctx, double *costs_out, int n)
+{
+    if (!ctx || n < 0) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    constexpr int kBlocks = 148, kTmpl = 128, kLmax = 4096;
+    DevBuf<float2> xhat, tmpl;
+    DevBuf<float> planes;
+    DevBuf<double> startr;
+    DevBuf<ab_bank> dbank;
+    DevBuf<CorrItem> items;
+    auto release = [&]() {
+        xhat.release();
+        tmpl.release();
+        planes.release();
+        startr.release();
+        dbank.release();
+        items.release();
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double costs[AB_COST_SLOTS] = {0};
+    cudaError_t e = cudaSuccess;
+    do {
+        if ((e = xhat.ensure((size_t) kBlocks * kLmax / 2)) != cudaSuccess) break;
+        if ((e = tmpl.ensure((size_t) kTmpl * kLmax)) != cudaSuccess) break;
+        if ((e = planes.ensure((size_t) kBlocks * kTmpl * (kLmax * 3 / 4))) != cudaSuccess) break;
+        if ((e = startr.ensure(kBlocks)) != cudaSuccess) break;
+        if ((e = dbank.ensure(1)) != cudaSuccess) break;
+        if ((e = items.ensure((size_t) kBlocks * kTmpl)) != cudaSuccess) break;
+        cudaMemsetAsync(xhat.p, 0, sizeof(float2) * xhat.n, ctx->stream);
+        cudaMemsetAsync(tmpl.p, 0, sizeof(float2) * tmpl.n, ctx->stream);
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int L = 512; L <= kLmax && e == cudaSuccess; L <<= 1) {
+            ab_bank b{};
+            b.numharm = b.harmnum = 1;
+            b.f = 1.0;
+            b.nz = b.ntmpl = kTmpl;
+            b.nw = 1;
+            b.fftlen_ref = L;
+            b.L = L;
+            b.hw0 = L / 16;
+            b.numrs_max = 3 * L / 4;
+            b.sbm = 1;
+            SearchConsts sc{};
+            sc.corr_uselen = b.numrs_max;
+            sc.rstep = b.numrs_max / 2;
+            sc.numz = kTmpl;
+            sc.numws = 1;
+            sc.nbanks = 1;
+            std::vector<double> st(kBlocks);
+            for (int k = 0; k < kBlocks; k++) st[k] = 1000.0 + (double) k * sc.rstep;
+            const int G = L >= 4096 ? 1 : 4096 / L, tile = 16 * G;
+            std::vector<CorrItem> it;
+            for (int t0 = 0; t0 < kTmpl; t0 += tile)
+                for (int bi = 0; bi < kBlocks; bi++) it.push_back(CorrItem{bi, 0, t0, tile});
+            cudaMemcpyAsync(dbank.p, &b, sizeof b, cudaMemcpyHostToDevice, ctx->stream);
+            cudaMemcpyAsync(startr.p, st.data(), sizeof(double) * kBlocks, cudaMemcpyHostToDevice,
+                            ctx->stream);
+            cudaMemcpyAsync(items.p, it.data(), sizeof(CorrItem) * it.size(), cudaMemcpyHostToDevice,
+                            ctx->stream);
+            BlockBatch bb{startr.p, 0, kBlocks, 0};
+            float best = 1e30f;
+            for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+                cudaEventRecord(e0, ctx->stream);
+                e = launch_corr(L, dbank.p, sc, bb, items.p, (int) it.size(), xhat.p, L / 2, tmpl.p,
+                                planes.p, (long long) kTmpl * b.numrs_max, nullptr, ctx->stream);
+                cudaEventRecord(e1, ctx->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0 && ms < best) best = ms;
+            }
+            int lg = 0;
+            while ((1 << lg) < L) lg++;
+            costs[lg] = (double) best / ((double) kBlocks * kTmpl);
+        }
+    } while (0);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaError_t es = cudaStreamSynchronize(ctx->stream);
+    release();
+    if (e == cudaSuccess) e = es;
+    if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "autotune failed: %s", cudaGetErrorString(e));
+    ab_set_transform_costs(costs, AB_COST_SLOTS);
+    for (int i = 0; i < n && costs_out; i++) costs_out[i] = i < AB_COST_SLOTS ? costs[i] : 0.0;
+    return AB_OK;
+}
 
 int ab_ctx_set_corr_path(ab_ctx *ctx, int path)
 {

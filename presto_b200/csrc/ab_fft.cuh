@@ -131,21 +131,25 @@ __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
 template <int L> struct FftShape {
     static constexpr int NT = L / 16;                 // threads per transform
-    static constexpr int G = 256 / NT;                // transforms per 256-thread CTA
-    static constexpr int R3 = L / 256;                // radix of the third pass (1: none)
+    static constexpr int CTA = NT > 256 ? NT : 256;   // threads per CTA
+    static constexpr int G = CTA / NT;                // transforms per CTA
+    static constexpr int R3 = L <= 4096 ? L / 256 : 16;   // radix of the third pass (1: none)
+    static constexpr int R4 = L > 4096 ? L / 4096 : 1;    // radix of the fourth pass (1: none)
     static constexpr int NB3 = (R3 > 1) ? 16 / R3 : 0;
+    static constexpr int NB4 = (R4 > 1) ? 16 / R4 : 0;
     static constexpr int SMEM = L + L / 16;           // padded float2 per transform
-    static_assert(L >= 256 && L <= 4096 && (L & (L - 1)) == 0, "FFT length");
+    static_assert(L >= 256 && L <= 8192 && (L & (L - 1)) == 0, "FFT length");
 };
 
-// Per-thread twiddles of passes 2 and 3 (pass 1 has none), stored as the
+// Per-thread twiddles of passes 2, 3 and 4 (pass 1 has none), stored as the
 // base powers w, w^2, w^4, w^8 of each butterfly's root w; the other powers
 // are formed with at most three complex products (a few ulp of error).
 template <int L, int S> struct FftTw {
     using SH = FftShape<L>;
     static constexpr int NBASE3 = SH::R3 >= 16 ? 4 : SH::R3 >= 8 ? 3 : SH::R3 >= 4 ? 2 : 1;
     float2 b2[4];                                   // pass 2: w = exp(S 2 pi i k / 256)
-    float2 b3[SH::NB3 > 0 ? SH::NB3 : 1][NBASE3];   // pass 3: w = exp(S 2 pi i k / L)
+    float2 b3[SH::NB3 > 0 ? SH::NB3 : 1][NBASE3];   // pass 3: w = exp(S 2 pi i k / (256 R3))
+    float2 b4[SH::NB4 > 0 ? SH::NB4 : 1];           // pass 4 (radix 2): w = exp(S 2 pi i k / L)
     __device__ __forceinline__ void init(int t)
     {
         int k = t & 15;
@@ -162,9 +166,19 @@ template <int L, int S> struct FftTw {
 #pragma unroll
                 for (int e = 0; e < NBASE3; e++) {
                     double s, c;
-                    sincospi(2.0 * (double) (kk << e) / (double) L, &s, &c);
+                    sincospi(2.0 * (double) (kk << e) / (double) (256 * SH::R3), &s, &c);
                     b3[b][e] = make_float2((float) c, (float) (S * s));
                 }
+            }
+        }
+        if constexpr (SH::R4 > 1) {
+            static_assert(SH::R4 == 2, "fourth pass is radix 2");
+#pragma unroll
+            for (int b = 0; b < SH::NB4; b++) {
+                int kk = (t + SH::NT * b) & 4095;
+                double s, c;
+                sincospi(2.0 * (double) kk / (double) L, &s, &c);
+                b4[b] = make_float2((float) c, (float) (S * s));
             }
         }
     }
@@ -206,11 +220,12 @@ __device__ __forceinline__ void apply_tw_pass(float2 *x, int b, int t, const Fft
 {
     if constexpr (PASS == 2) apply_tw<16>(x, tw.b2);
     if constexpr (PASS == 3) apply_tw<FftShape<L>::R3>(x, tw.b3[b]);
+    if constexpr (PASS == 4) apply_tw<FftShape<L>::R4>(x, &tw.b4[b]);
 }
 
 // One Stockham pass.  v holds x[t + NT m]; results of a non-final pass go
 // through shared memory and come back in the same strided layout.
-// PASS: 1, 2 or 3 (selects the twiddles).  TW: FftTw (register bases).
+// PASS: 1 to 4 (selects the twiddles).  TW: FftTw (register bases).
 template <int L, int R, int LS, int S, bool LAST, int PASS, class TW>
 __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const TW &tw)
 {
@@ -247,7 +262,12 @@ template <int L, int S, class TW>
 __device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const TW &tw)
 {
     using SH = FftShape<L>;
-    if constexpr (SH::R3 > 1) {
+    if constexpr (SH::R4 > 1) {
+        fft_pass<L, 16, 1, S, false, 1>(v, sm, t, tw);
+        fft_pass<L, 16, 16, S, false, 2>(v, sm, t, tw);
+        fft_pass<L, 16, 256, S, false, 3>(v, sm, t, tw);
+        fft_pass<L, SH::R4, 4096, S, true, 4>(v, sm, t, tw);
+    } else if constexpr (SH::R3 > 1) {
         fft_pass<L, 16, 1, S, false, 1>(v, sm, t, tw);
         fft_pass<L, 16, 16, S, false, 2>(v, sm, t, tw);
         fft_pass<L, SH::R3, 256, S, true, 3>(v, sm, t, tw);

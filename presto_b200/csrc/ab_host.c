@@ -324,18 +324,52 @@ static int calc_fftlen(int numharm, int harmnum, int zmax, int wmax, const ab_ob
     return ab_next_good_fftlen(bins_needed + end_effects);
 }
 
-/* Device transform cost per template and transform, by log2 L: the
- * radix-16 work L log2 L unless measured costs are supplied. */
+/* Correlation cost per template and transform (ms), by log2 L, as installed
+ * by ab_set_transform_costs (ab_autotune measures it).  The initial table is
+ * k_corr measured on a B200 (1965 MHz): 512 to 4096 points.  Lengths whose
+ * entry is <= 0 are not used for superblocks; an all-zero table falls back
+ * to the radix-16 work L log2 L for lengths up to 4096.  (8192-point
+ * transforms run one 512-thread CTA per SM; in whole searches on B200 they
+ * cost more than their calibrated figure, so the initial table leaves them
+ * out.) */
+static double g_costs[AB_COST_SLOTS] = {0, 0, 0, 0, 0, 0, 0, 0, 0,
+                                        1.846e-6, 2.981e-6, 5.764e-6, 1.1243e-5, 0, 0, 0};
+static pthread_mutex_t g_costs_mu = PTHREAD_MUTEX_INITIALIZER;
+
+int ab_set_transform_costs(const double *costs, int n)
+{
+    if (n < 0 || (n > 0 && !costs)) return AB_ERR_ARG;
+    pthread_mutex_lock(&g_costs_mu);
+    for (int i = 0; i < AB_COST_SLOTS; i++) g_costs[i] = (i < n) ? costs[i] : 0.0;
+    pthread_mutex_unlock(&g_costs_mu);
+    return AB_OK;
+}
+
+int ab_get_transform_costs(double *costs, int n)
+{
+    if (!costs || n < 0) return AB_ERR_ARG;
+    pthread_mutex_lock(&g_costs_mu);
+    for (int i = 0; i < n; i++) costs[i] = (i < AB_COST_SLOTS) ? g_costs[i] : 0.0;
+    pthread_mutex_unlock(&g_costs_mu);
+    return AB_OK;
+}
+
+/* Cost of one transform of length L, or a negative value when L is not a
+ * candidate (no measured entry). */
 static double transform_cost(const double *cost_by_log2L, int L)
 {
     int lg = twon_to_index(L);
-    if (cost_by_log2L && lg < AB_COST_SLOTS && cost_by_log2L[lg] > 0.0) return cost_by_log2L[lg];
-    return (double) L * lg;
+    int any = 0;
+    for (int i = 0; cost_by_log2L && i < AB_COST_SLOTS; i++) any |= cost_by_log2L[i] > 0.0;
+    if (!any) return L <= 4096 ? (double) L * lg : -1.0;
+    return (lg < AB_COST_SLOTS && cost_by_log2L[lg] > 0.0) ? cost_by_log2L[lg] : -1.0;
 }
 
 int ab_bankset_init(const ab_obs *obs, ab_bankset *bs)
 {
-    return ab_bankset_init_tuned(obs, NULL, bs);
+    double c[AB_COST_SLOTS];
+    ab_get_transform_costs(c, AB_COST_SLOTS);
+    return ab_bankset_init_tuned(obs, c, bs);
 }
 
 int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_bankset *bs)
@@ -411,8 +445,8 @@ int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_ban
          * 4 hw0 - 1 samples of template reach fits in L2.  (L2, m) minimises
          * the transform cost per block. */
         int sbm = 1;
-        if (!obs->inmem && need <= b->fftlen_ref && nblocks > 1) {
-            double best = transform_cost(cost_by_log2L, L);
+        double best = transform_cost(cost_by_log2L, L);
+        if (!obs->inmem && need <= b->fftlen_ref && nblocks > 1 && best > 0.0) {
             for (int m = 2; m <= AB_MAX_SBM && m <= nblocks; m++) {
                 long long span = 0;
                 for (long long k = 0; k + m - 1 < nblocks; k++) {
@@ -420,10 +454,14 @@ int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_ban
                     if (sp > span) span = sp;
                 }
                 long long need_m = 4LL * b->hw0 + span - 1;
-                for (int L2 = 512; L2 <= 4096; L2 <<= 1) {
+                /* 8192-point transforms only for w = 0 banks: their template
+                 * generation holds the placed kernel (128 KiB) and no chirp
+                 * in shared memory */
+                const int lmax = b->wmax == 0 ? 8192 : 4096;
+                for (int L2 = 512; L2 <= lmax; L2 <<= 1) {
                     if (need_m > L2 || L2 < need) continue;
                     double c = transform_cost(cost_by_log2L, L2) / m;
-                    if (c < best * 0.98) {
+                    if (c > 0.0 && c < best * 0.98) {
                         best = c;
                         L = L2;
                         sbm = m;

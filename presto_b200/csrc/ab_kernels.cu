@@ -522,6 +522,7 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
             AB_PREP_CASE(512)
             AB_PREP_CASE(1024)
             AB_PREP_CASE(2048)
+            AB_PREP_CASE(4096)
 #undef AB_PREP_CASE
             default:
                 return cudaErrorInvalidValue;
@@ -621,7 +622,7 @@ cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host
 // the data spectrum is staged in shared memory once, templates stream from
 // L2 (each template row is read by every block of the batch).
 template <int L>
-__global__ void __launch_bounds__(256) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+__global__ void __launch_bounds__(FftShape<L>::CTA) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
                                               const CorrItem *items, const float2 *xhat,
                                               long long xhat_per_block, const float2 *tmpl,
                                               float *planes, long long plane_per_block,
@@ -740,18 +741,21 @@ cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
                         cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    size_t smem = (size_t) (L / 2 + 256 * 17) * sizeof(float2) + (size_t) L;
     switch (L) {
 #define AB_CORR_CASE(N)                                                                       \
-    case N:                                                                                   \
+    case N: {                                                                                 \
+        using SH = FftShape<N>;                                                               \
+        const size_t smem = (size_t) (N / 2 + SH::G * SH::SMEM) * sizeof(float2) + (size_t) N; \
         cudaFuncSetAttribute(k_corr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
-        k_corr<N><<<nitems, 256, smem, st>>>(banks_dev, sc, bb, items, xhat, xhat_per_block,  \
-                                             tmpl, planes, plane_per_block, fullplane);       \
-        break;
+        k_corr<N><<<nitems, SH::CTA, smem, st>>>(banks_dev, sc, bb, items, xhat, xhat_per_block, \
+                                                 tmpl, planes, plane_per_block, fullplane);   \
+        break;                                                                                \
+    }
         AB_CORR_CASE(512)
         AB_CORR_CASE(1024)
         AB_CORR_CASE(2048)
         AB_CORR_CASE(4096)
+        AB_CORR_CASE(8192)
 #undef AB_CORR_CASE
         default:
             return cudaErrorInvalidValue;

@@ -22,8 +22,9 @@ using namespace ab;
 
 namespace {
 
-// Static scratch: 160 KiB, held by every GPU that loads the library until exit.
-constexpr size_t kScratchBytes = 160u << 10;
+// Static scratch: 192 KiB, held by every GPU that loads the library until exit
+// (work items and a data spectrum of up to 4096 points, for 8192-point banks).
+constexpr size_t kScratchBytes = 192u << 10;
 constexpr size_t kDescOff = 0;          // ab_bank
 constexpr size_t kStartOff = 1024;      // double
 constexpr size_t kItemsOff = 2048;      // CorrItem[kMaxItems]
@@ -97,7 +98,7 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
     }
     if (powers_capacity < need) return AB_ERR_OVERFLOW;
     if (g.numrs > b.numrs_max) return AB_ERR_ARG;
-    const int G = 4096 / b.L, tile = 16 * G;
+    const int G = b.L >= 4096 ? 1 : 4096 / b.L, tile = 16 * G;
     const int nitems = (b.ntmpl + tile - 1) / tile;
     if (nitems > kMaxItems || kXhatOff + sizeof(float2) * (size_t) (b.L / 2) > kScratchBytes) {
         fprintf(stderr, "ab_fderivs_vol_noalloc: bank %d/%d needs %d work items and a %d-point "

@@ -103,3 +103,26 @@ def test_sort_and_eliminate(ablib):
     e = ablib.eliminate_harmonics(s)
     # 300.5 ~ 2*150.2, 50.0 ~ 150.2/3, 100 ~ 150.2*2/3, 200 ~ 150.2*4/3 are removed
     assert [x[3] for x in e] == [150.2]
+
+
+def test_transform_cost_table_drives_schedule(ablib):
+    """The process-wide cost table chooses transform lengths and superblock
+    heights; lengths without a measured cost are not used, and every choice
+    keeps 4 hw0 + numrs - 1 <= L (the span of one block)."""
+    obs = ablib.obs_init(ablib.make_params(1 << 17, 64e-6, 1 << 16, zmax=60, wmax=0, numharm=4))
+    default = ablib.get_transform_costs()
+    try:
+        assert default[13] <= 0.0 and all(default[i] > 0.0 for i in range(9, 13))
+        for b in ablib.bank_geometry(obs):
+            assert b["L"] <= 4096 and 1 <= b["sbm"] <= 8
+            assert 4 * b["hw"] + b["numrs_max"] - 1 <= b["L"]
+        cheap8k = list(default)
+        cheap8k[13] = default[12] * 1.5
+        ablib.set_transform_costs(cheap8k)
+        geo = ablib.bank_geometry(obs)
+        assert any(b["L"] == 8192 and b["sbm"] > 1 for b in geo)
+        ablib.set_transform_costs([0.0] * 16)             # unmeasured: L log2 L up to 4096
+        assert all(b["L"] <= 4096 for b in ablib.bank_geometry(obs))
+    finally:
+        ablib.set_transform_costs(default)
+    assert ablib.get_transform_costs() == default

@@ -71,15 +71,29 @@ def test_responses_match_oracle(ctx, oracle, z, w):
     assert np.max(np.abs(dev - orc)) <= 2e-6 * np.max(np.abs(orc))
 
 
-def test_fundamental_templates_match_oracle(ctx, oracle, case):
+def test_fundamental_templates_match_oracle(ctx, oracle, ablib, case):
+    """Device templates against the oracle's: at the reference's fftlen when
+    the device uses it, else the oracle's response placed (centre at index 0,
+    place_complex_kernel) and transformed in FP64 at the device length (a
+    superblock transform serves several blocks)."""
     obs, oobs = case["obs"], case["oobs"]
     bank = oracle.Bank(oobs, 1, 1)
+    hwf = ablib.lib().ab_w_resp_halfwidth
     for wi in sorted({0, bank.nw // 2, bank.nw - 1}):
         for zi in (0, bank.nz // 3, bank.nz - 1):
             dev = ctx.bank_kernel(obs, 1, 1, wi, zi)
-            assert dev.size == bank.fftlen
-            orc = bank.kernel(wi, zi)
-            assert np.max(np.abs(dev - orc)) <= 2e-6 * np.max(np.abs(orc)), (wi, zi)
+            if dev.size == bank.fftlen:
+                orc = bank.kernel(wi, zi)
+            else:
+                z, w = -bank.zmax + 2.0 * zi, -bank.wmax + 20.0 * wi
+                numkern = 4 * hwf(z, w)
+                resp = oracle.response("w" if w != 0 else "z", 2, numkern, z=z, w=w)
+                placed = np.zeros(dev.size, np.complex128)
+                half = numkern // 2
+                placed[:half] = resp[half:]
+                placed[dev.size - half:] = resp[:half]
+                orc = np.fft.fft(placed)
+            assert np.max(np.abs(dev - orc)) <= 2e-6 * np.max(np.abs(orc)), (wi, zi, dev.size)
 
 
 def _harmonics(obs):
@@ -302,3 +316,35 @@ def test_wrapping_bank_matches_oracle(ctx, ablib, oracle):
         assert meta == ometa
         ok, worst = _close(dev, orc)
         assert ok, (b, worst)
+
+
+def test_search_with_8192_point_transforms(ablib, oracle):
+    """A cost table that makes 8192-point superblock transforms cheapest (the
+    four-pass FFT, 512-thread CTAs): the search still matches the oracle."""
+    c = CASES["std"]
+    fft = _spec(c["N"], c["seed"], c["pulsars"])
+    kw = dict(zmax=c["zmax"], wmax=c["wmax"], numharm=c["numharm"])
+    default = ablib.get_transform_costs()
+    table = list(default)
+    table[13] = default[12] * 1.5
+    ablib.set_transform_costs(table)
+    try:
+        obs = ablib.obs_init(ablib.make_params(c["N"], DT, fft.size, **kw))
+        assert any(b["L"] == 8192 for b in ablib.bank_geometry(obs))
+        cx = ablib.Context(0)
+        dev = cx.search(obs, fft)
+        blk, st, wi, zi, ri, pw = cx.last_hits()
+        cx.close()
+    finally:
+        ablib.set_transform_costs(default)
+    ocands, ohits, _ = oracle.accelsearch(oracle.make_params(c["N"], DT, fft.size, **kw), fft,
+                                          nthreads=os.cpu_count() or 1)
+    dset = {(int(b), int(s), int(w), int(z), int(r)): float(p)
+            for b, s, w, z, r, p in zip(blk, st, wi, zi, ri, pw)}
+    oset = {(b, s, w, z, r): p for b, s, w, z, r, p in ohits}
+    only_d = [k for k in dset if k not in oset and not _borderline(dset[k], k[1], obs)]
+    only_o = [k for k in oset if k not in dset and not _borderline(oset[k], k[1], obs)]
+    assert not only_d and not only_o, (only_d[:5], only_o[:5])
+    for k in set(dset) & set(oset):
+        assert abs(dset[k] - oset[k]) <= PTOL * oset[k], k
+    assert len(dev) == len(ocands)
