@@ -386,32 +386,72 @@ __device__ __forceinline__ void block_geom(const SearchConsts &sc, const ab_bank
                       sc.obs_wlo, sc.corr_uselen);
 }
 
-// Bitonic sort of n2 (power of two) floats in shared memory.
-__device__ void bitonic_sort(float *a, int n2)
+// k-th smallest (0-based) of n non-negative floats in shared memory, exactly:
+// a radix select over the IEEE bit patterns (which order like the values for
+// x >= 0), four passes of 8-bit digits from the top.  Each pass histograms the
+// digit of the candidates that match the prefix found so far (warp-aggregated
+// shared atomics), and one warp scans the 256 counts for the digit holding
+// rank k.  Called by every thread of the CTA (blockDim a multiple of 32).
+__device__ float select_rank(const float *a, int n, int k, unsigned *hist, unsigned *s_res)
 {
-    for (int k = 2; k <= n2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-                int l = i ^ j;
-                if (l > i) {
-                    float x = a[i], y = a[l];
-                    bool up = (i & k) == 0;
-                    if ((x > y) == up) {
-                        a[i] = y;
-                        a[l] = x;
+    const int lane = threadIdx.x & 31;
+    unsigned prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
+        __syncthreads();
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            unsigned key = 256u;                               // not a candidate
+            if (i < n) {
+                const unsigned u = __float_as_uint(a[i]);
+                if ((u & mask) == prefix) key = (u >> shift) & 255u;
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (key < 256u && lane == __ffs(peers) - 1) atomicAdd(&hist[key], (unsigned) __popc(peers));
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            // lane l owns digits 8l .. 8l+7
+            unsigned c[8], tot = 0;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                c[q] = hist[8 * lane + q];
+                tot += c[q];
+            }
+            unsigned incl = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            unsigned before = incl - tot;                     // candidates below this lane's digits
+            const bool mine = (unsigned) k >= before && (unsigned) k < incl;
+            if (mine) {
+                unsigned acc = before;
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    if ((unsigned) k >= acc && (unsigned) k < acc + c[q]) {
+                        s_res[0] = 8u * lane + q;
+                        s_res[1] = (unsigned) k - acc;
                     }
+                    acc += c[q];
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
+        prefix |= s_res[0] << shift;
+        mask |= 255u << shift;
+        k = (int) s_res[1];
+        __syncthreads();
     }
+    return __uint_as_float(prefix);
 }
 
 // Block normalisation 1/sqrt(median(|X|^2)/ln 2) of the numdata bins from
 // lobin (zero outside the spectrum), or 1/sqrt(nph) when nph is given
 // (src/accel_utils.c:1079-1099).  The median is taken over float POWER()
 // values without FMA, sorted exactly; even counts average the two central
-// values (GSL semantics).  pw: shared scratch of nextpow2(numdata) floats.
+// values (GSL semantics).  pw: shared scratch of numdata floats.
 // Called by every thread of the CTA.
 __device__ double block_norm(const SearchConsts &sc, long long lobin, int numdata, const float2 *fft,
                              float *pw, double *s_norm)
@@ -420,23 +460,18 @@ __device__ double block_norm(const SearchConsts &sc, long long lobin, int numdat
         if (threadIdx.x == 0) *s_norm = 1.0 / sqrt((double) sc.nph);
     } else {
         // block median of |X|^2 in float (POWER(), no FMA), src/accel_utils.c:1087-1099
-        int n2 = 1;
-        while (n2 < numdata) n2 <<= 1;
-        for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-            float p = INFINITY;
-            if (i < numdata) {
-                long long bin = lobin + i - sc.obs_lobin;
-                float2 v = (bin >= 0 && bin < sc.numbins) ? fft[bin] : make_float2(0.f, 0.f);
-                p = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
-            }
-            pw[i] = p;
+        for (int i = threadIdx.x; i < numdata; i += blockDim.x) {
+            long long bin = lobin + i - sc.obs_lobin;
+            float2 v = (bin >= 0 && bin < sc.numbins) ? fft[bin] : make_float2(0.f, 0.f);
+            pw[i] = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
         }
         __syncthreads();
-        bitonic_sort(pw, n2);
+        // the two central order statistics (equal for odd counts), as a sort gives them
+        __shared__ unsigned s_hist[256], s_res[2];
+        const float lo = select_rank(pw, numdata, (numdata - 1) / 2, s_hist, s_res);
+        const float hi = (numdata & 1) ? lo : select_rank(pw, numdata, numdata / 2, s_hist, s_res);
         if (threadIdx.x == 0) {
-            double m;
-            if (numdata & 1) m = pw[numdata / 2];
-            else m = 0.5 * ((double) pw[(numdata - 1) / 2] + (double) pw[numdata / 2]);
+            double m = (numdata & 1) ? (double) lo : 0.5 * ((double) lo + (double) hi);
             float med = (float) m;
             *s_norm = 1.0 / sqrt((double) med / 0.69314718055994530942);
         }
