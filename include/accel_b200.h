@@ -178,6 +178,29 @@ int ab_fund_to_ffdotplane(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fu
 int ab_inmem_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
                            int numharm, int harmnum);
 
+/* The -otheropt forms the reference's driver selects instead
+ * (src/accelsearch.c:145-159): add_ffdotpows_ptrs (src/accel_utils.c:1284-1309),
+ * fund_to_ffdotplane_trans (:1236-1250) and inmem_add_ffdotpows_trans
+ * (:1364-1409) compute the same sums as the plain forms over an [r][z] host
+ * plane.  The engine's full plane is its own device array, so these take the
+ * plain forms' arguments and give their results. */
+int ab_add_ffdotpows_ptrs(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
+                          const ab_ffdotpows *sub, int numharm, int harmnum, double fullrlo);
+int ab_fund_to_ffdotplane_trans(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fund);
+int ab_inmem_add_ffdotpows_trans(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
+                                 int numharm, int harmnum);
+
+/* copy_ffdotpows (src/accel_utils.c:1200-1217): geometry and powers of src
+ * into dst, whose powers array is the caller's (dst->capacity floats).
+ * Host only. */
+int ab_copy_ffdotpows(const ab_ffdotpows *src, ab_ffdotpows *dst);
+
+/* get_fourier_amplitudes (src/accel_utils.c:993-1022): numbins bins from
+ * lobin of the spectrum fft (obs->numbins bins starting at obs->lobin) into
+ * out, zero where the window runs off either end.  Host only. */
+int ab_get_fourier_amplitudes(const ab_obs *obs, const ab_fcomplex *fft, long long lobin,
+                              int numbins, ab_fcomplex *out);
+
 /* Candidate list (the GSList of accelcand built by search_ffdotpows). */
 typedef struct ab_list ab_candlist;
 ab_candlist *ab_candlist_new(void);

@@ -7,5 +7,6 @@ C ABI in include/accel_b200.h; this package is its Python host mirror.
 from .accel import (CORR_FFT, CORR_TC_SPLIT_BF16, AccelError, AccelSearch, CandList,  # noqa: F401
                     Context, algorithmic_counts,
                     bank_geometry, candidate_sigma, eliminate_harmonics, lib, make_params,
-                    get_transform_costs, num_blocks, obs_init, power_for_sigma,
+                    get_fourier_amplitudes, get_transform_costs, num_blocks, obs_init,
+                    power_for_sigma,
                     set_transform_costs, sort_cands)

@@ -32,7 +32,9 @@ EXPORTS = [
     "ab_fderivs_vol_noalloc", "ab_pool_create", "ab_pool_destroy", "ab_pool_last_error",
     "ab_pool_submit", "ab_pool_wait", "ab_pool_stats", "ab_pool_reset_stats", "ab_tc_gemm",
     "ab_ctx_set_corr_path", "ab_w_resp_halfwidth", "ab_set_transform_costs",
-    "ab_get_transform_costs", "ab_autotune",
+    "ab_get_transform_costs", "ab_autotune", "ab_add_ffdotpows_ptrs",
+    "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
+    "ab_get_fourier_amplitudes",
 ]
 
 COST_SLOTS = 16
@@ -118,6 +120,11 @@ def lib():
                                    C.POINTER(FFDotPows), i, i, d]
     L.ab_fund_to_ffdotplane.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows)]
     L.ab_inmem_add_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, i]
+    L.ab_add_ffdotpows_ptrs.argtypes = L.ab_add_ffdotpows.argtypes
+    L.ab_fund_to_ffdotplane_trans.argtypes = L.ab_fund_to_ffdotplane.argtypes
+    L.ab_inmem_add_ffdotpows_trans.argtypes = L.ab_inmem_add_ffdotpows.argtypes
+    L.ab_copy_ffdotpows.argtypes = [C.POINTER(FFDotPows), C.POINTER(FFDotPows)]
+    L.ab_get_fourier_amplitudes.argtypes = [C.POINTER(Obs), vp, ll, i, vp]
     L.ab_candlist_new.restype = vp
     L.ab_candlist_free.argtypes = [vp]
     L.ab_candlist_get.restype = ll
@@ -211,6 +218,17 @@ def bank_geometry(obs):
     lib().ab_bank_geometry(C.byref(obs), C.byref(n), info, n.value)
     keys = ("numharm", "harmnum", "nz", "nw", "fftlen_ref", "L", "hw", "numrs_max", "sbm")
     return [dict(zip(keys, info[9 * k:9 * k + 9])) for k in range(n.value)]
+
+
+def get_fourier_amplitudes(obs, fft, lobin, numbins):
+    """get_fourier_amplitudes: numbins bins from lobin, zero off the spectrum."""
+    fft = np.ascontiguousarray(fft, dtype=np.complex64)
+    out = np.zeros(numbins, np.complex64)
+    rc = lib().ab_get_fourier_amplitudes(C.byref(obs), fft.ctypes.data, int(lobin), int(numbins),
+                                         out.ctypes.data)
+    if rc:
+        raise AccelError(f"ab_get_fourier_amplitudes: {ERRORS.get(rc, rc)}")
+    return out
 
 
 def get_transform_costs():

@@ -1240,6 +1240,23 @@ int ab_fund_to_ffdotplane(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fu
     return AB_OK;
 }
 
+int ab_add_ffdotpows_ptrs(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund,
+                          const ab_ffdotpows *sub, int numharm, int harmnum, double fullrlo)
+{
+    return ab_add_ffdotpows(ctx, obs, fund, sub, numharm, harmnum, fullrlo);
+}
+
+int ab_fund_to_ffdotplane_trans(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *fund)
+{
+    return ab_fund_to_ffdotplane(ctx, obs, fund);
+}
+
+int ab_inmem_add_ffdotpows_trans(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund, int numharm,
+                                 int harmnum)
+{
+    return ab_inmem_add_ffdotpows(ctx, obs, fund, numharm, harmnum);
+}
+
 int ab_inmem_add_ffdotpows(ab_ctx *ctx, const ab_obs *obs, ab_ffdotpows *fund, int numharm,
                            int harmnum)
 {

@@ -989,4 +989,35 @@ int ab_bank_geometry(const ab_obs *obs, int *nbanks, int *info, int maxbanks)
     return AB_OK;
 }
 
+/* copy_ffdotpows (src/accel_utils.c:1200-1217) into caller-owned storage. */
+int ab_copy_ffdotpows(const ab_ffdotpows *src, ab_ffdotpows *dst)
+{
+    if (!src || !dst || (!src->powers && src->numrs > 0)) return AB_ERR_ARG;
+    size_t n = (size_t) src->numws * src->numzs * src->numrs;
+    if (!dst->powers || dst->capacity < n) return AB_ERR_OVERFLOW;
+    dst->rlo = src->rlo;
+    dst->zlo = src->zlo;
+    dst->wlo = src->wlo;
+    dst->numrs = src->numrs;
+    dst->numzs = src->numzs;
+    dst->numws = src->numws;
+    if (n) memcpy(dst->powers, src->powers, sizeof(float) * n);
+    return AB_OK;
+}
+
+/* get_fourier_amplitudes (src/accel_utils.c:993-1022): the window
+ * [lobin, lobin + numbins) of a spectrum that starts at bin obs->lobin, with
+ * zeros where it runs off either end. */
+int ab_get_fourier_amplitudes(const ab_obs *obs, const ab_fcomplex *fft, long long lobin,
+                              int numbins, ab_fcomplex *out)
+{
+    if (!obs || !fft || !out || numbins < 0) return AB_ERR_ARG;
+    for (int i = 0; i < numbins; i++) {
+        long long b = lobin - obs->lobin + i;
+        if (b >= 0 && b < obs->numbins) out[i] = fft[b];
+        else out[i].r = out[i].i = 0.0f;
+    }
+    return AB_OK;
+}
+
 long long ab_num_blocks_main(const ab_obs *obs) { return obs ? ab_num_blocks(obs) : -1; }

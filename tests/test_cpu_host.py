@@ -126,3 +126,26 @@ def test_transform_cost_table_drives_schedule(ablib):
     finally:
         ablib.set_transform_costs(default)
     assert ablib.get_transform_costs() == default
+
+
+def test_fourier_amplitudes_and_copy(ablib):
+    """get_fourier_amplitudes zero-pads past both ends of the spectrum;
+    copy_ffdotpows copies geometry and powers (host-only entry points)."""
+    import ctypes as C
+    obs = ablib.obs_init(ablib.make_params(1 << 12, 64e-6, 1 << 11, zmax=10, numharm=2))
+    rng = np.random.default_rng(5)
+    fft = (rng.standard_normal(obs.numbins) + 1j * rng.standard_normal(obs.numbins)).astype(np.complex64)
+    out = ablib.get_fourier_amplitudes(obs, fft, obs.lobin - 5, 20)
+    assert np.all(out[:5] == 0) and np.array_equal(out[5:], fft[:15])
+    out = ablib.get_fourier_amplitudes(obs, fft, obs.lobin + obs.numbins - 4, 10)
+    assert np.array_equal(out[:4], fft[-4:]) and np.all(out[4:] == 0)
+    src_pw = rng.random(2 * 3 * 7).astype(np.float32)
+    dst_pw = np.zeros(64, np.float32)
+    F = ablib.accel.FFDotPows
+    src = F(11, -4, 0, 7, 3, 2, src_pw.ctypes.data_as(C.POINTER(C.c_float)), src_pw.size)
+    dst = F(0, 0, 0, 0, 0, 0, dst_pw.ctypes.data_as(C.POINTER(C.c_float)), dst_pw.size)
+    assert ablib.lib().ab_copy_ffdotpows(C.byref(src), C.byref(dst)) == 0
+    assert (dst.rlo, dst.zlo, dst.numrs, dst.numzs, dst.numws) == (11, -4, 7, 3, 2)
+    assert np.array_equal(dst_pw[:src_pw.size], src_pw)
+    small = F(0, 0, 0, 0, 0, 0, dst_pw.ctypes.data_as(C.POINTER(C.c_float)), 5)
+    assert ablib.lib().ab_copy_ffdotpows(C.byref(src), C.byref(small)) == -4
