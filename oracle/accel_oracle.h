@@ -148,6 +148,41 @@ void      orc_search_ffdotpows(const orc_ffdot *ffd, int numharm, const orc_obs 
                                orc_list *l, long long block, orc_hit *hits,
                                long long maxhits, long long *numhits);
 
+/* ---- candidate polishing (polish_oracle.c) ---------------------------- */
+#define ORC_MAX_HARM 32
+typedef struct {                 /* rderivs, include/presto.h:160-168 */
+    double pow, phs, dpow, dphs, d2pow, d2phs, locpow;
+} orc_rderivs;
+typedef struct {                 /* fourierprops, include/presto.h:170-188 */
+    double r;
+    float rerr;
+    double z;
+    float zerr;
+    double w;
+    float werr;
+    float pow, powerr, sig, rawpow, phs, phserr, cen, cenerr, pur, purerr, locpow;
+} orc_fourierprops;
+
+int    orc_z_resp_halfwidth_acc(double z, int highacc);
+int    orc_w_resp_halfwidth_acc(double z, double w, int highacc);
+void   orc_rzw_interp(const orc_fcomplex *data, long numdata, double r, double z, double w,
+                      int kern_half_width, orc_fcomplex *ans);
+double orc_get_localpower3d(const orc_fcomplex *data, long numdata, double r, double z, double w);
+void   orc_get_derivs3d(const orc_fcomplex *data, long numdata, double r, double z, double w,
+                        double localpower, orc_rderivs *res);
+int    orc_calc_props(const orc_rderivs *d, double r, double z, double w, orc_fourierprops *o);
+double orc_max_rz_arr(const orc_fcomplex *data, long numdata, double rin, double zin,
+                      double *rout, double *zout, orc_rderivs *derivs);
+void   orc_max_rz_arr_harmonics(const orc_fcomplex *data, long numdata, int numharm, double rin,
+                                double zin, double *rout, double *zout, orc_rderivs *derivs,
+                                double *powers);
+int    orc_optimize_accelcand(const orc_fcomplex *fft, long long numbins, long long lobin,
+                              int numharm, double r, double z, double *pows, double *hirs,
+                              double *hizs, orc_rderivs *derivs);
+int    orc_optimize_cands(const orc_fcomplex *fft, long long numbins, long long lobin, int ncand,
+                          const int *numharm, const double *r, const double *z, double *pows,
+                          double *hirs, double *hizs, orc_rderivs *derivs, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -232,3 +232,90 @@ def ref_fresnel_lib():
     L.fresnl.argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.fresnl.restype = C.c_int
     return L
+
+
+# ---- candidate polishing (polish_oracle.c) --------------------------------
+MAX_HARM = 32
+
+
+class RDerivs(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("pow", "phs", "dpow", "dphs", "d2pow", "d2phs",
+                                         "locpow")]
+
+
+class FourierProps(C.Structure):
+    _fields_ = [("r", C.c_double), ("rerr", C.c_float), ("z", C.c_double), ("zerr", C.c_float),
+                ("w", C.c_double), ("werr", C.c_float)] + \
+               [(n, C.c_float) for n in ("pow", "powerr", "sig", "rawpow", "phs", "phserr", "cen",
+                                         "cenerr", "pur", "purerr", "locpow")]
+
+
+def _polish_lib():
+    L = lib(64)
+    if not getattr(L, "_polish_ready", False):
+        d, i, vp = C.c_double, C.c_int, C.c_void_p
+        L.orc_rzw_interp.argtypes = [vp, C.c_long, d, d, d, i, vp]
+        L.orc_get_localpower3d.restype = d
+        L.orc_get_localpower3d.argtypes = [vp, C.c_long, d, d, d]
+        L.orc_get_derivs3d.argtypes = [vp, C.c_long, d, d, d, d, C.POINTER(RDerivs)]
+        L.orc_calc_props.argtypes = [C.POINTER(RDerivs), d, d, d, C.POINTER(FourierProps)]
+        L.orc_max_rz_arr.restype = d
+        L.orc_max_rz_arr.argtypes = [vp, C.c_long, d, d, C.POINTER(d), C.POINTER(d),
+                                     C.POINTER(RDerivs)]
+        L.orc_max_rz_arr_harmonics.argtypes = [vp, C.c_long, i, d, d, C.POINTER(d), C.POINTER(d),
+                                               C.POINTER(RDerivs), C.POINTER(d)]
+        L.orc_optimize_cands.argtypes = [vp, C.c_longlong, C.c_longlong, i, vp, vp, vp, vp, vp,
+                                         vp, vp, i]
+        L.orc_z_resp_halfwidth_acc.argtypes = [d, i]
+        L._polish_ready = True
+    return L
+
+
+def rz_interp(data, r, z, kern_half_width, w=0.0):
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    a = np.zeros(1, np.complex64)
+    _polish_lib().orc_rzw_interp(data.ctypes.data, data.size, r, z, w, kern_half_width,
+                                 a.ctypes.data)
+    return complex(a[0])
+
+
+def max_rz_arr(data, r, z):
+    """(power, rout, zout, rderivs) of the single-harmonic optimiser."""
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    ro, zo, rd = C.c_double(), C.c_double(), RDerivs()
+    p = _polish_lib().orc_max_rz_arr(data.ctypes.data, data.size, r, z, C.byref(ro), C.byref(zo),
+                                      C.byref(rd))
+    return p, ro.value, zo.value, rd
+
+
+def max_rz_arr_harmonics(data, r, z, numharm):
+    """(rout, zout, [rderivs per harmonic], [raw power per harmonic])."""
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    ro, zo = C.c_double(), C.c_double()
+    rds = (RDerivs * numharm)()
+    pw = (C.c_double * numharm)()
+    _polish_lib().orc_max_rz_arr_harmonics(data.ctypes.data, data.size, numharm, r, z,
+                                           C.byref(ro), C.byref(zo), rds, pw)
+    return ro.value, zo.value, list(rds), list(pw)
+
+
+def optimize_cands(fft, lobin, cands, nthreads=1):
+    """optimize_accelcand for (numharm, r, z) candidates: per candidate a dict
+    of pows, hirs, hizs (numharm entries) and the derivs array."""
+    fft = np.ascontiguousarray(fft, dtype=np.complex64)
+    n = len(cands)
+    nh = np.array([c[0] for c in cands], np.int32)
+    r = np.array([c[1] for c in cands], np.float64)
+    z = np.array([c[2] for c in cands], np.float64)
+    pows = np.zeros((n, MAX_HARM))
+    hirs = np.zeros((n, MAX_HARM))
+    hizs = np.zeros((n, MAX_HARM))
+    der = np.zeros((n, MAX_HARM, 7))
+    rc = _polish_lib().orc_optimize_cands(fft.ctypes.data, fft.size, int(lobin), n, nh.ctypes.data,
+                                          r.ctypes.data, z.ctypes.data, pows.ctypes.data,
+                                          hirs.ctypes.data, hizs.ctypes.data, der.ctypes.data,
+                                          int(nthreads))
+    if rc:
+        raise RuntimeError("orc_optimize_cands failed")
+    return [dict(pows=pows[k, :nh[k]], hirs=hirs[k, :nh[k]], hizs=hizs[k, :nh[k]],
+                 derivs=der[k, :nh[k]]) for k in range(n)]
