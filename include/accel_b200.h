@@ -285,6 +285,26 @@ int  ab_pool_reset_stats(ab_pool *pool);
  * K <= 256, N % 16 == 0, 16 <= N <= 256. */
 int ab_tc_gemm(ab_ctx *ctx, const float *A, const float *B, float *C, int N, int K, int split);
 
+/* Candidate polishing: optimize_accelcand (src/accel_utils.c:552-626) for
+ * the candidates of an acceleration search (obs->numw == 0) with the
+ * reference's default harmonic polishing (max_rz_arr_harmonics,
+ * src/maximize_rz.c:173-228), every candidate at once on the device.  fft
+ * holds obs->numbins bins (device pointer when fft_on_device != 0).  out[k]
+ * receives the optimised r, z (and w = 0) of each harmonic of cands[k], its
+ * raw power and its rderivs (include/presto.h:160-168). */
+#define AB_POLISH_MAX_HARM 32
+typedef struct {
+    double pow, phs, dpow, dphs, d2pow, d2phs, locpow;
+} ab_rderivs;
+typedef struct {
+    int numharm;
+    double pows[AB_POLISH_MAX_HARM];
+    double hirs[AB_POLISH_MAX_HARM], hizs[AB_POLISH_MAX_HARM], hiws[AB_POLISH_MAX_HARM];
+    ab_rderivs derivs[AB_POLISH_MAX_HARM];
+} ab_polished;
+int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
+                      const ab_cand *cands, long long n, ab_polished *out);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -34,7 +34,7 @@ EXPORTS = [
     "ab_ctx_set_corr_path", "ab_w_resp_halfwidth", "ab_set_transform_costs",
     "ab_get_transform_costs", "ab_autotune", "ab_add_ffdotpows_ptrs",
     "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
-    "ab_get_fourier_amplitudes",
+    "ab_get_fourier_amplitudes", "ab_optimize_cands",
 ]
 
 COST_SLOTS = 16
@@ -42,6 +42,21 @@ COST_SLOTS = 16
 # correlation paths (ab_ctx_set_corr_path)
 CORR_FFT = 0
 CORR_TC_SPLIT_BF16 = 1
+
+
+POLISH_MAX_HARM = 32
+
+
+class RDerivs(C.Structure):
+    """rderivs (include/presto.h:160-168)."""
+    _fields_ = [(n, C.c_double) for n in ("pow", "phs", "dpow", "dphs", "d2pow", "d2phs",
+                                         "locpow")]
+
+
+class Polished(C.Structure):
+    _fields_ = [("numharm", C.c_int), ("pows", C.c_double * POLISH_MAX_HARM),
+                ("hirs", C.c_double * POLISH_MAX_HARM), ("hizs", C.c_double * POLISH_MAX_HARM),
+                ("hiws", C.c_double * POLISH_MAX_HARM), ("derivs", RDerivs * POLISH_MAX_HARM)]
 
 
 class AccelError(RuntimeError):
@@ -125,6 +140,8 @@ def lib():
     L.ab_inmem_add_ffdotpows_trans.argtypes = L.ab_inmem_add_ffdotpows.argtypes
     L.ab_copy_ffdotpows.argtypes = [C.POINTER(FFDotPows), C.POINTER(FFDotPows)]
     L.ab_get_fourier_amplitudes.argtypes = [C.POINTER(Obs), vp, ll, i, vp]
+    L.ab_optimize_cands.argtypes = [vp, C.POINTER(Obs), vp, i, C.POINTER(Cand), ll,
+                                    C.POINTER(Polished)]
     L.ab_candlist_new.restype = vp
     L.ab_candlist_free.argtypes = [vp]
     L.ab_candlist_get.restype = ll
@@ -422,6 +439,32 @@ class Context:
         self._check(self.L.ab_bank_kernel(self.ptr, C.byref(obs), numharm, harmnum, wi, zi,
                                           out.ctypes.data, L.value, C.byref(L)), "ab_bank_kernel")
         return out
+
+    def optimize_cands(self, obs, fft, cands, device_ptr=None):
+        """optimize_accelcand for (power, sigma, numharm, r, z, w) candidates of
+        an acceleration search: per candidate a dict of the harmonics'
+        optimised pows, hirs, hizs, hiws and derivs (numharm x 7)."""
+        n = len(cands)
+        if n == 0:
+            return []
+        arr = (Cand * n)(*[Cand(c[0], c[1], c[2], c[3], c[4], c[5]) for c in cands])
+        out = (Polished * n)()
+        if device_ptr is not None:
+            src, on_dev = C.c_void_p(device_ptr), 1
+        else:
+            fft = np.ascontiguousarray(fft, dtype=np.complex64)
+            src, on_dev = C.c_void_p(fft.ctypes.data), 0
+        self._check(self.L.ab_optimize_cands(self.ptr, C.byref(obs), src, on_dev, arr, n, out),
+                    "ab_optimize_cands")
+        res = []
+        for o in out:
+            h = o.numharm
+            d = np.array([[getattr(o.derivs[k], f) for f in ("pow", "phs", "dpow", "dphs", "d2pow",
+                                                              "d2phs", "locpow")]
+                          for k in range(h)])
+            res.append(dict(pows=np.array(o.pows[:h]), hirs=np.array(o.hirs[:h]),
+                            hizs=np.array(o.hizs[:h]), hiws=np.array(o.hiws[:h]), derivs=d))
+        return res
 
     def autotune(self):
         """Measure the correlation cost per transform length on this context's

@@ -957,6 +957,48 @@ int ab_autotune(ab_ctx *ctx, double *costs_out, int n)
     return AB_OK;
 }
 
+int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
+                      const ab_cand *cands, long long n, ab_polished *out)
+{
+    if (!ctx || !obs || !fft || (n > 0 && (!cands || !out)) || n < 0) return AB_ERR_ARG;
+    if (obs->numw > 0)
+        return fail(ctx, AB_ERR_ARG, "polishing of jerk-search candidates is not available");
+    if (n == 0) return AB_OK;
+    if (n > (1 << 24)) return fail(ctx, AB_ERR_ARG, "too many candidates");
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    const float2 *dfft = reinterpret_cast<const float2 *>(fft);
+    if (!fft_on_device) {
+        CK(ctx->fft.ensure((size_t) obs->numbins));
+        CK(cudaMemcpyAsync(ctx->fft.p, fft, sizeof(float2) * obs->numbins, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        ctx->fft_bins = obs->numbins;
+        ctx->fft_valid = true;
+        dfft = ctx->fft.p;
+    }
+    std::vector<PolishIn> in((size_t) n);
+    for (long long k = 0; k < n; k++) {
+        if (cands[k].numharm < 1 || cands[k].numharm > AB_POLISH_MAX_HARM)
+            return fail(ctx, AB_ERR_ARG, "candidate %lld has %d harmonics", k, cands[k].numharm);
+        in[k] = PolishIn{cands[k].r, cands[k].z, cands[k].numharm, 0};
+    }
+    DevBuf<PolishIn> din;
+    DevBuf<ab_polished> dout;
+    cudaError_t e = din.ensure((size_t) n);
+    if (e == cudaSuccess) e = dout.ensure((size_t) n);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(din.p, in.data(), sizeof(PolishIn) * n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_polish(dfft, obs->numbins, obs->lobin, din.p, (int) n, dout.p, ctx->stream);
+    if (e == cudaSuccess) ctx->launches++;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout.p, sizeof(ab_polished) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    din.release();
+    dout.release();
+    if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "candidate polishing failed: %s", cudaGetErrorString(e));
+    return AB_OK;
+}
+
 int ab_ctx_set_corr_path(ab_ctx *ctx, int path)
 {
     if (!ctx || (path != AB_CORR_FFT && path != AB_CORR_TC_SPLIT_BF16)) return AB_ERR_ARG;

@@ -131,4 +131,12 @@ cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, con
                            cudaStream_t st);
 size_t tc_corr_smem(int nks_max);
 
+// candidate polishing (optimize_accelcand for acceleration searches)
+struct PolishIn {
+    double r, z;
+    int numharm, pad;
+};
+cudaError_t launch_polish(const float2 *data, long long numdata, long long lobin, const PolishIn *in,
+                          int n, ab_polished *out, cudaStream_t st);
+
 }  // namespace ab
