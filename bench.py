@@ -149,6 +149,20 @@ def cpu_sample(name, threads, budget_s=20.0, first_block=200):
     return 1.0 / t_search, counts["cells"] / t_search, desc
 
 
+def cpu_polish_sample(fft, lobin, cands, threads, max_cands=16):
+    """Times the polishing oracle (optimize_accelcand restated, OpenMP over
+    candidates) on the first max_cands candidates; returns (ms per candidate,
+    description)."""
+    from oracle import pyoracle as po
+    sample = [(c[2], c[3], c[4]) for c in cands[:max_cands]]
+    if not sample:
+        return None, "no candidates"
+    t0 = time.perf_counter()
+    po.optimize_cands(fft, lobin, sample, nthreads=threads)
+    ms = (time.perf_counter() - t0) * 1e3 / len(sample)
+    return ms, f"polishing oracle, {threads} threads, {len(sample)} candidates"
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -259,6 +273,17 @@ def run_ours(args):
     e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device=f"cuda:{local}")
     nhits = len(ctx.last_hits()[0])
 
+    # ---- candidate polishing (optimize_accelcand) of the search's candidates ----
+    polish = None
+    if not obs.numw:
+        cl = ctx.search(obs, None, device_ptr=dev_fft.data_ptr())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.optimize_cands(obs, None, cl, device_ptr=dev_fft.data_ptr())
+        torch.cuda.synchronize()
+        polish = {"candidates": len(cl), "gpu_ms": (time.perf_counter() - t0) * 1e3,
+                  "what": "optimize_accelcand (harmonic polishing) of every candidate, device"}
+
     # ---- roofline of the dominant kernel (correlation) ----
     corr_ms_per_search = kms[2] / args.steps
     harm_ms = kms[3] / args.steps
@@ -326,6 +351,12 @@ def run_ours(args):
             sps, cps, desc = cpu_sample(name, os.cpu_count() or 1, budget_s=args.cpu_budget)
             line["cpu_baseline"] = {"value": cps, "unit": UNIT, "cores": os.cpu_count() or 1,
                                     "kind": "port", "sample": desc, "searches_per_s": sps}
+            if polish and polish["candidates"]:
+                pms, pdesc = cpu_polish_sample(fft, obs.lobin, cl, os.cpu_count() or 1)
+                polish["cpu_ms_per_candidate"] = pms
+                polish["cpu_sample"] = pdesc
+        if polish:
+            line["polish"] = polish
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
