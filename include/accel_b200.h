@@ -305,6 +305,22 @@ typedef struct {
 int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
                       const ab_cand *cands, long long n, ab_polished *out);
 
+/* The time-series input of create_accelobs (.dat files,
+ * src/accel_utils.c:1516-1563) on the device:
+ *   ab_realfft       realfft(data, n, -1) (src/fastffts.c:163-246): n float
+ *                    samples to n/2 bins, bin 0 = (DC, Nyquist); n/2 must be
+ *                    a power of two from 512 to 8192 or from 65536 to 2^26;
+ *   ab_deredden      deredden (src/misc_utils.c:912-1067) in place;
+ *   ab_series_to_fft both, with accelsearch's arguments (6, 200, 0.5/dt,
+ *                    n dt).
+ * *_on_device flags say whether each pointer is a device pointer. */
+int ab_realfft(ab_ctx *ctx, const float *series, long long n, int series_on_device, ab_fcomplex *out,
+               int out_on_device);
+int ab_deredden(ab_ctx *ctx, ab_fcomplex *fft, long long numbins, int startwidth, int endwidth,
+                double endfreq, double T, int fft_on_device);
+int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, int series_on_device,
+                     ab_fcomplex *out, int out_on_device);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -183,6 +183,12 @@ int    orc_optimize_cands(const orc_fcomplex *fft, long long numbins, long long 
                           const int *numharm, const double *r, const double *z, double *pows,
                           double *hirs, double *hizs, orc_rderivs *derivs, int nthreads);
 
+/* ---- time-series input path (series_oracle.c) -------------------------- */
+int   orc_realfft_forward(float *data, long n);
+float orc_invsqrtf(float x);
+long  orc_deredden(orc_fcomplex *fft, long numbins, int startwidth, int endwidth, double endfreq,
+                   double T);
+
 #ifdef __cplusplus
 }
 #endif

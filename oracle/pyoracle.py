@@ -319,3 +319,35 @@ def optimize_cands(fft, lobin, cands, nthreads=1):
         raise RuntimeError("orc_optimize_cands failed")
     return [dict(pows=pows[k, :nh[k]], hirs=hirs[k, :nh[k]], hizs=hizs[k, :nh[k]],
                  derivs=der[k, :nh[k]]) for k in range(n)]
+
+
+# ---- time-series input path (series_oracle.c) ------------------------------
+def _series_lib():
+    L = lib(64)
+    if not getattr(L, "_series_ready", False):
+        L.orc_realfft_forward.argtypes = [C.c_void_p, C.c_long]
+        L.orc_deredden.restype = C.c_long
+        L.orc_deredden.argtypes = [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orc_invsqrtf.restype = C.c_float
+        L.orc_invsqrtf.argtypes = [C.c_float]
+        L._series_ready = True
+    return L
+
+
+def realfft(series):
+    """realfft(data, n, -1): n/2 complex bins, bin 0 = (DC, Nyquist)."""
+    x = np.ascontiguousarray(series, dtype=np.float32).copy()
+    if _series_lib().orc_realfft_forward(x.ctypes.data, x.size):
+        raise ValueError("realfft needs a length divisible by 4")
+    return x.view(np.complex64)
+
+
+def deredden(fft, startwidth=6, endwidth=200, endfreq=None, T=1.0):
+    """deredden on a copy of fft (accelsearch uses 6, 200, Nyquist, N dt)."""
+    y = np.ascontiguousarray(fft, dtype=np.complex64).copy()
+    if endfreq is None:
+        endfreq = 1e300
+    n = _series_lib().orc_deredden(y.ctypes.data, y.size, startwidth, endwidth, endfreq, T)
+    if n < 0:
+        raise ValueError("deredden failed")
+    return y

@@ -34,7 +34,8 @@ EXPORTS = [
     "ab_ctx_set_corr_path", "ab_w_resp_halfwidth", "ab_set_transform_costs",
     "ab_get_transform_costs", "ab_autotune", "ab_add_ffdotpows_ptrs",
     "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
-    "ab_get_fourier_amplitudes", "ab_optimize_cands",
+    "ab_get_fourier_amplitudes", "ab_optimize_cands", "ab_realfft", "ab_deredden",
+    "ab_series_to_fft",
 ]
 
 COST_SLOTS = 16
@@ -142,6 +143,9 @@ def lib():
     L.ab_get_fourier_amplitudes.argtypes = [C.POINTER(Obs), vp, ll, i, vp]
     L.ab_optimize_cands.argtypes = [vp, C.POINTER(Obs), vp, i, C.POINTER(Cand), ll,
                                     C.POINTER(Polished)]
+    L.ab_realfft.argtypes = [vp, vp, ll, i, vp, i]
+    L.ab_deredden.argtypes = [vp, vp, ll, i, i, d, d, i]
+    L.ab_series_to_fft.argtypes = [vp, vp, ll, d, i, vp, i]
     L.ab_candlist_new.restype = vp
     L.ab_candlist_free.argtypes = [vp]
     L.ab_candlist_get.restype = ll
@@ -465,6 +469,28 @@ class Context:
             res.append(dict(pows=np.array(o.pows[:h]), hirs=np.array(o.hirs[:h]),
                             hizs=np.array(o.hizs[:h]), hiws=np.array(o.hiws[:h]), derivs=d))
         return res
+
+    def realfft(self, series):
+        """realfft(data, n, -1) on the device: n/2 complex bins."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        out = np.zeros(x.size // 2, np.complex64)
+        self._check(self.L.ab_realfft(self.ptr, x.ctypes.data, x.size, 0, out.ctypes.data, 0),
+                    "ab_realfft")
+        return out
+
+    def deredden(self, fft, startwidth=6, endwidth=200, endfreq=1e300, T=1.0):
+        y = np.ascontiguousarray(fft, dtype=np.complex64).copy()
+        self._check(self.L.ab_deredden(self.ptr, y.ctypes.data, y.size, startwidth, endwidth,
+                                       endfreq, T, 0), "ab_deredden")
+        return y
+
+    def series_to_fft(self, series, dt):
+        """accelsearch's .dat input: realfft, then deredden(6, 200, 0.5/dt, n dt)."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        out = np.zeros(x.size // 2, np.complex64)
+        self._check(self.L.ab_series_to_fft(self.ptr, x.ctypes.data, x.size, float(dt), 0,
+                                            out.ctypes.data, 0), "ab_series_to_fft")
+        return out
 
     def autotune(self):
         """Measure the correlation cost per transform length on this context's

@@ -82,6 +82,9 @@ struct ab_ctx {
     BankEntry *cur_bank = nullptr;
     int corr_path = AB_CORR_FFT;            // correlation path of searches and drop-ins
     DevBuf<float2> dtime;                   // normalised block data (tensor-core path)
+    DevBuf<float2> ser_in, ser_scr;         // time-series input path
+    DevBuf<int2> dered_blocks;
+    DevBuf<float> dered_means;
     DevBuf<TcItem> titems;
     std::vector<BankEntry *> bank_cache;
     unsigned long long bank_clock = 0;
@@ -841,6 +844,10 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->tmpb.release();
     ctx->errw.release();
     ctx->dtime.release();
+    ctx->ser_in.release();
+    ctx->ser_scr.release();
+    ctx->dered_blocks.release();
+    ctx->dered_means.release();
     ctx->titems.release();
     ctx->norms.release();
     ctx->keys.release();
@@ -996,6 +1003,110 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
     din.release();
     dout.release();
     if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "candidate polishing failed: %s", cudaGetErrorString(e));
+    return AB_OK;
+}
+
+// ---- time-series input path ------------------------------------------------
+static int realfft_dev(ab_ctx *ctx, const float *series, long long n, int series_on_device, float2 *dout)
+{
+    if (!realfft_supported(n))
+        return fail(ctx, AB_ERR_ARG, "realfft length %lld: need n/2 a power of two in 512..8192 or "
+                                     "65536..2^26", n);
+    const float *din = series;
+    if (!series_on_device) {
+        CK(ctx->ser_in.ensure((size_t) (n / 2)));
+        CK(cudaMemcpyAsync(ctx->ser_in.p, series, sizeof(float) * n, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        din = reinterpret_cast<const float *>(ctx->ser_in.p);
+    }
+    CK(ctx->ser_scr.ensure((size_t) (n / 2)));
+    CK(launch_realfft(din, dout, ctx->ser_scr.p, n, ctx->stream));
+    ctx->launches += 6;
+    return AB_OK;
+}
+
+static int deredden_dev(ab_ctx *ctx, float2 *dfft, long long numbins, int startwidth, int endwidth,
+                        double endfreq, double T)
+{
+    if (endwidth > AB_DERED_MAXW)
+        return fail(ctx, AB_ERR_ARG, "deredden endwidth %d above %d", endwidth, AB_DERED_MAXW);
+    long long nb = 0;
+    int rc = ab_dered_plan(numbins, startwidth, endwidth, endfreq, T, nullptr, 0, &nb);
+    if (rc) return fail(ctx, rc, "deredden: spectrum of %lld bins too short", numbins);
+    if (nb > (1LL << 30)) return fail(ctx, AB_ERR_ARG, "deredden: too many blocks");
+    std::vector<int> plan((size_t) (2 * nb));
+    ab_dered_plan(numbins, startwidth, endwidth, endfreq, T, plan.data(), nb, &nb);
+    CK(ctx->dered_blocks.ensure((size_t) nb));
+    CK(ctx->dered_means.ensure((size_t) nb));
+    CK(cudaMemcpyAsync(ctx->dered_blocks.p, plan.data(), sizeof(int) * 2 * nb, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(launch_deredden(dfft, ctx->dered_blocks.p, (int) nb, ctx->dered_means.p, ctx->stream));
+    ctx->launches += 2;
+    // the plan upload is pageable: wait before the vector goes away
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_realfft(ab_ctx *ctx, const float *series, long long n, int series_on_device, ab_fcomplex *out,
+               int out_on_device)
+{
+    if (!ctx || !series || !out) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    float2 *dout = reinterpret_cast<float2 *>(out);
+    if (!out_on_device) {
+        CK(ctx->fft.ensure((size_t) (n / 2)));
+        dout = ctx->fft.p;
+        ctx->fft_valid = false;
+    }
+    rc = realfft_dev(ctx, series, n, series_on_device, dout);
+    if (rc) return rc;
+    if (!out_on_device)
+        CK(cudaMemcpyAsync(out, dout, sizeof(float2) * (n / 2), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_deredden(ab_ctx *ctx, ab_fcomplex *fft, long long numbins, int startwidth, int endwidth,
+                double endfreq, double T, int fft_on_device)
+{
+    if (!ctx || !fft || numbins < 1) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    float2 *d = reinterpret_cast<float2 *>(fft);
+    if (!fft_on_device) {
+        CK(ctx->fft.ensure((size_t) numbins));
+        ctx->fft_valid = false;
+        d = ctx->fft.p;
+        CK(cudaMemcpyAsync(d, fft, sizeof(float2) * numbins, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    rc = deredden_dev(ctx, d, numbins, startwidth, endwidth, endfreq, T);
+    if (rc) return rc;
+    if (!fft_on_device)
+        CK(cudaMemcpyAsync(fft, d, sizeof(float2) * numbins, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, int series_on_device,
+                     ab_fcomplex *out, int out_on_device)
+{
+    if (!ctx || !series || !out || dt <= 0.0) return AB_ERR_ARG;
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    float2 *dout = reinterpret_cast<float2 *>(out);
+    if (!out_on_device) {
+        CK(ctx->fft.ensure((size_t) (n / 2)));
+        dout = ctx->fft.p;
+        ctx->fft_valid = false;
+    }
+    rc = realfft_dev(ctx, series, n, series_on_device, dout);
+    if (rc) return rc;
+    rc = deredden_dev(ctx, dout, n / 2, 6, 200, 0.5 / dt, dt * (double) n);
+    if (rc) return rc;
+    if (!out_on_device)
+        CK(cudaMemcpyAsync(out, dout, sizeof(float2) * (n / 2), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return AB_OK;
 }
 

@@ -286,7 +286,7 @@ __device__ __forceinline__ double2 dmul(double2 a, double2 b)
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-__device__ void fft64_inplace(double2 *x, int n, int log2n, const double2 *tw)
+static __device__ void fft64_inplace(double2 *x, int n, int log2n, const double2 *tw)
 {
     // bit reversal
     for (int i = threadIdx.x; i < n; i += blockDim.x) {

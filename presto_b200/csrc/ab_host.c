@@ -1020,4 +1020,40 @@ int ab_get_fourier_amplitudes(const ab_obs *obs, const ab_fcomplex *fft, long lo
     return AB_OK;
 }
 
+/* The block partition of deredden (src/misc_utils.c:912-1038): after bin 0,
+ * a first block of startwidth bins, then blocks of startwidth ln(binnum)
+ * bins (capped at endwidth, and endwidth once binnum / T reaches endfreq),
+ * the last one cut at the end of the spectrum.  blocks[2k] = first bin,
+ * blocks[2k+1] = length.  Returns AB_ERR_ARG when the spectrum is shorter
+ * than the first block, AB_ERR_OVERFLOW past maxblocks. */
+int ab_dered_plan(long long numbins, int startwidth, int endwidth, double endfreq, double T,
+                  int *blocks, long long maxblocks, long long *nblocks)
+{
+    if (!nblocks || startwidth < 1 || endwidth < startwidth || numbins < 1 + startwidth)
+        return AB_ERR_ARG;
+    const float Tf = (float) T;
+    long long rpos = 1, binnum = 1, nb = 0;
+    int bufflen = startwidth;
+    for (;;) {
+        long long n = numbins - rpos < bufflen ? numbins - rpos : bufflen;
+        if (n <= 0) break;
+        if (blocks) {
+            if (nb >= maxblocks) return AB_ERR_OVERFLOW;
+            blocks[2 * nb] = (int) rpos;
+            blocks[2 * nb + 1] = (int) n;
+        }
+        nb++;
+        rpos += n;
+        binnum += n;
+        if (nb == 1 || (float) binnum / Tf < endfreq) {
+            bufflen = (int) (startwidth * log((double) binnum));
+            if (bufflen > endwidth) bufflen = endwidth;
+        } else {
+            bufflen = endwidth;
+        }
+    }
+    *nblocks = nb;
+    return AB_OK;
+}
+
 long long ab_num_blocks_main(const ab_obs *obs) { return obs ? ab_num_blocks(obs) : -1; }

@@ -61,6 +61,8 @@ long long ab_num_blocks(const ab_obs *obs);
 long long ab_num_preblocks(const ab_obs *obs);
 
 int  ab_w_resp_halfwidth(double z, double w);
+int  ab_dered_plan(long long numbins, int startwidth, int endwidth, double endfreq, double T,
+                   int *blocks, long long maxblocks, long long *nblocks);
 int  ab_next_good_fftlen(int n);
 int  ab_fftlen_from_kernwidth(int kw);
 

@@ -139,4 +139,10 @@ struct PolishIn {
 cudaError_t launch_polish(const float2 *data, long long numdata, long long lobin, const PolishIn *in,
                           int n, ab_polished *out, cudaStream_t st);
 
+// time-series input path: realfft and deredden
+constexpr int AB_DERED_MAXW = 1024;     // longest de-reddening block
+bool realfft_supported(long long n);
+cudaError_t launch_realfft(const float *series, float2 *out, float2 *scratch, long long n, cudaStream_t st);
+cudaError_t launch_deredden(float2 *fft, const int2 *blocks, int nb, float *means, cudaStream_t st);
+
 }  // namespace ab

@@ -1,0 +1,248 @@
+// ab_series.cu -- the time-series input path of the search on the device:
+// create_accelobs' .dat branch (src/accel_utils.c:1516-1563), i.e. the
+// forward realfft (src/fastffts.c:163-246) and deredden(fft, n/2, 6, 200,
+// 0.5/dt, n dt) (src/misc_utils.c:912-1067).
+//
+// realfft: the n/2-point complex FFT of the samples taken in pairs, then the
+// untangling pass into n/2 bins with bin 0 = (DC, Nyquist).  The complex FFT
+// is one radix-16 Stockham transform in shared memory up to 8192 points, and
+// above that a four-step transform M = M1 M2: transpose, M2 transforms of
+// length M1 multiplied by exp(-2 pi i n2 k1 / M), transpose, M1 transforms of
+// length M2, transpose (each step one pass over HBM).
+//
+// deredden: the block partition depends only on bin indices (lengths
+// startwidth ln(bin) up to endwidth), so the host plans it; one CTA per block
+// takes the exact median of its powers, then one CTA per segment between
+// block midpoints scales the bins by the reference's interpolated
+// normalisation with its fast inverse square root, in float with explicit
+// rounding, so the same input gives the reference's bits.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "ab_fft.cuh"
+#include "ab_kernels.h"
+#include "ab_select.cuh"
+
+namespace ab {
+namespace {
+
+template <int L>
+__global__ void __launch_bounds__(FftShape<L>::CTA) k_fft_rows(const float2 *in, float2 *out,
+                                                             long long rows, long long twM)
+{
+    using SH = FftShape<L>;
+    extern __shared__ float2 fsm[];
+    const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
+    const long long row = (long long) blockIdx.x * SH::G + grp;
+    float2 *sm = fsm + grp * SH::SMEM;
+    FftTw<L, -1> tw;
+    tw.init(t);
+    const bool ok = row < rows;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = ok ? in[row * L + t + SH::NT * m] : make_float2(0.f, 0.f);
+    fft_run<L, -1>(v, sm, t, tw);
+    if (!ok) return;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const long long k = t + SH::NT * m;
+        float2 y = v[m];
+        if (twM) {
+            // W_M^{row k} = exp(-2 pi i row k / M), argument reduced mod M
+            double s, c;
+            sincospi(-2.0 * (double) ((row * k) % twM) / (double) twM, &s, &c);
+            const float cr = (float) c, ci = (float) s;
+            y = make_float2(y.x * cr - y.y * ci, y.x * ci + y.y * cr);
+        }
+        out[row * L + k] = y;
+    }
+}
+
+// out (C x R) = transpose of in (R x C), 32 x 32 tiles
+__global__ void __launch_bounds__(256) k_transpose(const float2 *in, float2 *out, int R, int C)
+{
+    __shared__ float2 tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int r = by + j, c = bx + threadIdx.x;
+        if (r < R && c < C) tile[j][threadIdx.x] = in[(long long) r * C + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int c = bx + j, r = by + threadIdx.x;
+        if (r < R && c < C) out[(long long) c * R + r] = tile[threadIdx.x][j];
+    }
+}
+
+// realfft's untangling (src/fastffts.c:195-229, forward): pair (il, n/2 - il)
+// per thread, sums of the float inputs in float as the reference, products
+// in FP64 without contraction, twiddles exp(-2 pi i il / n) computed directly.
+__global__ void k_untangle(float2 *c, long long n)
+{
+    const long long il = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nby2 = n >> 1, nby4 = n >> 2;
+    if (il == 0) {
+        const float t = c[0].x;
+        c[0] = make_float2(__fadd_rn(t, c[0].y), __fsub_rn(t, c[0].y));
+        return;
+    }
+    if (il > nby4) return;
+    const long long ih = nby2 - il;
+    const float2 a = c[il], b = c[ih];
+    double wi, wr;
+    sincospi(-2.0 * (double) il / (double) n, &wi, &wr);
+    const double h1r = 0.5 * (double) __fadd_rn(a.x, b.x), h1i = 0.5 * (double) __fsub_rn(a.y, b.y);
+    const double h2r = 0.5 * (double) __fadd_rn(a.y, b.y), h2i = -0.5 * (double) __fsub_rn(a.x, b.x);
+    const double h2rwr = __dmul_rn(h2r, wr), h2rwi = __dmul_rn(h2r, wi);
+    const double h2iwr = __dmul_rn(h2i, wr), h2iwi = __dmul_rn(h2i, wi);
+    const float2 lo = make_float2((float) __dsub_rn(__dadd_rn(h1r, h2rwr), h2iwi),
+                                  (float) __dadd_rn(__dadd_rn(h1i, h2iwr), h2rwi));
+    const float2 hi = make_float2((float) __dadd_rn(__dsub_rn(h1r, h2rwr), h2iwi),
+                                  (float) __dadd_rn(__dadd_rn(-h1i, h2iwr), h2rwi));
+    c[il] = lo;
+    c[ih] = hi;
+}
+
+// invsqrtf (src/misc_utils.c:291-302): the published fast inverse square
+// root, one Newton step, in float with explicit rounding.
+__device__ __forceinline__ float fast_invsqrtf(float x)
+{
+    const float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
+    const float t = __fmul_rn(__fmul_rn(__fmul_rn(0.5f, x), y), y);
+    return __fmul_rn(y, __fsub_rn(1.5f, t));
+}
+
+// Median of each block's powers / ln 2 (the block "mean" of deredden), one
+// 32-thread CTA per block.
+__global__ void __launch_bounds__(32) k_dered_means(const float2 *fft, const int2 *blocks, float *means)
+{
+    __shared__ float pw[AB_DERED_MAXW];
+    __shared__ unsigned hist[256], res[2];
+    const int2 b = blocks[blockIdx.x];
+    for (int i = threadIdx.x; i < b.y; i += blockDim.x) {
+        const float2 v = fft[b.x + i];
+        pw[i] = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+    }
+    __syncthreads();
+    const float lo = select_rank(pw, b.y, (b.y - 1) / 2, hist, res);
+    const float hi = (b.y & 1) ? lo : select_rank(pw, b.y, b.y / 2, hist, res);
+    if (threadIdx.x == 0) {
+        const float med = (b.y & 1) ? lo : (float) (0.5 * ((double) lo + (double) hi));
+        means[blockIdx.x] = (float) ((double) med / 0.69314718055994530942);
+    }
+}
+
+// Segment s of the output (one CTA each): s = 0 is the first half of block 0
+// (no slope); s = 1..nb-1 runs from the midpoint of block s-1 to the midpoint
+// of block s with the slope between their means; s = nb is the second half
+// of the last block with the last slope (1 when there is one block).  Bin 0
+// becomes (1, 0).
+__global__ void __launch_bounds__(256) k_dered_apply(float2 *fft, const int2 *blocks, const float *means,
+                                                    int nb)
+{
+    const int s = blockIdx.x;
+    long long start, end;
+    float mean_old, dslope = 1.0f;
+    if (s == 0) {
+        start = blocks[0].x;
+        end = start + blocks[0].y / 2;
+        mean_old = means[0];
+        if (threadIdx.x == 0) fft[0] = make_float2(1.0f, 0.0f);
+    } else {
+        const int k = s < nb ? s : nb - 1;              // slope of blocks k-1, k
+        if (k >= 1) {
+            const int2 b0 = blocks[k - 1], b1 = blocks[k];
+            dslope = (float) ((double) __fsub_rn(means[k], means[k - 1]) / (0.5 * (double) (b0.y + b1.y)));
+        }
+        const int2 bo = blocks[s - 1];
+        start = bo.x + bo.y / 2;
+        end = (s < nb) ? blocks[s].x + blocks[s].y / 2 : bo.x + bo.y;
+        mean_old = means[s - 1];
+    }
+    for (long long bin = start + threadIdx.x; bin < end; bin += blockDim.x) {
+        const float ii = (float) (bin - start);
+        const float norm = (s == 0) ? fast_invsqrtf(mean_old)
+                                    : fast_invsqrtf(__fadd_rn(mean_old, __fmul_rn(dslope, ii)));
+        const float2 v = fft[bin];
+        fft[bin] = make_float2(__fmul_rn(v.x, norm), __fmul_rn(v.y, norm));
+    }
+}
+
+template <int L>
+cudaError_t fft_rows_L(const float2 *in, float2 *out, long long rows, long long twM, cudaStream_t st)
+{
+    using SH = FftShape<L>;
+    const size_t smem = (size_t) SH::G * SH::SMEM * sizeof(float2);
+    cudaFuncSetAttribute(k_fft_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const long long grid = (rows + SH::G - 1) / SH::G;
+    k_fft_rows<L><<<(unsigned) grid, SH::CTA, smem, st>>>(in, out, rows, twM);
+    return cudaGetLastError();
+}
+
+cudaError_t fft_rows(int L, const float2 *in, float2 *out, long long rows, long long twM, cudaStream_t st)
+{
+    switch (L) {
+        case 256: return fft_rows_L<256>(in, out, rows, twM, st);
+        case 512: return fft_rows_L<512>(in, out, rows, twM, st);
+        case 1024: return fft_rows_L<1024>(in, out, rows, twM, st);
+        case 2048: return fft_rows_L<2048>(in, out, rows, twM, st);
+        case 4096: return fft_rows_L<4096>(in, out, rows, twM, st);
+        case 8192: return fft_rows_L<8192>(in, out, rows, twM, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t transpose(const float2 *in, float2 *out, int R, int C, cudaStream_t st)
+{
+    dim3 grid((C + 31) / 32, (R + 31) / 32), block(32, 8);
+    k_transpose<<<grid, block, 0, st>>>(in, out, R, C);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool realfft_supported(long long n)
+{
+    if (n < 1024 || n % 4) return false;
+    const long long M = n / 2;
+    if (M & (M - 1)) return false;
+    return M <= 8192 || (M >= (1 << 16) && M <= (1LL << 26));
+}
+
+cudaError_t launch_realfft(const float *series, float2 *out, float2 *scratch, long long n, cudaStream_t st)
+{
+    if (!realfft_supported(n)) return cudaErrorInvalidValue;
+    const long long M = n / 2;
+    const float2 *in = reinterpret_cast<const float2 *>(series);
+    cudaError_t e;
+    if (M <= 8192) {
+        e = fft_rows((int) M, in, out, 1, 0, st);
+    } else {
+        int m = 0;
+        while ((1LL << m) < M) m++;
+        const int M1 = 1 << (m / 2), M2 = (int) (M / M1);
+        // x[n1][n2] (M1 x M2) -> scratch[n2][n1]; rows of length M1 with the
+        // twiddle; -> out[k1][n2]; rows of length M2; -> scratch[k2][k1]; copy
+        e = transpose(in, scratch, M1, M2, st);
+        if (e == cudaSuccess) e = fft_rows(M1, scratch, scratch, M2, M, st);
+        if (e == cudaSuccess) e = transpose(scratch, out, M2, M1, st);
+        if (e == cudaSuccess) e = fft_rows(M2, out, out, M1, 0, st);
+        if (e == cudaSuccess) e = transpose(out, scratch, M1, M2, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, scratch, sizeof(float2) * M, cudaMemcpyDeviceToDevice, st);
+    }
+    if (e != cudaSuccess) return e;
+    const long long nthr = M / 2 + 1;
+    k_untangle<<<(unsigned) ((nthr + 255) / 256), 256, 0, st>>>(out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_deredden(float2 *fft, const int2 *blocks, int nb, float *means, cudaStream_t st)
+{
+    if (nb <= 0) return cudaErrorInvalidValue;
+    k_dered_means<<<nb, 32, 0, st>>>(fft, blocks, means);
+    k_dered_apply<<<nb + 1, 256, 0, st>>>(fft, blocks, means, nb);
+    return cudaGetLastError();
+}
+
+}  // namespace ab

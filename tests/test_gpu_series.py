@@ -1,0 +1,50 @@
+"""Device time-series input path against its oracle: realfft at lengths that
+take the single-transform, four-pass and four-step routes (FP32 on the device
+vs the oracle's FP64 FFT: within 2e-6 of the largest bin), deredden
+bit-exact on the same input, the whole chain within 1e-4 of the largest bin,
+and a search of the device's spectrum giving the same candidates as a search
+of the oracle's."""
+import numpy as np
+import pytest
+
+from presto_b200 import synth
+
+pytestmark = pytest.mark.gpu
+DT = 64e-6
+
+
+@pytest.mark.parametrize("n", [1 << 12, 1 << 14, 1 << 17, 1 << 21, 1 << 23])
+def test_device_realfft(ctx, oracle, n):
+    x = np.random.default_rng(n + 1).standard_normal(n).astype(np.float32)
+    dev = ctx.realfft(x)
+    orc = oracle.realfft(x)
+    scale = np.max(np.abs(orc))
+    assert np.max(np.abs(dev - orc)) <= 2e-6 * scale
+
+
+@pytest.mark.parametrize("numbins", [1 << 11, 1 << 16, 1 << 22])
+def test_device_deredden_bitexact(ctx, oracle, numbins):
+    rng = np.random.default_rng(numbins)
+    k = np.arange(1, numbins + 1)
+    spec = ((rng.standard_normal(numbins) + 1j * rng.standard_normal(numbins)) *
+            (1.0 + 3e3 / k)).astype(np.complex64)
+    T = 2 * numbins * DT
+    dev = ctx.deredden(spec, 6, 200, 0.5 / DT, T)
+    orc = oracle.deredden(spec, 6, 200, 0.5 / DT, T)
+    assert np.array_equal(dev.view(np.uint32), orc.view(np.uint32))
+
+
+def test_series_to_fft_and_search(ctx, ablib, oracle):
+    n = 1 << 20
+    series = synth.time_series(n, 1000, [dict(r=123.4 * n * DT, z=40.0, harms=[(0.05, 0.0)])])
+    series = np.asarray(series, np.float32)
+    dev = ctx.series_to_fft(series, DT)
+    orc = oracle.deredden(oracle.realfft(series), 6, 200, 0.5 / DT, n * DT)
+    assert np.max(np.abs(dev - orc)) <= 1e-4 * np.max(np.abs(orc))
+    obs = ablib.obs_init(ablib.make_params(n, DT, dev.size, zmax=200, numharm=8))
+    a = ctx.search(obs, dev)
+    b = ctx.search(obs, orc)
+    assert len(a) == len(b) and len(a) > 0
+    for x, y in zip(a, b):
+        assert x[2] == y[2] and abs(x[3] - y[3]) < 1e-3 and abs(x[4] - y[4]) < 1e-3
+        assert abs(x[0] - y[0]) <= 1e-3 * y[0]
