@@ -273,6 +273,25 @@ def run_ours(args):
     e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device=f"cuda:{local}")
     nhits = len(ctx.last_hits()[0])
 
+    # ---- the time-series input path (realfft + deredden) at this N ----
+    series = torch.randn(w["N"], dtype=torch.float32, device=f"cuda:{local}")
+    sfft = torch.empty(w["N"], dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(2):
+        ctx.L.ab_series_to_fft(ctx.ptr, series.data_ptr(), w["N"], w["dt"], 1, sfft.data_ptr(), 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        rcs = ctx.L.ab_series_to_fft(ctx.ptr, series.data_ptr(), w["N"], w["dt"], 1,
+                                     sfft.data_ptr(), 1)
+    torch.cuda.synchronize()
+    s_ms = (time.perf_counter() - t0) * 1e3 / reps
+    series_line = {"n": w["N"], "ms": s_ms, "status": int(rcs),
+                   "gb_per_s_algorithmic": 8.0 * w["N"] / (s_ms / 1e3) / 1e9,
+                   "what": "realfft + deredden(6, 200, Nyquist, N dt), device in and out, wall "
+                           "time per call including the host block plan"}
+    del series, sfft
+
     # ---- candidate polishing (optimize_accelcand) of the search's candidates ----
     polish = None
     if not obs.numw:
@@ -357,6 +376,7 @@ def run_ours(args):
                 polish["cpu_sample"] = pdesc
         if polish:
             line["polish"] = polish
+        line["series_to_fft"] = series_line
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
