@@ -438,7 +438,7 @@ static void build_tc_plan(const ab_ctx::TcBank &tb, const ab_bankset &bs, int nb
         const ab_bank &b = bs.b[tb.tiles[i].bank];
         for (int p = 0; p < 2; p++) {
             const int na = (b.numrs_max - p + 1) / 2;
-            for (int a0 = 0; a0 < na; a0 += 2 * TC_ATILE)
+            for (int a0 = 0; a0 < na; a0 += TC_ACC * TC_ATILE)
                 for (int bi = 0; bi < nblk; bi++) items.push_back(TcItem{bi, i, p, a0});
         }
     }

@@ -103,7 +103,8 @@ cudaError_t launch_tc_gemm(const float *A, const float *B, float *C, int N, int 
 // complex contraction in split BF16 (hi + lo) with FP32 accumulation.
 constexpr int TC_TILE_T = 128;          // templates per tile (MMA N = 2 per template)
 constexpr int TC_ATILE = 128;           // output positions per accumulator (MMA M)
-constexpr int TC_STAGES = 4;            // template K-step ring
+constexpr int TC_ACC = 1;               // accumulators (128 x 256 FP32, 256 TMEM columns) per CTA
+constexpr int TC_STAGES = 3;            // template K-step ring
 constexpr int TC_CHUNK = 64 * 2 * TC_TILE_T;   // bytes of one K step (hi + lo) at N = 256
 
 struct TcTile {                 // templates perm[t0 .. t0+nt) of one bank
@@ -112,7 +113,7 @@ struct TcTile {                 // templates perm[t0 .. t0+nt) of one bank
     long long off;              // byte offset of the packed operand (parity 0;
                                 // parity 1 follows after nks * 64 n bytes)
 };
-struct TcItem {                 // one CTA: positions a0 .. a0+255 of one parity
+struct TcItem {                 // one CTA: positions a0 .. a0 + 128 TC_ACC - 1 of one parity
     int bi, tile, parity, a0;
 };
 

@@ -163,10 +163,12 @@ cudaError_t launch_tc_pack(const ab_bank *b, const TcTile *tiles_dev, int ntiles
 
 size_t tc_corr_smem(int nks_max)
 {
-    // data rows (hi + lo) for two accumulators, then the template ring; at
-    // least ~116 KB so that one CTA (512 tensor-memory columns) runs per SM
-    size_t s = (size_t) (2 * TC_ATILE + 8 * nks_max) * 64 + (size_t) TC_STAGES * TC_CHUNK;
-    return s < 116 * 1024 ? 116 * 1024 : s;
+    // data rows (hi + lo) for the accumulators, then the template ring; at
+    // least ~77 KB so that at most two CTAs (256 tensor-memory columns each)
+    // share an SM: one's MMAs run while the other builds its data operand or
+    // drains its accumulator
+    size_t s = (size_t) (TC_ACC * TC_ATILE + 8 * nks_max) * 64 + (size_t) TC_STAGES * TC_CHUNK;
+    return s < 77 * 1024 ? 77 * 1024 : s;
 }
 
 struct TcArgs {
@@ -184,9 +186,9 @@ struct TcArgs {
     float *fullplane;
 };
 
-// One CTA = 128 threads: positions a0 .. a0 + 255 (two accumulators of 128
-// rows, 256 tensor-memory columns each) of one parity, against one template
-// tile.  Thread 0 streams the tile's K steps into a 4-stage ring with bulk
+// One CTA = 128 threads: positions a0 .. a0 + 128 TC_ACC - 1 (accumulators of
+// 128 rows, 256 tensor-memory columns each) of one parity, against one
+// template tile.  Thread 0 streams the tile's K steps into a ring with bulk
 // copies; thread 32 issues the MMAs (3 per accumulator and K step) and frees
 // each stage with a commit; all four warps then read the accumulators back
 // (warp w owns rows 32 w .. 32 w + 31) and store |y|^2.  The data operand is a
@@ -224,10 +226,10 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
         if (lim > b.numrs_max) lim = b.numrs_max;
     }
     const long long na_all = lim > p ? (lim - p + 1) / 2 : 0;
-    const long long na_l = na_all - it.a0 < 2 * TC_ATILE ? na_all - it.a0 : 2 * TC_ATILE;
+    const long long na_l = na_all - it.a0 < TC_ACC * TC_ATILE ? na_all - it.a0 : TC_ACC * TC_ATILE;
     if (na_l <= 0) return;                      // uniform over the CTA
     const int na = (int) na_l;
-    const int nat = na > TC_ATILE ? 2 : 1;
+    const int nat = (na + TC_ATILE - 1) / TC_ATILE;
     const int nrows = TC_ATILE * nat + 8 * tl.nks;
     unsigned char *h_hi = tsm, *h_lo = tsm + (size_t) nrows * 32;
     unsigned char *ring = tsm + (size_t) nrows * 64;
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
         *reinterpret_cast<__nv_bfloat162 *>(h_hi + o) = __halves2bfloat162(hr, hi_);
         *reinterpret_cast<__nv_bfloat162 *>(h_lo + o) = __halves2bfloat162(lr, li);
     }
-    if (threadIdx.x < 32) tc::tmem_alloc(&s_taddr, 512);
+    if (threadIdx.x < 32) tc::tmem_alloc(&s_taddr, 256 * TC_ACC);
     if (threadIdx.x == 0) {
         for (int i = 0; i < TC_STAGES; i++) {
             tc::mbar_init(&full[i], 1);
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (threadIdx.x < 32) tc::tmem_free(taddr, 512);
+    if (threadIdx.x < 32) tc::tmem_free(taddr, 256 * TC_ACC);
 }
 
 cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, const BlockBatch &bb,
