@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -60,8 +61,8 @@ struct ab_ctx {
     // template banks
     ab_bankset bs{};
     bool have_banks = false;
-    // template banks of recently used search geometries, least recently used
-    // evicted beyond kBankCache entries; tmpl points into the current one
+    // template banks: entries of the device-wide cache (shared by every
+    // context on the device); tmpl_p points into the current one
     // operands of the tensor-core correlation for one bank set: templates
     // sorted by half-width into tiles, packed split-BF16 taps per tile
     struct TcBank {
@@ -76,8 +77,10 @@ struct ab_ctx {
     struct BankEntry {
         ab_bankset bs;
         DevBuf<float2> tmpl;
-        unsigned long long used;
+        unsigned long long used = 0;
         TcBank tc;
+        int refs = 0;                       // contexts whose current banks these are
+        cudaEvent_t ready = nullptr;        // templates written (recorded by the builder)
     };
     BankEntry *cur_bank = nullptr;
     int corr_path = AB_CORR_FFT;            // correlation path of searches and drop-ins
@@ -86,8 +89,6 @@ struct ab_ctx {
     DevBuf<int2> dered_blocks;
     DevBuf<float> dered_means;
     DevBuf<TcItem> titems;
-    std::vector<BankEntry *> bank_cache;
-    unsigned long long bank_clock = 0;
     float2 *tmpl_p = nullptr;
     DevBuf<ab_bank> dbanks;
     DevBuf<double2> tw64;
@@ -183,7 +184,34 @@ static void harvest(ab_ctx *ctx)
 }
 
 // ---- banks ----------------------------------------------------------------
-constexpr int kBankCache = 4;
+// Template banks are shared by every context of a device: a request pool's
+// workers and plain contexts reuse the banks any of them built.  Entries are
+// reference-counted by the contexts whose current banks they are; a cache
+// miss builds into an unreferenced entry (least recently used, once the cache
+// holds kBankCache) after a device synchronisation, so no queued kernel of
+// any stream still reads it.  The builder records an event that later users
+// wait on.  Every search and drop-in returns with its stream drained, so a
+// context that moves to other banks leaves nothing in flight on the old ones.
+constexpr int kBankCache = 16;
+constexpr int kMaxDevices = 64;
+
+struct SharedBanks {
+    std::mutex mu;
+    std::vector<ab_ctx::BankEntry *> entries;
+    unsigned long long clock = 0;
+    int live = 0;                           // contexts alive on the device
+};
+static SharedBanks g_banks[kMaxDevices];
+
+static void free_entry(ab_ctx::BankEntry *e)
+{
+    e->tmpl.release();
+    e->tc.dtiles.release();
+    e->tc.dperm.release();
+    e->tc.pack.release();
+    if (e->ready) cudaEventDestroy(e->ready);
+    delete e;
+}
 
 static bool same_templates(const ab_bankset &a, const ab_bankset &b)
 {
@@ -197,8 +225,20 @@ static bool same_templates(const ab_bankset &a, const ab_bankset &b)
     return true;
 }
 
-// Makes the template banks of obs current: from the cache when a search with
-// the same template geometry ran before, else generated on the device.
+// The context's FP64 twiddle table, used by every response and template
+// transform; built on first use, since a context whose banks come from the
+// device-wide cache never generates templates itself.
+static int ensure_tw64(ab_ctx *ctx)
+{
+    if (ctx->tw64.n) return AB_OK;
+    CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
+    launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
+    CK(cudaGetLastError());
+    return AB_OK;
+}
+
+// Makes the template banks of obs current: from the device-wide cache when a
+// search with the same template geometry ran before, else built on the device.
 static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
 {
     ab_bankset nb;
@@ -206,29 +246,29 @@ static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
     if (rc) return fail(ctx, rc, "unsupported search geometry (FFT span above 4096 or "
                                  "circular wrap into valid cells)");
     CK(ctx->dbanks.ensure(AB_MAX_BANKS));
+    SharedBanks &sb = g_banks[ctx->device];
+    std::lock_guard<std::mutex> lock(sb.mu);
     ab_ctx::BankEntry *hit = nullptr;
-    for (auto *e : ctx->bank_cache)
-        if (same_templates(e->bs, nb)) hit = e;
-    if (!hit) {
-        if (ctx->tw64.n == 0) {
-            CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
-            launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
-            CK(cudaGetLastError());
-        }
-        if ((int) ctx->bank_cache.size() >= kBankCache) {
-            auto lru = std::min_element(ctx->bank_cache.begin(), ctx->bank_cache.end(),
-                                        [](ab_ctx::BankEntry *x, ab_ctx::BankEntry *y) {
-                                            return x->used < y->used;
-                                        });
-            // the evicted buffer may still be read by queued kernels
-            CK(cudaStreamSynchronize(ctx->stream));
-            hit = *lru;
+    for (auto *e : sb.entries)
+        if (e->bs.nbanks && same_templates(e->bs, nb)) hit = e;
+    if (hit) {
+        CK(cudaStreamWaitEvent(ctx->stream, hit->ready, 0));
+    } else {
+        if (int rc2 = ensure_tw64(ctx)) return rc2;
+        ab_ctx::BankEntry *victim = nullptr;
+        if ((int) sb.entries.size() >= kBankCache)
+            for (auto *e : sb.entries)
+                if (e->refs == 0 && e != ctx->cur_bank && (!victim || e->used < victim->used)) victim = e;
+        if (victim) {
+            CK(cudaDeviceSynchronize());    // nothing queued may still read it
+            hit = victim;
         } else {
             hit = new ab_ctx::BankEntry();
-            ctx->bank_cache.push_back(hit);
+            sb.entries.push_back(hit);
         }
         hit->bs.nbanks = 0;
         hit->tc.ready = false;
+        if (!hit->ready) CK(cudaEventCreateWithFlags(&hit->ready, cudaEventDisableTiming));
         CK(hit->tmpl.ensure((size_t) nb.tmpl_total));
         for (int i = 0; i < nb.nbanks; i++) {
             tick(ctx, 0, true);
@@ -239,10 +279,14 @@ static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
             if (e != cudaSuccess)
                 return fail(ctx, AB_ERR_CUDA, "template generation failed: %s", cudaGetErrorString(e));
         }
+        CK(cudaEventRecord(hit->ready, ctx->stream));
+        hit->bs = nb;
     }
-    // strides (numrs_max) follow the spectrum length; templates do not
-    hit->bs = nb;
-    hit->used = ++ctx->bank_clock;
+    if (ctx->cur_bank != hit) {
+        if (ctx->cur_bank) ctx->cur_bank->refs--;
+        hit->refs++;
+    }
+    hit->used = ++sb.clock;
     ctx->tmpl_p = hit->tmpl.p;
     ctx->cur_bank = hit;
     ctx->bs = nb;
@@ -347,8 +391,11 @@ static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
 // raw responses and the packed split-BF16 operand, built once per bank set.
 static int ensure_tc(ab_ctx *ctx)
 {
+    // the operands live in the shared bank entry: built once, under its lock
+    std::lock_guard<std::mutex> lock(g_banks[ctx->device].mu);
     ab_ctx::TcBank &tb = ctx->cur_bank->tc;
     if (tb.ready) return AB_OK;
+    if (int rc0 = ensure_tw64(ctx)) return rc0;
     const ab_bankset &bs = ctx->bs;
     tb.tiles.clear();
     tb.tile_lo.assign(1, 0);
@@ -800,7 +847,8 @@ int ab_ctx_create(int device, ab_ctx **out)
     if (!out) return AB_ERR_ARG;
     *out = nullptr;
     int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0 ||
+        device >= kMaxDevices)
         return AB_ERR_CUDA;
     ab_ctx *ctx = new ab_ctx();
     ctx->device = device;
@@ -813,6 +861,10 @@ int ab_ctx_create(int device, ab_ctx **out)
     cudaMemGetInfo(&fr, &tot);
     ctx->hbm_budget = (size_t) (0.85 * (double) fr);
     ctx->scratch_budget = std::min<size_t>(8ull << 30, ctx->hbm_budget / 4);
+    {
+        std::lock_guard<std::mutex> lock(g_banks[device].mu);
+        g_banks[device].live++;
+    }
     *out = ctx;
     return AB_OK;
 }
@@ -822,14 +874,17 @@ void ab_ctx_destroy(ab_ctx *ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (auto *e : ctx->bank_cache) {
-        e->tmpl.release();
-        e->tc.dtiles.release();
-        e->tc.dperm.release();
-        e->tc.pack.release();
-        delete e;
+    {
+        SharedBanks &sb = g_banks[ctx->device];
+        std::lock_guard<std::mutex> lock(sb.mu);
+        if (ctx->cur_bank) ctx->cur_bank->refs--;
+        ctx->cur_bank = nullptr;
+        if (--sb.live == 0) {
+            // the last context on the device: the cache goes with it
+            for (auto *e : sb.entries) free_entry(e);
+            sb.entries.clear();
+        }
     }
-    ctx->bank_cache.clear();
     ctx->dbanks.release();
     ctx->tw64.release();
     ctx->resp.release();
@@ -1498,10 +1553,7 @@ int ab_gen_response(ab_ctx *ctx, double roffset, int numbetween, double z, doubl
         return fail(ctx, AB_ERR_ARG, "bad response arguments (src/responses.c:344-360)");
     int rc = use_device(ctx);
     if (rc) return rc;
-    if (ctx->tw64.n == 0) {
-        CK(ctx->tw64.ensure((size_t) 1 << (kTwLog2 - 1)));
-        launch_twiddle64(ctx->tw64.p, 1 << kTwLog2, -1, ctx->stream);
-    }
+    if ((rc = ensure_tw64(ctx))) return rc;
     CK(ctx->resp.ensure((size_t) numkern));
     cudaError_t e = launch_response(roffset, numbetween, z, w, numkern, ctx->resp.p, ctx->tw64.p,
                                     kTwLog2, nullptr, ctx->stream);

@@ -786,6 +786,8 @@ static void *rs_worker(void *p)
     return NULL;
 }
 
+static int g_active_sorts = 0;
+
 /* Sorts keys[] (and the payload pl[] with it) in place by key. */
 static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long long n)
 {
@@ -800,8 +802,13 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     if (npasses == 0) return AB_OK;
     rs_ctx c;
     memset(&c, 0, sizeof(c));
+    /* sorts running at once (several contexts replaying, e.g. a request
+     * pool's workers) share the host's cores */
     long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-    c.nt = n < (1 << 16) ? 1 : (int) (ncpu > RS_MAXT ? RS_MAXT : (ncpu < 1 ? 1 : ncpu));
+    const int active = __atomic_add_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
+    long share = (ncpu < 1 ? 1 : ncpu) / active;
+    if (share < 1) share = 1;
+    c.nt = n < (1 << 16) ? 1 : (int) (share > RS_MAXT ? RS_MAXT : share);
     c.n = (size_t) n;
     c.npasses = npasses;
     c.ka = keys;
@@ -811,6 +818,7 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     c.hist = malloc(sizeof(size_t) * RS_BINS * (size_t) c.nt);
     if (!c.kb || !c.ob || !c.hist) {
         free(c.kb); free(c.ob); free(c.hist);
+        __atomic_sub_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
         return AB_ERR_NOMEM;
     }
     for (long long i = 0; i < n; i++) keys[i] -= kmin;
@@ -845,6 +853,7 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     }
     for (long long i = 0; i < n; i++) keys[i] += kmin;
     free(c.kb); free(c.ob); free(c.hist);
+    __atomic_sub_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
     return AB_OK;
 }
 
