@@ -285,13 +285,15 @@ int  ab_pool_reset_stats(ab_pool *pool);
  * K <= 256, N % 16 == 0, 16 <= N <= 256. */
 int ab_tc_gemm(ab_ctx *ctx, const float *A, const float *B, float *C, int N, int K, int split);
 
-/* Candidate polishing: optimize_accelcand (src/accel_utils.c:552-626) for
- * the candidates of an acceleration search (obs->numw == 0) with the
- * reference's default harmonic polishing (max_rz_arr_harmonics,
- * src/maximize_rz.c:173-228), every candidate at once on the device.  fft
- * holds obs->numbins bins (device pointer when fft_on_device != 0).  out[k]
- * receives the optimised r, z (and w = 0) of each harmonic of cands[k], its
- * raw power and its rderivs (include/presto.h:160-168). */
+/* Candidate polishing: optimize_accelcand (src/accel_utils.c:552-626) with
+ * the reference's default harmonic polishing, every candidate at once on the
+ * device: max_rz_arr_harmonics (src/maximize_rz.c:173-228) for an
+ * acceleration search (obs->numw == 0), max_rzw_arr_harmonics
+ * (src/maximize_rzw.c:81-191) for a jerk search (obs->numw > 0).  fft holds
+ * obs->numbins bins (device pointer when fft_on_device != 0).  out[k]
+ * receives the optimised r, z, w of each harmonic of cands[k], its raw power
+ * and its rderivs (include/presto.h:160-168).  AB_ERR_ARG for a jerk
+ * candidate whose responses need chirps above 2^17 samples. */
 #define AB_POLISH_MAX_HARM 32
 typedef struct {
     double pow, phs, dpow, dphs, d2pow, d2phs, locpow;

@@ -182,6 +182,18 @@ int    orc_optimize_accelcand(const orc_fcomplex *fft, long long numbins, long l
 int    orc_optimize_cands(const orc_fcomplex *fft, long long numbins, long long lobin, int ncand,
                           const int *numharm, const double *r, const double *z, double *pows,
                           double *hirs, double *hizs, orc_rderivs *derivs, int nthreads);
+/* jerk searches (numw > 0): max_rzw_arr / max_rzw_arr_harmonics */
+void   orc_rzw_vol_point(const orc_fcomplex *data, long numdata, long beginbin, int numbetween,
+                         long j, const orc_fcomplex *resp, int numkern, orc_fcomplex *out);
+double orc_max_rzw_arr(const orc_fcomplex *data, long numdata, double rin, double zin, double win,
+                       double *rout, double *zout, double *wout, orc_rderivs *derivs);
+void   orc_max_rzw_arr_harmonics(const orc_fcomplex *data, long numdata, int numharm, double rin,
+                                 double zin, double win, double *rout, double *zout, double *wout,
+                                 orc_rderivs *derivs, double *powers);
+int    orc_optimize_cands_w(const orc_fcomplex *fft, long long numbins, long long lobin, int ncand,
+                            int jerk, const int *numharm, const double *r, const double *z,
+                            const double *w, double *pows, double *hirs, double *hizs,
+                            double *hiws, orc_rderivs *derivs, int nthreads);
 
 /* ---- time-series input path (series_oracle.c) -------------------------- */
 int   orc_realfft_forward(float *data, long n);

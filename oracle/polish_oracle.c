@@ -385,3 +385,209 @@ int orc_optimize_cands(const orc_fcomplex *fft, long long numbins, long long lob
     (void) nthreads;
     return bad ? -1 : 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Jerk searches (numw > 0).
+ *
+ * corr_rzw_vol (src/rzwinterp.c:3-140) correlates the data window that
+ * starts kern_half_width bins below lobin, spread to numbetween points per
+ * bin, with each (z, w) response (numbetween points per bin, numkern =
+ * 2 numbetween kern_half_width) through FFTs of fftlen points, and keeps the
+ * uncontaminated outputs from chopbins = kern_half_width numbetween on
+ * (corr_complex, src/corr_routines.c:5-262; complex_corr_conv,
+ * src/correlations.c:3-60; chop_complex_ends).  Output j of that volume is,
+ * exactly, the direct sum
+ *     vol[j] = sum_i d[beginbin + i] conj(resp[numbetween i - j]),
+ *     0 <= numbetween i - j < numkern,  beginbin = lobin - kern_half_width,
+ * with d = 0 outside the spectrum: the complex amplitude at r = lobin +
+ * j / numbetween.  It is computed here as that sum in FP64.  For j < 0 or
+ * beyond the volume's numgoodbins the reference reads outside its result
+ * array (src/maximize_rzw.c:137 can form rind < 0 for harmonics just below
+ * the highest); the sum above gives the amplitude at that r instead. */
+void orc_rzw_vol_point(const orc_fcomplex *data, long numdata, long beginbin, int numbetween,
+                       long j, const orc_fcomplex *resp, int numkern, orc_fcomplex *out)
+{
+    const long i0 = j >= 0 ? (j + numbetween - 1) / numbetween : -((-j) / numbetween);
+    double ar = 0.0, ai = 0.0;
+    for (long i = i0; numbetween * i - j < numkern; i++) {
+        const long b = beginbin + i;
+        if (b < 0 || b >= numdata) continue;
+        const orc_fcomplex d = data[b], p = resp[numbetween * i - j];
+        ar += (double) d.r * p.r + (double) d.i * p.i;
+        ai += (double) d.i * p.r - (double) d.r * p.i;
+    }
+    out->r = (float) ar;
+    out->i = (float) ai;
+}
+
+#define P_ACCEL_DZ 2               /* include/accel.h:25 */
+#define P_ACCEL_DW 20              /* include/accel.h:29 */
+#define P_ACCEL_RDR 2              /* include/accel.h:23 */
+
+/* next2_to_n (src/misc_utils.c) */
+static long p_next2(long x)
+{
+    long n = 1;
+    while (n < x) n <<= 1;
+    return n;
+}
+
+/* The (numw x numz x numr) power volume of one harmonic, rind[] selecting
+ * the r outputs: vol_pow[(ii numz + jj) numr + kk] = |vol[rind[kk]]|^2 in
+ * float, as corr_rzw_vol's volume is read. */
+static void rzw_volume_powers(const orc_fcomplex *data, long numdata, int numbetween, long lobin,
+                              double zlo, double zhi, int numz, double wlo, double whi, int numw,
+                              const long *rind, int numr, float *vol_pow)
+{
+    const double dz = numz == 1 ? 0.0 : (zhi - zlo) / (numz - 1);
+    const double maxz = (fabs(zlo) < fabs(zhi)) ? zhi : zlo;
+    const double dw = numw == 1 ? 0.0 : (whi - wlo) / (numw - 1);
+    const double maxw = (fabs(wlo) < fabs(whi)) ? whi : wlo;
+    const int hw = orc_w_resp_halfwidth_acc(maxz, maxw, 0);
+    const int numkern = 2 * numbetween * hw;
+    orc_fcomplex *resp = (orc_fcomplex *) malloc(sizeof(orc_fcomplex) * (size_t) numkern);
+    for (int ii = 0; ii < numw; ii++)
+        for (int jj = 0; jj < numz; jj++) {
+            orc_gen_w_response(0.0, numbetween, zlo + jj * dz, wlo + ii * dw, numkern, resp);
+            for (int kk = 0; kk < numr; kk++) {
+                orc_fcomplex a;
+                orc_rzw_vol_point(data, numdata, lobin - hw, numbetween, rind[kk], resp, numkern, &a);
+                const float pr = a.r, pi = a.i;
+                vol_pow[((size_t) ii * numz + jj) * numr + kk] = pr * pr + pi * pi;
+            }
+        }
+    free(resp);
+}
+
+/* max_rzw_arr (src/maximize_rzw.c:3-52): the highest power of the volume
+ * oversampled 4x around (rin, zin, win), then derivatives there. */
+double orc_max_rzw_arr(const orc_fcomplex *data, long numdata, double rin, double zin, double win,
+                       double *rout, double *zout, double *wout, orc_rderivs *derivs)
+{
+    const float locpow = (float) orc_get_localpower3d(data, numdata, rin, zin, win);
+    const int interpfac = 4, startbin = (int) rin - 1;
+    const int numbetween = interpfac * P_ACCEL_RDR, numr = 3 * interpfac * P_ACCEL_RDR;
+    const int numz = 2 * interpfac + 1, numw = numz;
+    long rind[3 * 4 * P_ACCEL_RDR];
+    for (int kk = 0; kk < numr; kk++) rind[kk] = kk;
+    float *vp = (float *) malloc(sizeof(float) * (size_t) numw * numz * numr);
+    rzw_volume_powers(data, numdata, numbetween, startbin, zin - P_ACCEL_DZ, zin + P_ACCEL_DZ, numz,
+                      win - P_ACCEL_DW, win + P_ACCEL_DW, numw, rind, numr, vp);
+    float maxpow = 0.0f;
+    int wind = 0, zind = 0, rbest = 0;
+    for (int ii = 0; ii < numw; ii++)
+        for (int jj = 0; jj < numz; jj++)
+            for (int kk = 0; kk < numr; kk++) {
+                const float p = vp[((size_t) ii * numz + jj) * numr + kk];
+                if (p > maxpow) {
+                    maxpow = p;
+                    wind = ii;
+                    zind = jj;
+                    rbest = kk;
+                }
+            }
+    free(vp);
+    *rout = startbin + rbest * 0.5 / (double) interpfac;
+    *zout = zin - P_ACCEL_DZ + zind * P_ACCEL_DZ / (double) interpfac;
+    *wout = win - P_ACCEL_DW + wind * P_ACCEL_DW / (double) interpfac;
+    orc_get_derivs3d(data, numdata, *rout, *zout, *wout, locpow, derivs);
+    return maxpow;
+}
+
+/* max_rzw_arr_harmonics (src/maximize_rzw.c:81-191): per harmonic, from the
+ * highest, the volume over z and w in exact harmonic ratios (2 peak widths
+ * either side, 4x oversampled) and r on the highest harmonic's grid of 1/8
+ * bin, powers divided by the harmonic's local power and summed in float;
+ * the best cell gives (r, z, w) and each harmonic's derivatives there. */
+void orc_max_rzw_arr_harmonics(const orc_fcomplex *data, long numdata, int numharm, double rin,
+                               double zin, double win, double *rout, double *zout, double *wout,
+                               orc_rderivs *derivs, double *powers)
+{
+    const int interpfac = 4, numwid = 2;
+    const int numbetween = interpfac * P_ACCEL_RDR, numr = 3 * numbetween;
+    const int numz = 2 * numwid * interpfac + 1, numw = numz;
+    const double dr = 1.0 / (double) numbetween;
+    const size_t ncell = (size_t) numw * numz * numr;
+    float *powsum = (float *) calloc(ncell, sizeof(float));
+    float *vp = (float *) malloc(sizeof(float) * ncell);
+    long hhlobin = 0, rind[3 * 4 * P_ACCEL_RDR];
+    for (int hind = 0; hind < numharm; hind++) {
+        const int n = numharm - hind;
+        const double rh = rin * n, zh = zin * n, wh = win * n;
+        const double hfrac = n / (double) numharm;
+        const float locpow = (float) orc_get_localpower3d(data, numdata, rh, zh, wh);
+        double rh_int;
+        modf(rh, &rh_int);
+        const long lobin = (long) rh_int - 1;
+        if (hind == 0) hhlobin = lobin;
+        for (int kk = 0; kk < numr; kk++)
+            rind[kk] = (long) round(((hhlobin + kk * dr) * hfrac - lobin) * numbetween);
+        rzw_volume_powers(data, numdata, numbetween, lobin, zh - numwid * hfrac * P_ACCEL_DZ,
+                          zh + numwid * hfrac * P_ACCEL_DZ, numz, wh - numwid * hfrac * P_ACCEL_DW,
+                          wh + numwid * hfrac * P_ACCEL_DW, numw, rind, numr, vp);
+        for (size_t c = 0; c < ncell; c++) powsum[c] += vp[c] / locpow;
+    }
+    float maxpow = 0.0f;
+    int wind = 0, zind = 0, rbest = 0;
+    for (int ii = 0; ii < numw; ii++)
+        for (int jj = 0; jj < numz; jj++)
+            for (int kk = 0; kk < numr; kk++) {
+                const float p = powsum[((size_t) ii * numz + jj) * numr + kk];
+                if (p > maxpow) {
+                    maxpow = p;
+                    wind = ii;
+                    zind = jj;
+                    rbest = kk;
+                }
+            }
+    free(powsum);
+    free(vp);
+    const double nh = numharm;
+    *rout = (hhlobin + rbest * dr) / nh;
+    *zout = ((zin * nh) - numwid * P_ACCEL_DZ + zind * P_ACCEL_DZ / (double) interpfac) / nh;
+    *wout = ((win * nh) - numwid * P_ACCEL_DW + wind * P_ACCEL_DW / (double) interpfac) / nh;
+    for (int ii = 0; ii < numharm; ii++) {
+        const int hh = ii + 1;
+        const double rr = *rout * hh, zz = *zout * hh, ww = *wout * hh;
+        const float locpow = (float) orc_get_localpower3d(data, numdata, rr, zz, ww);
+        orc_get_derivs3d(data, numdata, rr, zz, ww, locpow, &derivs[ii]);
+        powers[ii] = derivs[ii].pow;
+    }
+}
+
+/* optimize_accelcand (src/accel_utils.c:552-626) with harmonic polishing for
+ * acceleration (jerk = 0) or jerk (jerk = 1) searches, OpenMP over
+ * candidates; per candidate k the outputs hold ORC_MAX_HARM entries from
+ * k * ORC_MAX_HARM. */
+int orc_optimize_cands_w(const orc_fcomplex *fft, long long numbins, long long lobin, int ncand,
+                         int jerk, const int *numharm, const double *r, const double *z,
+                         const double *w, double *pows, double *hirs, double *hizs, double *hiws,
+                         orc_rderivs *derivs, int nthreads)
+{
+    int bad = 0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1) reduction(| : bad)
+#endif
+    for (int k = 0; k < ncand; k++) {
+        const int nh = numharm[k];
+        const size_t o = (size_t) k * ORC_MAX_HARM;
+        if (nh < 1 || nh > ORC_MAX_HARM) {
+            bad = 1;
+            continue;
+        }
+        double ro, zo, wo = 0.0;
+        if (jerk)
+            orc_max_rzw_arr_harmonics(fft, (long) numbins, nh, r[k] - (double) lobin, z[k], w[k], &ro,
+                                      &zo, &wo, derivs + o, pows + o);
+        else
+            orc_max_rz_arr_harmonics(fft, (long) numbins, nh, r[k] - (double) lobin, z[k], &ro, &zo,
+                                     derivs + o, pows + o);
+        for (int ii = 0; ii < nh; ii++) {
+            hirs[o + ii] = (ro + (double) lobin) * (ii + 1);
+            hizs[o + ii] = zo * (ii + 1);
+            hiws[o + ii] = jerk ? wo * (ii + 1) : 0.0;
+        }
+    }
+    (void) nthreads;
+    return bad ? -1 : 0;
+}

@@ -267,6 +267,16 @@ def _polish_lib():
         L.orc_optimize_cands.argtypes = [vp, C.c_longlong, C.c_longlong, i, vp, vp, vp, vp, vp,
                                          vp, vp, i]
         L.orc_z_resp_halfwidth_acc.argtypes = [d, i]
+        L.orc_w_resp_halfwidth_acc.argtypes = [d, d, i]
+        L.orc_max_rzw_arr.restype = d
+        L.orc_max_rzw_arr.argtypes = [vp, C.c_long, d, d, d, C.POINTER(d), C.POINTER(d),
+                                      C.POINTER(d), C.POINTER(RDerivs)]
+        L.orc_max_rzw_arr_harmonics.argtypes = [vp, C.c_long, i, d, d, d, C.POINTER(d),
+                                                C.POINTER(d), C.POINTER(d), C.POINTER(RDerivs),
+                                                C.POINTER(d)]
+        L.orc_optimize_cands_w.argtypes = [vp, C.c_longlong, C.c_longlong, i, i, vp, vp, vp, vp,
+                                           vp, vp, vp, vp, vp, i]
+        L.orc_rzw_vol_point.argtypes = [vp, C.c_long, C.c_long, i, C.c_long, vp, i, vp]
         L._polish_ready = True
     return L
 
@@ -297,6 +307,63 @@ def max_rz_arr_harmonics(data, r, z, numharm):
     _polish_lib().orc_max_rz_arr_harmonics(data.ctypes.data, data.size, numharm, r, z,
                                            C.byref(ro), C.byref(zo), rds, pw)
     return ro.value, zo.value, list(rds), list(pw)
+
+
+def max_rzw_arr(data, r, z, w):
+    """(power, rout, zout, wout, rderivs) of the single-harmonic jerk maximiser."""
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    ro, zo, wo, rd = C.c_double(), C.c_double(), C.c_double(), RDerivs()
+    p = _polish_lib().orc_max_rzw_arr(data.ctypes.data, data.size, r, z, w, C.byref(ro),
+                                       C.byref(zo), C.byref(wo), C.byref(rd))
+    return p, ro.value, zo.value, wo.value, rd
+
+
+def max_rzw_arr_harmonics(data, r, z, w, numharm):
+    """(rout, zout, wout, [rderivs per harmonic], [power per harmonic])."""
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    ro, zo, wo = C.c_double(), C.c_double(), C.c_double()
+    rds = (RDerivs * numharm)()
+    pw = (C.c_double * numharm)()
+    _polish_lib().orc_max_rzw_arr_harmonics(data.ctypes.data, data.size, numharm, r, z, w,
+                                            C.byref(ro), C.byref(zo), C.byref(wo), rds, pw)
+    return ro.value, zo.value, wo.value, list(rds), list(pw)
+
+
+def rzw_vol_point(data, beginbin, numbetween, j, resp):
+    """One output of corr_rzw_vol's volume as the direct correlation sum."""
+    data = np.ascontiguousarray(data, dtype=np.complex64)
+    resp = np.ascontiguousarray(resp, dtype=np.complex64)
+    a = np.zeros(1, np.complex64)
+    _polish_lib().orc_rzw_vol_point(data.ctypes.data, data.size, int(beginbin), int(numbetween),
+                                    int(j), resp.ctypes.data, resp.size, a.ctypes.data)
+    return complex(a[0])
+
+
+def w_resp_halfwidth_acc(z, w, highacc=False):
+    return _polish_lib().orc_w_resp_halfwidth_acc(float(z), float(w), int(bool(highacc)))
+
+
+def optimize_cands_w(fft, lobin, cands, jerk, nthreads=1):
+    """optimize_accelcand for (numharm, r, z, w) candidates of an acceleration
+    (jerk False) or jerk (jerk True) search: per candidate a dict of pows,
+    hirs, hizs, hiws (numharm entries) and the derivs array."""
+    fft = np.ascontiguousarray(fft, dtype=np.complex64)
+    n = len(cands)
+    nh = np.array([c[0] for c in cands], np.int32)
+    r = np.array([c[1] for c in cands], np.float64)
+    z = np.array([c[2] for c in cands], np.float64)
+    w = np.array([c[3] if len(c) > 3 else 0.0 for c in cands], np.float64)
+    pows, hirs, hizs, hiws = (np.zeros((n, MAX_HARM)) for _ in range(4))
+    der = np.zeros((n, MAX_HARM, 7))
+    rc = _polish_lib().orc_optimize_cands_w(fft.ctypes.data, fft.size, int(lobin), n, int(bool(jerk)),
+                                            nh.ctypes.data, r.ctypes.data, z.ctypes.data,
+                                            w.ctypes.data, pows.ctypes.data, hirs.ctypes.data,
+                                            hizs.ctypes.data, hiws.ctypes.data, der.ctypes.data,
+                                            int(nthreads))
+    if rc:
+        raise RuntimeError("orc_optimize_cands_w failed")
+    return [dict(pows=pows[k, :nh[k]], hirs=hirs[k, :nh[k]], hizs=hizs[k, :nh[k]],
+                 hiws=hiws[k, :nh[k]], derivs=der[k, :nh[k]]) for k in range(n)]
 
 
 def optimize_cands(fft, lobin, cands, nthreads=1):

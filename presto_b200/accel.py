@@ -446,8 +446,9 @@ class Context:
 
     def optimize_cands(self, obs, fft, cands, device_ptr=None):
         """optimize_accelcand for (power, sigma, numharm, r, z, w) candidates of
-        an acceleration search: per candidate a dict of the harmonics'
-        optimised pows, hirs, hizs, hiws and derivs (numharm x 7)."""
+        an acceleration search (max_rz_arr_harmonics) or, when obs.numw > 0, a
+        jerk search (max_rzw_arr_harmonics): per candidate a dict of the
+        harmonics' optimised pows, hirs, hizs, hiws and derivs (numharm x 7)."""
         n = len(cands)
         if n == 0:
             return []

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libaccel_b200.so")
 BUILD = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu", "ab_pool.cu", "ab_tc.cu", "ab_polish.cu", "ab_series.cu"]
+CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu", "ab_pool.cu", "ab_tc.cu", "ab_polish.cu", "ab_polish_rzw.cu", "ab_series.cu"]
 C_SOURCES = ["ab_host.c"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]

@@ -92,6 +92,7 @@ struct ab_ctx {
     float2 *tmpl_p = nullptr;
     DevBuf<ab_bank> dbanks;
     DevBuf<double2> tw64;
+    DevBuf<double2> tw_rzw;                 // exp(-2 pi i m / 2^RZW_NMAX_LOG2), jerk polishing
     DevBuf<float2> resp;
 
     // spectrum, scratch, planes
@@ -887,6 +888,7 @@ void ab_ctx_destroy(ab_ctx *ctx)
     }
     ctx->dbanks.release();
     ctx->tw64.release();
+    ctx->tw_rzw.release();
     ctx->resp.release();
     ctx->fft.release();
     ctx->xhat.release();
@@ -1023,8 +1025,6 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
                       const ab_cand *cands, long long n, ab_polished *out)
 {
     if (!ctx || !obs || !fft || (n > 0 && (!cands || !out)) || n < 0) return AB_ERR_ARG;
-    if (obs->numw > 0)
-        return fail(ctx, AB_ERR_ARG, "polishing of jerk-search candidates is not available");
     if (n == 0) return AB_OK;
     if (n > (1 << 24)) return fail(ctx, AB_ERR_ARG, "too many candidates");
     int rc = use_device(ctx);
@@ -1038,12 +1038,25 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
         ctx->fft_valid = true;
         dfft = ctx->fft.p;
     }
-    std::vector<PolishIn> in((size_t) n);
-    for (long long k = 0; k < n; k++) {
+    for (long long k = 0; k < n; k++)
         if (cands[k].numharm < 1 || cands[k].numharm > AB_POLISH_MAX_HARM)
             return fail(ctx, AB_ERR_ARG, "candidate %lld has %d harmonics", k, cands[k].numharm);
-        in[k] = PolishIn{cands[k].r, cands[k].z, cands[k].numharm, 0};
+    if (obs->numw > 0) {
+        // jerk search: max_rzw_arr_harmonics (src/accel_utils.c:563-568)
+        if (ctx->tw_rzw.n == 0) {
+            CK(ctx->tw_rzw.ensure((size_t) 1 << (RZW_NMAX_LOG2 - 1)));
+            launch_twiddle64(ctx->tw_rzw.p, 1 << RZW_NMAX_LOG2, -1, ctx->stream);
+            CK(cudaGetLastError());
+        }
+        char msg[256] = {0};
+        const size_t budget = std::min<size_t>(ctx->scratch_budget, 1ull << 30);
+        rc = rzw_optimize(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p, budget,
+                          ctx->stream, msg, sizeof msg, &ctx->launches);
+        if (rc) return fail(ctx, rc, "%s", msg);
+        return AB_OK;
     }
+    std::vector<PolishIn> in((size_t) n);
+    for (long long k = 0; k < n; k++) in[k] = PolishIn{cands[k].r, cands[k].z, cands[k].numharm, 0};
     DevBuf<PolishIn> din;
     DevBuf<ab_polished> dout;
     cudaError_t e = din.ensure((size_t) n);

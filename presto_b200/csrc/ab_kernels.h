@@ -140,6 +140,42 @@ struct PolishIn {
 cudaError_t launch_polish(const float2 *data, long long numdata, long long lobin, const PolishIn *in,
                           int n, ab_polished *out, cudaStream_t st);
 
+// Jerk-search polishing: one job = one response (gen_z_response or
+// gen_w_response at roffset, numbetween nb, numkern points) and the
+// correlation outputs that use it, out_j[o] giving output o's offset j:
+//   amp[o] = sum_i d[beginbin + i] conj(resp[nb i - j]),  0 <= nb i - j < numkern,
+// d = 0 outside the spectrum.  mode 2 copies bin beginbin (rz_interp's exact
+// bin case).
+constexpr int RZW_PMAX = 4096;              // largest in-shared-memory FFT of a chirp phase
+constexpr int RZW_NMAX_LOG2 = 17;           // chirps up to 2^17 samples
+constexpr int RZW_VOL = 17 * 17 * 24;       // (w, z, r) cells of one harmonic's volume
+struct RzwJob {
+    double roffset, z, w;
+    long long beginbin;
+    long long resp_off;                     // float2 offset of the response in the scratch
+    long long acc_off;                      // double2 offset of the accumulator (npts > RZW_PMAX)
+    int mode;                               // 0: z response, 1: w response, 2: copy a bin
+    int nb, numkern, npts;
+    int nout, out_off;
+};
+cudaError_t launch_rzw_jobs(const RzwJob *jobs, int njobs, const float2 *data, long long numdata,
+                            const double2 *tw, float2 *resp, double2 *acc, const long long *out_j,
+                            float2 *out_amp, cudaStream_t st);
+// Per candidate c: harmonics' local powers from the amplitudes
+// amp[lp_off[c * 32 + h] ...] (lp_n of them; mean over NUMLOCPOWAVG = 20),
+// the float sum over harmonics of |vol|^2 / locpow in the reference's order
+// (volume amplitudes at amp[vol_off[c] + h * RZW_VOL + cell]) and the first
+// cell of the highest sum: best[c] = cell index.
+cudaError_t launch_rzw_sum(const float2 *amp, const int *numharm, const int *vol_off,
+                           const int *lp_off, const int *lp_n, int ncand, int *best, cudaStream_t st);
+// max_rzw_arr_harmonics for every candidate (host planning + the two
+// kernels above): data is the device spectrum of numdata bins, tw the FP64
+// table exp(-2 pi i m / 2^RZW_NMAX_LOG2), budget the response scratch per
+// launch.  Returns an AB_* code, with a message in err on failure.
+int rzw_optimize(const float2 *data, long long numdata, long long lobin, const ab_cand *cands,
+                 long long n, ab_polished *out, const double2 *tw, size_t budget, cudaStream_t st,
+                 char *err, size_t errlen, long long *launches);
+
 // time-series input path: realfft and deredden
 constexpr int AB_DERED_MAXW = 1024;     // longest de-reddening block
 bool realfft_supported(long long n);
