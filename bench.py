@@ -149,18 +149,19 @@ def cpu_sample(name, threads, budget_s=20.0, first_block=200):
     return 1.0 / t_search, counts["cells"] / t_search, desc
 
 
-def cpu_polish_sample(fft, lobin, cands, threads, max_cands=16):
+def cpu_polish_sample(fft, lobin, cands, threads, jerk=False, max_cands=16):
     """Times the polishing oracle (optimize_accelcand restated, OpenMP over
     candidates) on the first max_cands candidates; returns (ms per candidate,
     description)."""
     from oracle import pyoracle as po
-    sample = [(c[2], c[3], c[4]) for c in cands[:max_cands]]
+    sample = [(c[2], c[3], c[4], c[5]) for c in cands[:max_cands]]
     if not sample:
         return None, "no candidates"
     t0 = time.perf_counter()
-    po.optimize_cands(fft, lobin, sample, nthreads=threads)
+    po.optimize_cands_w(fft, lobin, sample, jerk=jerk, nthreads=threads)
     ms = (time.perf_counter() - t0) * 1e3 / len(sample)
-    return ms, f"polishing oracle, {threads} threads, {len(sample)} candidates"
+    what = "max_rzw_arr_harmonics" if jerk else "max_rz_arr_harmonics"
+    return ms, f"polishing oracle ({what}), {threads} threads, {len(sample)} candidates"
 
 
 def run_reference(args):
@@ -293,15 +294,14 @@ def run_ours(args):
     del series, sfft
 
     # ---- candidate polishing (optimize_accelcand) of the search's candidates ----
-    polish = None
-    if not obs.numw:
-        cl = ctx.search(obs, None, device_ptr=dev_fft.data_ptr())
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ctx.optimize_cands(obs, None, cl, device_ptr=dev_fft.data_ptr())
-        torch.cuda.synchronize()
-        polish = {"candidates": len(cl), "gpu_ms": (time.perf_counter() - t0) * 1e3,
-                  "what": "optimize_accelcand (harmonic polishing) of every candidate, device"}
+    cl = ctx.search(obs, None, device_ptr=dev_fft.data_ptr())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.optimize_cands(obs, None, cl, device_ptr=dev_fft.data_ptr())
+    torch.cuda.synchronize()
+    polish = {"candidates": len(cl), "gpu_ms": (time.perf_counter() - t0) * 1e3,
+              "what": "optimize_accelcand (harmonic polishing: max_rz%s_arr_harmonics) of every "
+                      "candidate, device" % ("w" if obs.numw else "")}
 
     # ---- roofline of the dominant kernel (correlation) ----
     corr_ms_per_search = kms[2] / args.steps
@@ -356,9 +356,12 @@ def run_ours(args):
                     "searches_per_s": args.steps * world / (e2e_ms / 1e3)},
             "roofline": roof,
             "roofline_harmsum": {"bound": "hbm", "kernel": "k_harmsum (sum + search)",
-                                 "achieved": counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9,
+                                 "achieved": counts["harmsum_min_bytes"] / (harm_ms / 1e3) / 1e9,
                                  "peak": hbm, "unit": "GB/s",
-                                 "frac": counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9 / hbm,
+                                 "frac": counts["harmsum_min_bytes"] / (harm_ms / 1e3) / 1e9 / hbm,
+                                 "bytes": "planes read once (the fused kernel's minimum)",
+                                 "unfused_equivalent_gbs":
+                                     counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9,
                                  "kernel_ms_per_search": harm_ms},
             "kernel_ms_per_search": {"templates": kms[0] / args.steps, "prep": kms[1] / args.steps,
                                      "corr": corr_ms_per_search, "harmsum": harm_ms},
@@ -371,7 +374,8 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": cps, "unit": UNIT, "cores": os.cpu_count() or 1,
                                     "kind": "port", "sample": desc, "searches_per_s": sps}
             if polish and polish["candidates"]:
-                pms, pdesc = cpu_polish_sample(fft, obs.lobin, cl, os.cpu_count() or 1)
+                pms, pdesc = cpu_polish_sample(fft, obs.lobin, cl, os.cpu_count() or 1,
+                                               jerk=bool(obs.numw))
                 polish["cpu_ms_per_candidate"] = pms
                 polish["cpu_sample"] = pdesc
         if polish:

@@ -272,8 +272,9 @@ def algorithmic_counts(obs):
     """Work of one search: f-fdot cells (numrs x numz x max(numw,1) per block
     per stage), correlation FLOPs at the reference FFT lengths
     (numz_h numw_h (5 L log2 L + 8 L) + 5 L log2 L per block and harmonic),
-    and harmonic-sum/search bytes when unfused (4 B per cell per stage read,
-    4 B per subharmonic gather, 8 B read-modify-write per later stage)."""
+    harmonic-sum/search bytes when unfused (4 B per cell per stage read,
+    4 B per subharmonic gather, 8 B read-modify-write per later stage) and
+    the bytes the fused sum + search cannot avoid reading."""
     import math
     nb = num_blocks(obs)
     nws = max(obs.numw, 1)
@@ -288,6 +289,12 @@ def algorithmic_counts(obs):
     flops *= nb
     sum_bytes = 4.0 * fund_cells * obs.numharmstages + 4.0 * fund_cells * (numharm - 1) + \
         8.0 * fund_cells * (obs.numharmstages - 1)
+    # what the fused sum + search must read: in standard mode every block's
+    # planes (all banks) once; in memory one value per harmonic per cell
+    if obs.inmem:
+        min_bytes = 4.0 * fund_cells * numharm
+    else:
+        min_bytes = 4.0 * nb * sum(b["nz"] * b["nw"] * b["numrs_max"] for b in bank_geometry(obs))
     # tensor-core path: 8 FLOPs per complex tap, numkern / 2 = 2 hw taps per
     # output cell, 3 products (hi.hi, hi.lo, lo.hi), numrs_max cells per row
     tc = 0.0
@@ -298,7 +305,7 @@ def algorithmic_counts(obs):
                    for wi in range(b["nw"]) for zi in range(b["nz"]))
         tc += 8.0 * 3.0 * taps * b["numrs_max"]
     return dict(blocks=nb, cells=cells, corr_flops=flops, harmsum_bytes=sum_bytes,
-                tc_flops=tc * nb)
+                harmsum_min_bytes=min_bytes, tc_flops=tc * nb)
 
 
 class Context:

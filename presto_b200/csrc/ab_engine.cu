@@ -109,15 +109,18 @@ struct ab_ctx {
     DevBuf<float> tmpa, tmpb;
     DevBuf<unsigned> errw;                   // device error word
 
-    // hits: two sets so that the host replays one batch while the device
-    // fills the other
-    DevBuf<unsigned long long> keys, keys2;
-    DevBuf<float> pows, pows2;
-    DevBuf<unsigned int> count, count2;
-    DevBuf<float> sigs, sigs2;
+    // hits: a ring of kHitSets sets, so that the device runs up to
+    // kHitSets - 1 batches ahead of the host's replay (batches that hold a
+    // strong signal cross the threshold millions of times and replay slowly);
+    // set 0 is keys/pows/sigs/count, set i > 0 the (i - 1)th of the _x arrays
+    static constexpr int kHitSets = 4;
+    DevBuf<unsigned long long> keys, keys_x[kHitSets - 1];
+    DevBuf<float> pows, pows_x[kHitSets - 1];
+    DevBuf<unsigned int> count, count_x[kHitSets - 1];
+    DevBuf<float> sigs, sigs_x[kHitSets - 1];
     std::vector<float> hsigs;
-    unsigned *hcount = nullptr;              // pinned [2]
-    cudaEvent_t batch_done[2] = {nullptr, nullptr};
+    unsigned *hcount = nullptr;              // pinned [kHitSets]
+    cudaEvent_t batch_done[kHitSets] = {};
     cudaStream_t cstream = nullptr;          // device->host copies of hits
     unsigned int hit_cap = 1u << 22;
     std::vector<unsigned long long> hkeys;
@@ -528,12 +531,16 @@ static int ensure_hitsets(ab_ctx *ctx)
     CK(ctx->pows.ensure(ctx->hit_cap));
     CK(ctx->sigs.ensure(ctx->hit_cap));
     CK(ctx->count.ensure(1));
-    CK(ctx->keys2.ensure(ctx->hit_cap));
-    CK(ctx->pows2.ensure(ctx->hit_cap));
-    CK(ctx->sigs2.ensure(ctx->hit_cap));
-    CK(ctx->count2.ensure(1));
-    if (!ctx->hcount) CK(cudaHostAlloc((void **) &ctx->hcount, 2 * sizeof(unsigned), cudaHostAllocDefault));
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < ab_ctx::kHitSets - 1; i++) {
+        CK(ctx->keys_x[i].ensure(ctx->hit_cap));
+        CK(ctx->pows_x[i].ensure(ctx->hit_cap));
+        CK(ctx->sigs_x[i].ensure(ctx->hit_cap));
+        CK(ctx->count_x[i].ensure(1));
+    }
+    if (!ctx->hcount)
+        CK(cudaHostAlloc((void **) &ctx->hcount, ab_ctx::kHitSets * sizeof(unsigned),
+                         cudaHostAllocDefault));
+    for (int i = 0; i < ab_ctx::kHitSets; i++)
         if (!ctx->batch_done[i]) CK(cudaEventCreateWithFlags(&ctx->batch_done[i], cudaEventDisableTiming));
     if (!ctx->cstream) CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
     return AB_OK;
@@ -541,8 +548,9 @@ static int ensure_hitsets(ab_ctx *ctx)
 
 static HitSet hitset(ab_ctx *ctx, int i)
 {
-    return i == 0 ? HitSet{ctx->keys.p, ctx->pows.p, ctx->sigs.p, ctx->count.p}
-                  : HitSet{ctx->keys2.p, ctx->pows2.p, ctx->sigs2.p, ctx->count2.p};
+    if (i == 0) return HitSet{ctx->keys.p, ctx->pows.p, ctx->sigs.p, ctx->count.p};
+    return HitSet{ctx->keys_x[i - 1].p, ctx->pows_x[i - 1].p, ctx->sigs_x[i - 1].p,
+                  ctx->count_x[i - 1].p};
 }
 
 // After the launches that fill hit set i: sigma of every hit, the count to
@@ -707,7 +715,8 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     }
 
     // standard mode: batches of blocks, each correlated for every bank, then
-    // summed; hit sets alternate so the host replays batch k-1 meanwhile
+    // summed; hit sets rotate so the host replays batch k - (kHitSets - 1)
+    // meanwhile
     const bool tcp = ctx->corr_path == AB_CORR_TC_SPLIT_BF16;
     if (tcp) {
         rc = ensure_tc(ctx);
@@ -752,7 +761,7 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     int k = 0;
     for (long long b0 = first; b0 < first + count; b0 += B, k++) {
         int nb = (int) std::min<long long>(B, first + count - b0);
-        const int set = k & 1;
+        const int set = k % ab_ctx::kHitSets;
         HitSet h = hitset(ctx, set);
         CK(cudaMemsetAsync(h.count, 0, sizeof(unsigned), ctx->stream));
         BlockBatch bb{ctx->startr.p + b0, b0, nb, 0};
@@ -787,12 +796,16 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
         rc = close_hitset(ctx, obs, set);
         if (rc) return rc;
-        if (k > 0) {
-            rc = drain_hitset(ctx, obs, set ^ 1, list, replay_ms);
+        if (k >= ab_ctx::kHitSets - 1) {
+            rc = drain_hitset(ctx, obs, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, list,
+                              replay_ms);
             if (rc) return rc;
         }
     }
-    if (k > 0) return drain_hitset(ctx, obs, (k - 1) & 1, list, replay_ms);
+    for (int d = std::max(0, k - (ab_ctx::kHitSets - 1)); d < k; d++) {
+        rc = drain_hitset(ctx, obs, d % ab_ctx::kHitSets, list, replay_ms);
+        if (rc) return rc;
+    }
     return AB_OK;
 }
 
@@ -911,12 +924,14 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->pows.release();
     ctx->count.release();
     ctx->sigs.release();
-    ctx->keys2.release();
-    ctx->pows2.release();
-    ctx->count2.release();
-    ctx->sigs2.release();
+    for (int i = 0; i < ab_ctx::kHitSets - 1; i++) {
+        ctx->keys_x[i].release();
+        ctx->pows_x[i].release();
+        ctx->count_x[i].release();
+        ctx->sigs_x[i].release();
+    }
     if (ctx->hcount) cudaFreeHost(ctx->hcount);
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < ab_ctx::kHitSets; i++)
         if (ctx->batch_done[i]) cudaEventDestroy(ctx->batch_done[i]);
     if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
     for (auto e : ctx->evpool) cudaEventDestroy(e);
