@@ -15,8 +15,17 @@
 
 namespace ab {
 
-__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex arithmetic on sm_100's paired FP32 instructions (FADD2 / FMUL2 /
+// FFMA2: both components in one instruction, each rounded as the scalar
+// operation would be).  a - b is fma(b, -1, a), exactly the rounded
+// difference; the products keep the scalar forms' roundings:
+//   a * b       = (fma(a.x, b.x, -(a.y b.y)), fma(a.x, b.y, a.y b.x))
+//   a * conj(b) = (fma(a.x, b.x, a.y b.y),    fma(a.y, b.x, -(a.x b.y)))
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b)
+{
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
@@ -51,14 +60,14 @@ template <int S, int M> __device__ __forceinline__ float2 tw16(float2 a)
         // (+-1 +- i) H
         constexpr float cr = (m == 2 || m == 14) ? H : -H;
         constexpr float ci = ((m == 2 || m == 6) ? H : -H) * (S < 0 ? -1.f : 1.f);
-        return make_float2(fmaf(a.x, cr, -a.y * ci), fmaf(a.x, ci, a.y * cr));
+        return cmul(a, make_float2(cr, ci));
     } else {
         constexpr float cr = (m == 1 || m == 15) ? C1 : (m == 3 || m == 13) ? S1
                            : (m == 5 || m == 11) ? -S1 : -C1;
         constexpr float si = (m == 1 || m == 7) ? S1 : (m == 3 || m == 5) ? C1
                            : (m == 9 || m == 15) ? -S1 : -C1;
         constexpr float ci = si * (S < 0 ? -1.f : 1.f);
-        return make_float2(fmaf(a.x, cr, -a.y * ci), fmaf(a.x, ci, a.y * cr));
+        return cmul(a, make_float2(cr, ci));
     }
 }
 
@@ -71,11 +80,17 @@ template <int S> __device__ __forceinline__ void dft2(float2 *x)
 
 template <int S> __device__ __forceinline__ void dft4v(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
 {
-    float2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_i<S>(a1 - a3);
+    const float2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, d = a1 - a3;
     a0 = t0 + t2;
     a2 = t0 - t2;
-    a1 = t1 + t3;
-    a3 = t1 - t3;
+    // t1 +- (S i) d: cross-component sums, as scalar operations
+    if constexpr (S < 0) {
+        a1 = make_float2(t1.x + d.y, t1.y - d.x);
+        a3 = make_float2(t1.x - d.y, t1.y + d.x);
+    } else {
+        a1 = make_float2(t1.x - d.y, t1.y + d.x);
+        a3 = make_float2(t1.x + d.y, t1.y - d.x);
+    }
 }
 
 template <int S> __device__ __forceinline__ void dft4(float2 *x) { dft4v<S>(x[0], x[1], x[2], x[3]); }
@@ -133,11 +148,16 @@ template <int L> struct FftShape {
     static constexpr int NT = L / 16;                 // threads per transform
     static constexpr int CTA = NT > 256 ? NT : 256;   // threads per CTA
     static constexpr int G = CTA / NT;                // transforms per CTA
+    static constexpr int MINB = CTA <= 256 ? 2 : 1;   // CTAs per SM the register cap keeps
     static constexpr int R3 = L <= 4096 ? L / 256 : 16;   // radix of the third pass (1: none)
     static constexpr int R4 = L > 4096 ? L / 4096 : 1;    // radix of the fourth pass (1: none)
     static constexpr int NB3 = (R3 > 1) ? 16 / R3 : 0;
     static constexpr int NB4 = (R4 > 1) ? 16 / R4 : 0;
     static constexpr int SMEM = L + L / 16;           // padded float2 per transform
+    // shared-memory exchanges per transform (passes - 1); with exactly two,
+    // a second buffer removes the barrier after each read-back (DBUF)
+    static constexpr int NEX = 1 + (R3 > 1 ? 1 : 0) + (R4 > 1 ? 1 : 0);
+    static constexpr bool DBUF = NEX == 2;
     static_assert(L >= 256 && L <= 8192 && (L & (L - 1)) == 0, "FFT length");
 };
 
@@ -226,7 +246,9 @@ __device__ __forceinline__ void apply_tw_pass(float2 *x, int b, int t, const Fft
 // One Stockham pass.  v holds x[t + NT m]; results of a non-final pass go
 // through shared memory and come back in the same strided layout.
 // PASS: 1 to 4 (selects the twiddles).  TW: FftTw (register bases).
-template <int L, int R, int LS, int S, bool LAST, int PASS, class TW>
+// TRAIL: barrier after the read-back (not needed when the next exchange
+// writes another buffer).
+template <int L, int R, int LS, int S, bool LAST, int PASS, bool TRAIL = true, class TW>
 __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, const TW &tw)
 {
     constexpr int NT = L / 16, NB = 16 / R;
@@ -252,16 +274,29 @@ __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2 *sm, int t, con
         __syncthreads();
 #pragma unroll
         for (int m = 0; m < 16; m++) v[m] = sm[pad16(t + NT * m)];
-        __syncthreads();
+        if constexpr (TRAIL) __syncthreads();
     }
 }
 
 // Full transform of the group's data, in place in v.  Must be called by all
-// threads of the CTA (it contains __syncthreads).
+// threads of the CTA (it contains __syncthreads).  With sm2 (a second
+// buffer of SMEM float2, only where FftShape<L>::DBUF) the two exchanges use
+// sm then sm2 and skip the barrier after each read-back: a buffer is written
+// again only after every thread has passed the barrier of the other
+// exchange, which follows its last read of that buffer.
 template <int L, int S, class TW>
-__device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const TW &tw)
+__device__ __forceinline__ void fft_run(float2 (&v)[16], float2 *sm, int t, const TW &tw,
+                                        float2 *sm2 = nullptr)
 {
     using SH = FftShape<L>;
+    if constexpr (SH::DBUF) {
+        if (sm2) {
+            fft_pass<L, 16, 1, S, false, 1, false>(v, sm, t, tw);
+            fft_pass<L, 16, 16, S, false, 2, false>(v, sm2, t, tw);
+            fft_pass<L, SH::R3, 256, S, true, 3>(v, sm, t, tw);
+            return;
+        }
+    }
     if constexpr (SH::R4 > 1) {
         fft_pass<L, 16, 1, S, false, 1>(v, sm, t, tw);
         fft_pass<L, 16, 16, S, false, 2>(v, sm, t, tw);

@@ -483,7 +483,7 @@ cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host
 // the data spectrum is staged in shared memory once, templates stream from
 // L2 (each template row is read by every block of the batch).
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::CTA) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
+__global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
                                               const CorrItem *items, const float2 *xhat,
                                               long long xhat_per_block, const float2 *tmpl,
                                               float *planes, long long plane_per_block,
@@ -498,10 +498,14 @@ __global__ void __launch_bounds__(FftShape<L>::CTA) k_corr(const ab_bank *banks,
     const CorrItem it = items[blockIdx.x];              // it.bi: transform unit
     const ab_bank b = banks[it.bank];
     const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
+    // exchange buffers: one per transform group, a second set where the
+    // transform has exactly two exchanges (fewer barriers)
+    constexpr int NBUF = SH::DBUF ? 2 : 1;
     float2 *sm = fsm + L / 2 + grp * SH::SMEM;
+    float2 *sm2 = SH::DBUF ? fsm + L / 2 + (SH::G + grp) * SH::SMEM : nullptr;
     // column -> block map of a superblock: low / high nibble = first / second
     // block whose sub-plane holds the column (15 = none)
-    unsigned char *cmap = reinterpret_cast<unsigned char *>(fsm + L / 2 + SH::G * SH::SMEM);
+    unsigned char *cmap = reinterpret_cast<unsigned char *>(fsm + L / 2 + NBUF * SH::G * SH::SMEM);
     const float2 *xsrc = xhat + (long long) it.bi * xhat_per_block + b.xhat_off;
     for (int i = threadIdx.x; i < L / 2; i += blockDim.x) xs[i] = xsrc[i];
     const bool sb = !sc.inmem && sc.superblocks && b.sbm > 1;
@@ -555,7 +559,7 @@ __global__ void __launch_bounds__(FftShape<L>::CTA) k_corr(const ab_bank *banks,
 #pragma unroll
             for (int m = 0; m < 16; m++) v[m] = make_float2(0.f, 0.f);
         }
-        fft_run<L, 1>(v, sm, t, tw);
+        fft_run<L, 1>(v, sm, t, tw, sm2);
         if (valid && sb) {
             const long long row = (long long) tl * b.numrs_max;
 #pragma unroll
@@ -606,7 +610,8 @@ cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
 #define AB_CORR_CASE(N)                                                                       \
     case N: {                                                                                 \
         using SH = FftShape<N>;                                                               \
-        const size_t smem = (size_t) (N / 2 + SH::G * SH::SMEM) * sizeof(float2) + (size_t) N; \
+        const size_t smem = (size_t) (N / 2 + (SH::DBUF ? 2 : 1) * SH::G * SH::SMEM) *      \
+                            sizeof(float2) + (size_t) N;                                     \
         cudaFuncSetAttribute(k_corr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
         k_corr<N><<<nitems, SH::CTA, smem, st>>>(banks_dev, sc, bb, items, xhat, xhat_per_block, \
                                                  tmpl, planes, plane_per_block, fullplane);   \
