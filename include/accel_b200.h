@@ -307,6 +307,36 @@ typedef struct {
 int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on_device,
                       const ab_cand *cands, long long n, ab_polished *out);
 
+/* Candidate properties (Middleditch, Deich & Kulkarni 1993) and the .cand
+ * file.  ab_fourierprops has fourierprops' members and layout
+ * (include/presto.h:170-188): the reference's .cand file is an array of it
+ * written raw (src/accelsearch.c:282-284), so an array of n of these is that
+ * file's content.  ab_rzwerrs is rzwerrs (include/presto.h:233-246).
+ *   ab_calc_props    calc_props (src/characteristics.c:195-264); AB_ERR_ARG
+ *                    where the reference exits (|pow| or locpow < 1e-14);
+ *   ab_calc_rzwerrs  calc_rzwerrs (src/characteristics.c:353-392); AB_ERR_ARG
+ *                    for T <= 0;
+ *   ab_cand_props    per polished candidate, the fundamental's properties
+ *                    at the search's (r, z, w) with the reference's error
+ *                    overrides ACCEL_DR, ACCEL_DZ, ACCEL_DW / numharm
+ *                    (src/accelsearch.c:261-272). */
+typedef struct {
+    double r;
+    float rerr;
+    double z;
+    float zerr;
+    double w;
+    float werr;
+    float pow, powerr, sig, rawpow, phs, phserr, cen, cenerr, pur, purerr, locpow;
+} ab_fourierprops;
+typedef struct {
+    double p, pd, pdd, f, fd, fdd;
+    float perr, pderr, pdderr, ferr, fderr, fdderr;
+} ab_rzwerrs;
+int ab_calc_props(const ab_rderivs *d, double r, double z, double w, ab_fourierprops *out);
+int ab_calc_rzwerrs(const ab_fourierprops *props, double T, ab_rzwerrs *out);
+int ab_cand_props(const ab_cand *cands, const ab_polished *pol, long long n, ab_fourierprops *out);
+
 /* The time-series input of create_accelobs (.dat files,
  * src/accel_utils.c:1516-1563) on the device:
  *   ab_realfft       realfft(data, n, -1) (src/fastffts.c:163-246): n float

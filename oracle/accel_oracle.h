@@ -171,6 +171,11 @@ double orc_get_localpower3d(const orc_fcomplex *data, long numdata, double r, do
 void   orc_get_derivs3d(const orc_fcomplex *data, long numdata, double r, double z, double w,
                         double localpower, orc_rderivs *res);
 int    orc_calc_props(const orc_rderivs *d, double r, double z, double w, orc_fourierprops *o);
+typedef struct {                 /* rzwerrs, include/presto.h:233-246 */
+    double p, pd, pdd, f, fd, fdd;
+    float perr, pderr, pdderr, ferr, fderr, fdderr;
+} orc_rzwerrs;
+int    orc_calc_rzwerrs(const orc_fourierprops *p, double T, orc_rzwerrs *o);
 double orc_max_rz_arr(const orc_fcomplex *data, long numdata, double rin, double zin,
                       double *rout, double *zout, orc_rderivs *derivs);
 void   orc_max_rz_arr_harmonics(const orc_fcomplex *data, long numdata, int numharm, double rin,

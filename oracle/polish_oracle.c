@@ -591,3 +591,29 @@ int orc_optimize_cands_w(const orc_fcomplex *fft, long long numbins, long long l
     (void) nthreads;
     return bad ? -1 : 0;
 }
+
+/* calc_rzwerrs (src/characteristics.c:353-392). */
+int orc_calc_rzwerrs(const orc_fourierprops *p, double T, orc_rzwerrs *o)
+{
+    if (T <= 0.0) return -1;
+    double T2 = T * T, T3 = T2 * T;
+    double r2 = p->r * p->r, sr2 = p->rerr * p->rerr, r4 = r2 * r2;
+    double z2 = p->z * p->z, sz2 = p->zerr * p->zerr;
+    double tmp = p->r * p->w - 3 * z2;
+    o->f = p->r / T;
+    o->ferr = p->rerr / T;
+    o->fd = p->z / T2;
+    o->fderr = p->zerr / T2;
+    o->fdd = p->w / T3;
+    o->fdderr = p->werr / T3;
+    o->p = T / p->r;
+    o->perr = T * p->rerr / r2;
+    o->pd = -p->z / r2;
+    o->pderr = sqrt(4 * z2 * sr2 / (r4 * r2) + sz2 / r4);
+    if (p->w == 0.0)
+        o->pdd = 0.0;
+    else
+        o->pdd = (2 * z2 - p->r * p->w) / (T * r2 * p->r);
+    o->pdderr = sqrt((p->werr * p->werr * r4 + 16 * sz2 * r2 + 4 * tmp * tmp * sr2) / (r4 * r4 * T2));
+    return 0;
+}

@@ -35,7 +35,7 @@ EXPORTS = [
     "ab_get_transform_costs", "ab_autotune", "ab_add_ffdotpows_ptrs",
     "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
     "ab_get_fourier_amplitudes", "ab_optimize_cands", "ab_realfft", "ab_deredden",
-    "ab_series_to_fft",
+    "ab_series_to_fft", "ab_calc_props", "ab_calc_rzwerrs", "ab_cand_props",
 ]
 
 COST_SLOTS = 16
@@ -58,6 +58,20 @@ class Polished(C.Structure):
     _fields_ = [("numharm", C.c_int), ("pows", C.c_double * POLISH_MAX_HARM),
                 ("hirs", C.c_double * POLISH_MAX_HARM), ("hizs", C.c_double * POLISH_MAX_HARM),
                 ("hiws", C.c_double * POLISH_MAX_HARM), ("derivs", RDerivs * POLISH_MAX_HARM)]
+
+
+class FourierProps(C.Structure):
+    """fourierprops (include/presto.h:170-188); an array of it is a .cand file."""
+    _fields_ = [("r", C.c_double), ("rerr", C.c_float), ("z", C.c_double), ("zerr", C.c_float),
+                ("w", C.c_double), ("werr", C.c_float)] + \
+               [(n, C.c_float) for n in ("pow", "powerr", "sig", "rawpow", "phs", "phserr", "cen",
+                                         "cenerr", "pur", "purerr", "locpow")]
+
+
+class RzwErrs(C.Structure):
+    """rzwerrs (include/presto.h:233-246)."""
+    _fields_ = [(n, C.c_double) for n in ("p", "pd", "pdd", "f", "fd", "fdd")] + \
+               [(n, C.c_float) for n in ("perr", "pderr", "pdderr", "ferr", "fderr", "fdderr")]
 
 
 class AccelError(RuntimeError):
@@ -143,6 +157,9 @@ def lib():
     L.ab_get_fourier_amplitudes.argtypes = [C.POINTER(Obs), vp, ll, i, vp]
     L.ab_optimize_cands.argtypes = [vp, C.POINTER(Obs), vp, i, C.POINTER(Cand), ll,
                                     C.POINTER(Polished)]
+    L.ab_calc_props.argtypes = [C.POINTER(RDerivs), d, d, d, C.POINTER(FourierProps)]
+    L.ab_calc_rzwerrs.argtypes = [C.POINTER(FourierProps), d, C.POINTER(RzwErrs)]
+    L.ab_cand_props.argtypes = [C.POINTER(Cand), C.POINTER(Polished), ll, C.POINTER(FourierProps)]
     L.ab_realfft.argtypes = [vp, vp, ll, i, vp, i]
     L.ab_deredden.argtypes = [vp, vp, ll, i, i, d, d, i]
     L.ab_series_to_fft.argtypes = [vp, vp, ll, d, i, vp, i]
@@ -266,6 +283,61 @@ def set_transform_costs(costs):
     rc = lib().ab_set_transform_costs(c, COST_SLOTS)
     if rc:
         raise AccelError(f"ab_set_transform_costs: {ERRORS.get(rc, rc)}")
+
+
+def calc_props(derivs, r, z, w):
+    """calc_props (src/characteristics.c:195-264) of one rderivs (a RDerivs
+    or a sequence of its 7 values)."""
+    rd = derivs if isinstance(derivs, RDerivs) else RDerivs(*[float(v) for v in derivs])
+    out = FourierProps()
+    rc = lib().ab_calc_props(C.byref(rd), float(r), float(z), float(w), C.byref(out))
+    if rc:
+        raise AccelError(f"ab_calc_props: {ERRORS.get(rc, rc)} (power or local power ~ 0)")
+    return out
+
+
+def calc_rzwerrs(props, T):
+    """calc_rzwerrs (src/characteristics.c:353-392): period, frequency, their
+    derivatives and errors at the start of a run of T seconds."""
+    out = RzwErrs()
+    rc = lib().ab_calc_rzwerrs(C.byref(props), float(T), C.byref(out))
+    if rc:
+        raise AccelError(f"ab_calc_rzwerrs: {ERRORS.get(rc, rc)}")
+    return out
+
+
+def cand_props(cands, polished):
+    """The .cand file's records (src/accelsearch.c:261-272): per candidate
+    (power, sigma, numharm, r, z, w) and its polishing (a dict from
+    Context.optimize_cands), the fundamental's fourierprops at the search's
+    r, z, w with the errors set to ACCEL_DR, ACCEL_DZ, ACCEL_DW / numharm."""
+    n = len(cands)
+    arr = (Cand * max(n, 1))(*[Cand(c[0], c[1], c[2], c[3], c[4], c[5]) for c in cands])
+    pol = (Polished * max(n, 1))()
+    for k, p in enumerate(polished):
+        pol[k].numharm = len(p["pows"])
+        for h in range(len(p["pows"])):
+            pol[k].derivs[h] = RDerivs(*[float(v) for v in p["derivs"][h]])
+    out = (FourierProps * max(n, 1))()
+    rc = lib().ab_cand_props(arr, pol, n, out)
+    if rc:
+        raise AccelError(f"ab_cand_props: {ERRORS.get(rc, rc)}")
+    return list(out[:n])
+
+
+def write_candfile(path, props):
+    """Writes fourierprops records as the reference's binary .cand file
+    (src/accelsearch.c:282-284: the struct array, raw)."""
+    arr = (FourierProps * len(props))(*props)
+    with open(path, "wb") as f:
+        f.write(bytes(arr))
+
+
+def read_candfile(path):
+    """The fourierprops records of a .cand file."""
+    data = open(path, "rb").read()
+    n = len(data) // C.sizeof(FourierProps)
+    return list((FourierProps * n).from_buffer_copy(data[:n * C.sizeof(FourierProps)]))
 
 
 def algorithmic_counts(obs):

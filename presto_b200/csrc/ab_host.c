@@ -1066,3 +1066,81 @@ int ab_dered_plan(long long numbins, int startwidth, int endwidth, double endfre
 }
 
 long long ab_num_blocks_main(const ab_obs *obs) { return obs ? ab_num_blocks(obs) : -1; }
+
+/* ------------------------------------------------------------------ */
+/* candidate properties and the .cand file                             */
+/* ------------------------------------------------------------------ */
+
+/* calc_props (src/characteristics.c:195-264): purity from the curvature of
+ * the locally normalised power, then the errors of r, z, w, power, phase
+ * and centroid.  The purity is stored as float first and the later
+ * formulas use that stored value, as the reference's do. */
+int ab_calc_props(const ab_rderivs *d, double r, double z, double w, ab_fourierprops *o)
+{
+    if (!d || !o) return AB_ERR_ARG;
+    if (fabs(d->pow) < AB_DBLCORRECT || d->locpow < AB_DBLCORRECT) return AB_ERR_ARG;
+    const double tmppow = d->pow / d->locpow, tmpd2pow = d->d2pow / d->locpow;
+    memset(o, 0, sizeof *o);
+    o->pur = (float) (sqrt(1.5 * fabs(tmpd2pow) / tmppow) / AB_PI);
+    if (fabs(tmppow) < AB_DBLCORRECT) o->pur = 1.0f;
+    o->purerr = (float) (1.0 / (o->pur * sqrt(10.0 * tmppow)));
+    o->r = r;
+    o->rerr = (float) (3.0 / (AB_PI * o->pur * sqrt(6.0 * tmppow)));
+    o->z = z;
+    o->zerr = (float) (3.0 * sqrt(10.0) / (AB_PI * o->pur * o->pur * sqrt(tmppow)));
+    o->w = w;
+    o->werr = (float) (6.0 * sqrt(105.0) / (AB_PI * o->pur * o->pur * o->pur * sqrt(tmppow)));
+    o->pow = (float) tmppow;
+    o->powerr = (float) sqrt(2.0 * tmppow);
+    o->sig = (float) sqrt(2.0 * tmppow - log(AB_PI * tmppow));
+    o->rawpow = (float) d->pow;
+    o->phs = (float) d->phs;
+    o->phserr = (float) (1.0 / o->powerr);
+    o->cen = (float) (-d->dphs / (2.0 * AB_PI));
+    o->cenerr = (float) (1.0 / sqrt(24.0 * tmppow));
+    o->locpow = (float) d->locpow;
+    return AB_OK;
+}
+
+/* calc_rzwerrs (src/characteristics.c:353-392): period, frequency, their
+ * first two derivatives at the start of the run, and their errors. */
+int ab_calc_rzwerrs(const ab_fourierprops *p, double T, ab_rzwerrs *o)
+{
+    if (!p || !o || !(T > 0.0)) return AB_ERR_ARG;
+    const double T2 = T * T, T3 = T2 * T;
+    /* the float errors are squared in float, as the reference does */
+    const double r2 = p->r * p->r, sr2 = p->rerr * p->rerr, r4 = r2 * r2;
+    const double z2 = p->z * p->z, sz2 = p->zerr * p->zerr;
+    const double tmp = p->r * p->w - 3 * z2;
+    memset(o, 0, sizeof *o);
+    o->f = p->r / T;
+    o->ferr = (float) (p->rerr / T);
+    o->fd = p->z / T2;
+    o->fderr = (float) (p->zerr / T2);
+    o->fdd = p->w / T3;
+    o->fdderr = (float) (p->werr / T3);
+    o->p = T / p->r;
+    o->perr = (float) (T * p->rerr / r2);
+    o->pd = -p->z / r2;
+    o->pderr = (float) sqrt(4 * z2 * sr2 / (r4 * r2) + sz2 / r4);
+    o->pdd = p->w == 0.0 ? 0.0 : (2 * z2 - p->r * p->w) / (T * r2 * p->r);
+    o->pdderr = (float) sqrt((p->werr * p->werr * r4 + 16 * sz2 * r2 + 4 * tmp * tmp * sr2) /
+                             (r4 * r4 * T2));
+    return AB_OK;
+}
+
+/* src/accelsearch.c:261-272: the fundamentals' properties written to the
+ * .cand file. */
+int ab_cand_props(const ab_cand *c, const ab_polished *pol, long long n, ab_fourierprops *out)
+{
+    if (n < 0 || (n > 0 && (!c || !pol || !out))) return AB_ERR_ARG;
+    for (long long i = 0; i < n; i++) {
+        if (c[i].numharm < 1) return AB_ERR_ARG;
+        int rc = ab_calc_props(&pol[i].derivs[0], c[i].r, c[i].z, c[i].w, &out[i]);
+        if (rc) return rc;
+        out[i].rerr = (float) AB_DR / c[i].numharm;
+        out[i].zerr = (float) AB_DZ / c[i].numharm;
+        out[i].werr = (float) AB_DW / c[i].numharm;
+    }
+    return AB_OK;
+}
