@@ -665,3 +665,23 @@ class AccelSearch:
         fft = np.ascontiguousarray(fft, dtype=np.complex64)
         obs = self.obs(N, dt, fft.size)
         return self.ctx.search(obs, fft)
+
+    def run(self, fft, N, dt, harmremove=True, candfile=None):
+        """The whole of src/accelsearch.c:155-284 for one spectrum: the search,
+        sort_accelcands, eliminate_harmonics (numharm > 1 unless harmremove
+        is False, as -noharmremove), optimize_accelcand of every candidate on
+        the device, and the fundamentals' .cand records (written to candfile
+        when given).  Returns dict(cands, polished, props)."""
+        fft = np.ascontiguousarray(fft, dtype=np.complex64)
+        obs = self.obs(N, dt, fft.size)
+        cands = self.ctx.search(obs, fft)
+        polished, props = [], []
+        if cands:
+            cands = sort_cands(cands)
+            if self.opts["numharm"] > 1 and harmremove:
+                cands = eliminate_harmonics(cands)
+            polished = self.ctx.optimize_cands(obs, fft, cands)
+            props = cand_props(cands, polished)
+            if candfile:
+                write_candfile(candfile, props)
+        return dict(cands=cands, polished=polished, props=props)

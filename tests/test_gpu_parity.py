@@ -295,6 +295,33 @@ def test_injected_signal_recovered(ctx, ablib):
     assert abs(best[4] * best[2] - 40.0) <= 2.0 or abs(best[4] - 40.0) <= 2.0
 
 
+def test_accelsearch_run_writes_cand_file(ctx, ablib, tmp_path):
+    """AccelSearch.run: the search, sort, harmonic removal, polishing and the
+    .cand records of src/accelsearch.c:229-284.  The strongest candidate is
+    the injected f = 123.4 Hz, z = 40 tone; its record gives that frequency
+    through calc_rzwerrs; the file is the raw record array."""
+    N = 1 << 19
+    fft = synth.cfg1_spectrum(N=N, amp=0.05)
+    s = ablib.AccelSearch(zmax=200, numharm=8, sigma=2.0, ctx=ctx)
+    path = tmp_path / "cfg1_ACCEL_200.cand"
+    res = s.run(fft, N, DT, candfile=str(path))
+    cands, pol, props = res["cands"], res["polished"], res["props"]
+    assert cands and len(cands) == len(pol) == len(props)
+    assert [c[1] for c in cands] == sorted((c[1] for c in cands), reverse=True)
+    assert ablib.eliminate_harmonics(ablib.sort_cands(s(fft, N, DT))) == cands
+    T = N * DT
+    f0 = ablib.calc_rzwerrs(props[0], T).f          # the search's fundamental, r / T
+    assert f0 == cands[0][3] / T
+    # the tone is harmonic k of the strongest candidate (k = 1 unless a sum won)
+    ks = [k for k in range(1, cands[0][2] + 1) if abs(f0 * k - 123.4) < 1.0 / T]
+    assert ks, (f0, cands[0])
+    # its polished r lies within half a bin of the injected frequency
+    assert abs(pol[0]["hirs"][ks[0] - 1] - 123.4 * T) < 0.5
+    assert path.stat().st_size == 88 * len(props)
+    back = ablib.read_candfile(str(path))
+    assert [(p.r, p.z, p.sig) for p in back] == [(p.r, p.z, p.sig) for p in props]
+
+
 def test_wrapping_bank_matches_oracle(ctx, ablib, oracle):
     """zmax=100, wmax=200, numharm=16: the reference's 192-point FFT for the
     1/16 harmonic is one sample shorter than the span its valid cells read, so
