@@ -62,6 +62,7 @@ typedef struct {
     long long lobin;      /* -lobin */
     int inmemP;           /* -inmem */
     float nph;            /* > 0: -photon normalisation with this level */
+    int locpowP;          /* -locpow: double-tophat local-power normalisation */
 } ab_params;
 
 /* accelobs geometry (include/accel.h:37-81), hot-path fields only. */

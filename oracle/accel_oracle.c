@@ -130,7 +130,7 @@ int orc_obs_init(const orc_params *p, orc_obs *obs)
     obs->N = p->N;
     obs->numbins = p->numbins;
     obs->nph = p->nph > 0 ? p->nph : 0.0f;
-    obs->norm_type = 0;
+    obs->norm_type = (p->nph > 0 || !p->locpowP) ? 0 : 1;     /* src/accel_utils.c:1598-1620 */
     obs->lobin = p->lobin;
     if (obs->lobin > 0) {
         obs->nph = 0.0f;
@@ -881,8 +881,22 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
     /* normalisation (:1079-1115) */
     rcplx *pdata = (rcplx *) calloc(L, sizeof(rcplx));
     double norm;
+    float *lnorm = NULL;            /* -locpow: per-bin factors */
     if (obs->nph > 0.0) {
         norm = 1.0 / sqrt(obs->nph);
+    } else if (obs->norm_type == 1) {
+        /* src/accel_utils.c:1100-1113: invsqrtf of corr_loc_pow per bin */
+        float *pw = (float *) malloc(sizeof(float) * numdata);
+        lnorm = (float *) malloc(sizeof(float) * numdata);
+        for (int ii = 0; ii < numdata; ii++) {
+            volatile float a = data[ii].r * data[ii].r;
+            volatile float b = data[ii].i * data[ii].i;
+            pw[ii] = a + b;
+        }
+        orc_loc_pow(pw, numdata, lnorm);
+        for (int ii = 0; ii < numdata; ii++) lnorm[ii] = orc_invsqrtf(lnorm[ii]);
+        free(pw);
+        norm = 0.0;
     } else {
         float *pw = (float *) malloc(sizeof(float) * numdata);
         for (int ii = 0; ii < numdata; ii++) {
@@ -894,7 +908,12 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
         free(pw);
     }
     /* spread_no_pad (src/corr_prep.c:62-74) */
-    for (int ii = 0; ii < numdata; ii++) {
+    for (int ii = 0; ii < numdata && lnorm; ii++) {
+        const float f = lnorm[ii];
+        pdata[2 * ii].r = (real) (data[ii].r * f);          /* float products */
+        pdata[2 * ii].i = (real) (data[ii].i * f);
+    }
+    for (int ii = 0; ii < numdata && !lnorm; ii++) {
 #if defined(ORC_FP32_DATA)
         pdata[2 * ii].r = (real) (float) (data[ii].r * norm);
         pdata[2 * ii].i = (real) (float) (data[ii].i * norm);
@@ -904,6 +923,7 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
 #endif
     }
     free(data);
+    free(lnorm);
     rcplx *tmp = (rcplx *) malloc(sizeof(rcplx) * L);
     cfft(pdata, tmp, L, -1);
     free(tmp);

@@ -45,6 +45,7 @@ typedef struct {
     long long lobin;
     int inmemP;
     float nph;            /* >0: photon normalisation (-photon) */
+    int locpowP;          /* -locpow: local-power normalisation */
 } orc_params;
 
 /* Geometry subset of accelobs (include/accel.h:37-81). */
@@ -203,6 +204,7 @@ int    orc_optimize_cands_w(const orc_fcomplex *fft, long long numbins, long lon
 /* ---- time-series input path (series_oracle.c) -------------------------- */
 int   orc_realfft_forward(float *data, long n);
 float orc_invsqrtf(float x);
+void  orc_loc_pow(const float *pw, int n, float *local);
 long  orc_deredden(orc_fcomplex *fft, long numbins, int startwidth, int endwidth, double endfreq,
                    double T);
 

@@ -18,7 +18,8 @@ class Params(C.Structure):
                 ("numharm", C.c_int), ("sigma", C.c_float),
                 ("flo", C.c_double), ("fhi", C.c_double), ("floP", C.c_int), ("fhiP", C.c_int),
                 ("rlo", C.c_double), ("rhi", C.c_double), ("rloP", C.c_int), ("rhiP", C.c_int),
-                ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float)]
+                ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float),
+                ("locpowP", C.c_int)]
 
 
 class Obs(C.Structure):
@@ -123,7 +124,8 @@ def lib(prec=64):
 
 
 def make_params(N, dt, numbins, zmax=200, wmax=None, numharm=8, sigma=2.0,
-                flo=1.0, fhi=10000.0, inmem=False, rlo=None, rhi=None, nph=0.0, lobin=0):
+                flo=1.0, fhi=10000.0, inmem=False, rlo=None, rhi=None, nph=0.0, lobin=0,
+                locpow=False):
     """Mirror of the accelsearch command line defaults (src/accelsearch_cmd.c:22-61)."""
     p = Params()
     p.N, p.dt, p.numbins = N, dt, numbins
@@ -139,6 +141,7 @@ def make_params(N, dt, numbins, zmax=200, wmax=None, numharm=8, sigma=2.0,
     p.rloP = 0 if rlo is None else 1
     p.rhiP = 0 if rhi is None else 1
     p.lobin, p.inmemP, p.nph = lobin, int(inmem), nph
+    p.locpowP = int(bool(locpow))
     return p
 
 
@@ -399,6 +402,16 @@ def _series_lib():
         L.orc_invsqrtf.argtypes = [C.c_float]
         L._series_ready = True
     return L
+
+
+def loc_pow(powers):
+    """corr_loc_pow (src/corr_routines.c:309-366) restated exactly."""
+    pw = np.ascontiguousarray(powers, dtype=np.float32)
+    out = np.zeros_like(pw)
+    L = _series_lib()
+    L.orc_loc_pow.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.orc_loc_pow(pw.ctypes.data, pw.size, out.ctypes.data)
+    return out
 
 
 def realfft(series):

@@ -170,3 +170,21 @@ done:
     free(pw);
     return ret;
 }
+
+/* corr_loc_pow (src/corr_routines.c:309-366): the powers correlated with a
+ * double top-hat of 20 taps at +-6..+-15 bins, each (n / 2) / NUMLOCPOWAVG in
+ * integer arithmetic, through real FFTs whose round trip (real_corr_conv,
+ * src/correlations.c) carries 2 / n; the first and last 15 values take the
+ * nearest value 15 from the edge.  Restated as the exact sum the FFTs
+ * compute (they round it in FP32); no tap of a kept value wraps. */
+void orc_loc_pow(const float *pw, int n, float *local)
+{
+    const int khw = 20 / 2 + 5;
+    const double normal = (double) ((n / 2) / 20);
+    for (int i = 0; i < n; i++) {
+        const int c = i < khw ? khw : (i > n - 1 - khw ? n - 1 - khw : i);
+        double s = 0.0;
+        for (int j = 6; j <= khw; j++) s += (double) pw[c - j] + (double) pw[c + j];
+        local[i] = (float) (s * normal * (2.0 / (double) n));
+    }
+}

@@ -84,7 +84,8 @@ class Params(C.Structure):
                 ("numharm", C.c_int), ("sigma", C.c_float),
                 ("flo", C.c_double), ("fhi", C.c_double), ("floP", C.c_int), ("fhiP", C.c_int),
                 ("rlo", C.c_double), ("rhi", C.c_double), ("rloP", C.c_int), ("rhiP", C.c_int),
-                ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float)]
+                ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float),
+                ("locpowP", C.c_int)]
 
 
 class Obs(C.Structure):
@@ -207,10 +208,11 @@ def lib():
 
 
 def make_params(N, dt, numbins=None, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0,
-                fhi=10000.0, rlo=None, rhi=None, inmem=False, photon=None, lobin=0):
+                fhi=10000.0, rlo=None, rhi=None, inmem=False, photon=None, lobin=0,
+                locpow=False):
     """accelsearch options (src/accelsearch_cmd.c:22-61 defaults).  wmax=None
     means -wmax not given (an explicit -wmax 0 disables in-memory mode,
-    src/accel_utils.c:1795)."""
+    src/accel_utils.c:1795); locpow=True is -locpow."""
     p = Params()
     lib().ab_params_default(C.byref(p))
     p.N, p.dt = int(N), float(dt)
@@ -229,6 +231,7 @@ def make_params(N, dt, numbins=None, zmax=200, wmax=None, numharm=8, sigma=2.0, 
     p.inmemP = int(bool(inmem))
     p.nph = float(photon) if photon else 0.0
     p.lobin = int(lobin)
+    p.locpowP = int(bool(locpow))
     return p
 
 
@@ -653,9 +656,10 @@ class AccelSearch:
     """accelsearch for one spectrum: options as on the command line."""
 
     def __init__(self, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0, fhi=10000.0,
-                 rlo=None, rhi=None, inmem=False, photon=None, lobin=0, device=0, ctx=None):
+                 rlo=None, rhi=None, inmem=False, photon=None, lobin=0, locpow=False, device=0,
+                 ctx=None):
         self.opts = dict(zmax=zmax, wmax=wmax, numharm=numharm, sigma=sigma, flo=flo, fhi=fhi,
-                         rlo=rlo, rhi=rhi, inmem=inmem, photon=photon, lobin=lobin)
+                         rlo=rlo, rhi=rhi, inmem=inmem, photon=photon, lobin=lobin, locpow=locpow)
         self.ctx = ctx or Context(device)
 
     def obs(self, N, dt, numbins=None):

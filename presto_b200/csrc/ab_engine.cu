@@ -318,6 +318,7 @@ static SearchConsts make_consts(const ab_obs *obs, const ab_bankset &bs)
     sc.inmem = obs->inmem;
     sc.nbanks = bs.nbanks;
     sc.nph = obs->nph;
+    sc.norm_type = obs->norm_type;
     for (int i = 0; i < AB_MAX_STAGES; i++) sc.powcut[i] = i < obs->numharmstages ? obs->powcut[i] : 0.f;
     sc.err = nullptr;
     return sc;

@@ -219,7 +219,9 @@ int ab_obs_init(const ab_params *p, ab_obs *obs)        /* src/accel_utils.c:159
     obs->N = p->N;
     obs->numbins = p->numbins;
     obs->nph = p->nph > 0.0f ? p->nph : 0.0f;
-    obs->norm_type = 0;
+    /* -photon takes precedence; otherwise -locpow selects the local-power
+     * normalisation (src/accel_utils.c:1598-1620) */
+    obs->norm_type = (p->nph > 0.0f || !p->locpowP) ? 0 : 1;
     obs->lobin = p->lobin;
     if (obs->lobin > 0) {
         obs->nph = 0.0f;
@@ -446,7 +448,10 @@ int ab_bankset_init_tuned(const ab_obs *obs, const double *cost_by_log2L, ab_ban
          * the transform cost per block. */
         int sbm = 1;
         double best = transform_cost(cost_by_log2L, L);
-        if (!obs->inmem && need <= b->fftlen_ref && nblocks > 1 && best > 0.0) {
+        /* not with the local-power normalisation: it scales every bin of
+         * each block's own window, which one shared transform cannot hold */
+        if (!obs->inmem && obs->norm_type == 0 && need <= b->fftlen_ref && nblocks > 1 &&
+            best > 0.0) {
             for (int m = 2; m <= AB_MAX_SBM && m <= nblocks; m++) {
                 long long span = 0;
                 for (long long k = 0; k + m - 1 < nblocks; k++) {

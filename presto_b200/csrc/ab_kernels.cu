@@ -20,6 +20,7 @@
 #include "ab_fft.cuh"
 #include "ab_index.h"
 #include "ab_kernels.h"
+#include "ab_norm.cuh"
 #include "ab_resp.cuh"
 #include "ab_select.cuh"
 
@@ -279,11 +280,22 @@ __device__ __forceinline__ void block_geom(const SearchConsts &sc, const ab_bank
 // values without FMA, sorted exactly; even counts average the two central
 // values (GSL semantics).  pw: shared scratch of numdata floats.
 // Called by every thread of the CTA.
+// The block's normalisation (src/accel_utils.c:1079-1113): 1/sqrt(nph) with
+// -photon, else 1/sqrt(median/ln 2) of the window's powers.  With -locpow
+// (sc.norm_type 1) it leaves the window's powers in pw for locpow_invsqrt
+// and returns 0 (the factor is per bin).
 __device__ double block_norm(const SearchConsts &sc, long long lobin, int numdata, const float2 *fft,
                              float *pw, double *s_norm)
 {
     if (sc.nph > 0.0f) {
         if (threadIdx.x == 0) *s_norm = 1.0 / sqrt((double) sc.nph);
+    } else if (sc.norm_type == 1) {
+        for (int i = threadIdx.x; i < numdata; i += blockDim.x) {
+            long long bin = lobin + i - sc.obs_lobin;
+            float2 v = (bin >= 0 && bin < sc.numbins) ? fft[bin] : make_float2(0.f, 0.f);
+            pw[i] = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+        }
+        if (threadIdx.x == 0) *s_norm = 0.0;
     } else {
         // block median of |X|^2 in float (POWER(), no FMA), src/accel_utils.c:1087-1099
         for (int i = threadIdx.x; i < numdata; i += blockDim.x) {
@@ -326,6 +338,10 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
     const int numdata = sb ? LH : b.fftlen_ref / AB_NUMBETWEEN;
     const double norm = sb ? sc.norms[(long long) blk * sc.nbanks + b.index]
                            : block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
+    // -locpow: per-bin factors from the window's powers that block_norm left in
+    // shared memory (superblocks are never formed with it)
+    const bool locpow = !sb && sc.nph <= 0.0f && sc.norm_type == 1;
+    const float *pw = reinterpret_cast<const float *>(fsm);
     // spread data d[i] = norm * x[i mod numdata] at even samples: the
     // reference's window of numdata bins repeated with period fftlen_ref, so
     // that a device transform longer than the reference's reproduces its
@@ -344,7 +360,12 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
             long long bin = lobin + i - sc.obs_lobin;
             if (bin >= 0 && bin < sc.numbins) {
                 float2 a = fft[bin];
-                x = make_float2((float) ((double) a.x * norm), (float) ((double) a.y * norm));
+                if (locpow) {
+                    const float f = locpow_invsqrt(pw, numdata, i);
+                    x = make_float2(__fmul_rn(a.x, f), __fmul_rn(a.y, f));
+                } else {
+                    x = make_float2((float) ((double) a.x * norm), (float) ((double) a.y * norm));
+                }
             }
         }
         v[m] = x;
@@ -446,13 +467,20 @@ __global__ void __launch_bounds__(256) k_prep_time(const ab_bank *banks, SearchC
     const long long lobin = g.rlo - b.hw0;
     const int numdata = b.fftlen_ref / AB_NUMBETWEEN;
     const double norm = block_norm(sc, lobin, numdata, fft, reinterpret_cast<float *>(fsm), &s_norm);
+    const bool locpow = sc.nph <= 0.0f && sc.norm_type == 1;
+    const float *pw = reinterpret_cast<const float *>(fsm);
     float2 *o = dtime + (long long) bi * dt_per_block + b.dtime_off;
     for (int i = threadIdx.x; i < numdata; i += blockDim.x) {
         long long bin = lobin + i - sc.obs_lobin;
         float2 x = make_float2(0.f, 0.f);
         if (bin >= 0 && bin < sc.numbins) {
             float2 v = fft[bin];
-            x = make_float2((float) ((double) v.x * norm), (float) ((double) v.y * norm));
+            if (locpow) {
+                const float f = locpow_invsqrt(pw, numdata, i);
+                x = make_float2(__fmul_rn(v.x, f), __fmul_rn(v.y, f));
+            } else {
+                x = make_float2((float) ((double) v.x * norm), (float) ((double) v.y * norm));
+            }
         }
         o[i] = x;
     }

@@ -20,6 +20,7 @@ struct SearchConsts {
     unsigned *err;             // device error word for bounded waits; may be null
     int superblocks;           // standard search: banks with sbm > 1 share transforms
     const double *norms;       // [block][bank] normalisations (superblock banks)
+    int norm_type;             // 0: block median, 1: local power (-locpow)
 };
 
 // Blocks of one launch: global ordinal block0 + i, start frequency startr[i].

@@ -141,6 +141,7 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
     sc.inmem = 0;
     sc.nbanks = 1;
     sc.nph = obs->nph;
+    sc.norm_type = obs->norm_type;
     BlockBatch bb{d_start, 0, 1, 0};
     if (launch_prep(d_desc, &b, 1, sc, bb, reinterpret_cast<const float2 *>(d_fft), d_xhat,
                     b.L / 2, st) != cudaSuccess)

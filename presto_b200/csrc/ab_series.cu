@@ -21,6 +21,7 @@
 
 #include "ab_fft.cuh"
 #include "ab_kernels.h"
+#include "ab_norm.cuh"
 #include "ab_select.cuh"
 
 namespace ab {
@@ -103,14 +104,6 @@ __global__ void k_untangle(float2 *c, long long n)
     c[ih] = hi;
 }
 
-// invsqrtf (src/misc_utils.c:291-302): the published fast inverse square
-// root, one Newton step, in float with explicit rounding.
-__device__ __forceinline__ float fast_invsqrtf(float x)
-{
-    const float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
-    const float t = __fmul_rn(__fmul_rn(__fmul_rn(0.5f, x), y), y);
-    return __fmul_rn(y, __fsub_rn(1.5f, t));
-}
 
 // Median of each block's powers / ln 2 (the block "mean" of deredden), one
 // 32-thread CTA per block.

@@ -90,3 +90,27 @@ def test_fft_roundtrip(oracle):
         assert np.allclose(y, np.fft.fft(x), atol=1e-9)
         L.orc_cfft_double(y.ctypes.data, n, 1)
         assert np.allclose(y / n, x, atol=1e-12)
+
+
+def test_loc_pow_is_corr_loc_pow(oracle):
+    """The oracle's local power (-locpow) against corr_loc_pow computed the
+    reference's way (src/corr_routines.c:309-366): the double top-hat kernel
+    (taps (n/2)/20 at +-6..+-15) correlated with the powers by real FFTs,
+    the product scaled by 2/n (real_corr_conv, src/correlations.c), the
+    inverse normalised, and the first and last 15 values replaced."""
+    rng = np.random.default_rng(41)
+    for n in (64, 1024, 4096):
+        pw = rng.exponential(1.0, n).astype(np.float32) * (1.0 + np.arange(n) / n)
+        kern = np.zeros(n)
+        kern[6:16] = (n // 2) // 20
+        kern[n - 15:n - 5] = (n // 2) // 20
+        corr = np.fft.irfft(np.fft.rfft(pw.astype(np.float64)) * np.conj(np.fft.rfft(kern)), n)
+        want = corr * (2.0 / n)
+        want[:15] = want[15]
+        want[n - 15:] = want[n - 16]
+        got = oracle.loc_pow(pw)
+        np.testing.assert_allclose(got, want, rtol=2e-7)
+        # the mean of 20 neighbours scaled by (2/n) floor(n/40) * 20
+        i = n // 2
+        direct = (pw[i - 15:i - 5].sum() + pw[i + 6:i + 16].sum()) * ((n // 2) // 20) * 2.0 / n
+        assert abs(got[i] - direct) <= 1e-6 * direct

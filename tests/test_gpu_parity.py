@@ -36,6 +36,11 @@ CASES = {
     # jerk search
     "jerk": dict(N=1 << 16, seed=13, zmax=20, wmax=40, numharm=2,
                  pulsars=[dict(r=900.2, z=6.0, w=25.0, harms=[(0.12, 0.0), (0.06, 0.5)])]),
+    # -locpow (double-tophat local-power normalisation), standard and in-memory
+    "std_locpow": dict(N=1 << 17, seed=14, zmax=60, wmax=0, numharm=4, locpow=True,
+                       pulsars=[dict(r=1700.6, z=-9.0, harms=[(0.08, 0.2), (0.05, 0.9)])]),
+    "inmem_locpow": dict(N=1 << 17, seed=15, zmax=40, wmax=None, numharm=8, locpow=True,
+                         pulsars=[dict(r=2048.4, z=14.0, harms=[(0.06, 0.4)] * 5)]),
 }
 
 
@@ -43,9 +48,10 @@ CASES = {
 def case(request, ablib, oracle):
     c = CASES[request.param]
     fft = _spec(c["N"], c["seed"], c["pulsars"])
-    kw = dict(zmax=c["zmax"], wmax=c["wmax"], numharm=c["numharm"])
+    kw = dict(zmax=c["zmax"], wmax=c["wmax"], numharm=c["numharm"], locpow=c.get("locpow", False))
     obs = ablib.obs_init(ablib.make_params(c["N"], DT, fft.size, **kw))
     oobs = oracle.obs_init(oracle.make_params(c["N"], DT, fft.size, **kw))
+    assert obs.norm_type == oobs.norm_type == int(kw["locpow"])
     return dict(name=request.param, fft=fft, obs=obs, oobs=oobs, kw=kw, N=c["N"])
 
 

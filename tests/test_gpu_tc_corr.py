@@ -34,7 +34,7 @@ def tcctx(ablib):
 def case(request, ablib, oracle):
     c = CASES[request.param]
     fft = _spec(c["N"], c["seed"], c["pulsars"])
-    kw = dict(zmax=c["zmax"], wmax=c["wmax"], numharm=c["numharm"])
+    kw = dict(zmax=c["zmax"], wmax=c["wmax"], numharm=c["numharm"], locpow=c.get("locpow", False))
     obs = ablib.obs_init(ablib.make_params(c["N"], DT, fft.size, **kw))
     oobs = oracle.obs_init(oracle.make_params(c["N"], DT, fft.size, **kw))
     return dict(name=request.param, fft=fft, obs=obs, oobs=oobs, kw=kw, N=c["N"])
