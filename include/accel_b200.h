@@ -63,6 +63,7 @@ typedef struct {
     int inmemP;           /* -inmem */
     float nph;            /* > 0: -photon normalisation with this level */
     int locpowP;          /* -locpow: double-tophat local-power normalisation */
+    int noharmpolishP;    /* -noharmpolish: polish each harmonic on its own */
 } ab_params;
 
 /* accelobs geometry (include/accel.h:37-81), hot-path fields only. */
@@ -74,6 +75,7 @@ typedef struct {
     float nph, sigma;
     float powcut[6];
     long long numindep[6];
+    int use_harmonic_polishing;   /* 0 with -noharmpolish (src/accel_utils.c:1489-1494) */
 } ab_obs;
 
 /* accelcand search fields (include/accel.h:83-95). */

@@ -46,6 +46,7 @@ typedef struct {
     int inmemP;
     float nph;            /* >0: photon normalisation (-photon) */
     int locpowP;          /* -locpow: local-power normalisation */
+    int noharmpolishP;    /* -noharmpolish */
 } orc_params;
 
 /* Geometry subset of accelobs (include/accel.h:37-81). */
@@ -57,6 +58,7 @@ typedef struct {
     float nph, sigma;
     float powcut[6];
     long long numindep[6];
+    int use_harmonic_polishing;   /* src/accel_utils.c:1489-1494 */
 } orc_obs;
 
 /* One plane (ffdotpows, include/accel.h:120-130), powers[w][z][r]. */

@@ -19,7 +19,7 @@ class Params(C.Structure):
                 ("flo", C.c_double), ("fhi", C.c_double), ("floP", C.c_int), ("fhiP", C.c_int),
                 ("rlo", C.c_double), ("rhi", C.c_double), ("rloP", C.c_int), ("rhiP", C.c_int),
                 ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float),
-                ("locpowP", C.c_int)]
+                ("locpowP", C.c_int), ("noharmpolishP", C.c_int)]
 
 
 class Obs(C.Structure):
@@ -33,7 +33,8 @@ class Obs(C.Structure):
                 ("dr", C.c_double), ("zlo", C.c_double), ("zhi", C.c_double), ("dz", C.c_double),
                 ("wlo", C.c_double), ("whi", C.c_double), ("dw", C.c_double),
                 ("nph", C.c_float), ("sigma", C.c_float),
-                ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6)]
+                ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6),
+                ("use_harmonic_polishing", C.c_int)]
 
 
 class FFDot(C.Structure):
@@ -125,7 +126,7 @@ def lib(prec=64):
 
 def make_params(N, dt, numbins, zmax=200, wmax=None, numharm=8, sigma=2.0,
                 flo=1.0, fhi=10000.0, inmem=False, rlo=None, rhi=None, nph=0.0, lobin=0,
-                locpow=False):
+                locpow=False, noharmpolish=False):
     """Mirror of the accelsearch command line defaults (src/accelsearch_cmd.c:22-61)."""
     p = Params()
     p.N, p.dt, p.numbins = N, dt, numbins
@@ -142,6 +143,7 @@ def make_params(N, dt, numbins, zmax=200, wmax=None, numharm=8, sigma=2.0,
     p.rhiP = 0 if rhi is None else 1
     p.lobin, p.inmemP, p.nph = lobin, int(inmem), nph
     p.locpowP = int(bool(locpow))
+    p.noharmpolishP = int(bool(noharmpolish))
     return p
 
 

@@ -85,7 +85,7 @@ class Params(C.Structure):
                 ("flo", C.c_double), ("fhi", C.c_double), ("floP", C.c_int), ("fhiP", C.c_int),
                 ("rlo", C.c_double), ("rhi", C.c_double), ("rloP", C.c_int), ("rhiP", C.c_int),
                 ("lobin", C.c_longlong), ("inmemP", C.c_int), ("nph", C.c_float),
-                ("locpowP", C.c_int)]
+                ("locpowP", C.c_int), ("noharmpolishP", C.c_int)]
 
 
 class Obs(C.Structure):
@@ -99,7 +99,8 @@ class Obs(C.Structure):
                 ("dr", C.c_double), ("zlo", C.c_double), ("zhi", C.c_double), ("dz", C.c_double),
                 ("wlo", C.c_double), ("whi", C.c_double), ("dw", C.c_double),
                 ("nph", C.c_float), ("sigma", C.c_float),
-                ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6)]
+                ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6),
+                ("use_harmonic_polishing", C.c_int)]
 
 
 class Cand(C.Structure):
@@ -209,7 +210,7 @@ def lib():
 
 def make_params(N, dt, numbins=None, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0,
                 fhi=10000.0, rlo=None, rhi=None, inmem=False, photon=None, lobin=0,
-                locpow=False):
+                locpow=False, noharmpolish=False):
     """accelsearch options (src/accelsearch_cmd.c:22-61 defaults).  wmax=None
     means -wmax not given (an explicit -wmax 0 disables in-memory mode,
     src/accel_utils.c:1795); locpow=True is -locpow."""
@@ -232,6 +233,7 @@ def make_params(N, dt, numbins=None, zmax=200, wmax=None, numharm=8, sigma=2.0, 
     p.nph = float(photon) if photon else 0.0
     p.lobin = int(lobin)
     p.locpowP = int(bool(locpow))
+    p.noharmpolishP = int(bool(noharmpolish))
     return p
 
 
@@ -656,10 +658,11 @@ class AccelSearch:
     """accelsearch for one spectrum: options as on the command line."""
 
     def __init__(self, zmax=200, wmax=None, numharm=8, sigma=2.0, flo=1.0, fhi=10000.0,
-                 rlo=None, rhi=None, inmem=False, photon=None, lobin=0, locpow=False, device=0,
-                 ctx=None):
+                 rlo=None, rhi=None, inmem=False, photon=None, lobin=0, locpow=False,
+                 noharmpolish=False, device=0, ctx=None):
         self.opts = dict(zmax=zmax, wmax=wmax, numharm=numharm, sigma=sigma, flo=flo, fhi=fhi,
-                         rlo=rlo, rhi=rhi, inmem=inmem, photon=photon, lobin=lobin, locpow=locpow)
+                         rlo=rlo, rhi=rhi, inmem=inmem, photon=photon, lobin=lobin, locpow=locpow,
+                         noharmpolish=noharmpolish)
         self.ctx = ctx or Context(device)
 
     def obs(self, N, dt, numbins=None):

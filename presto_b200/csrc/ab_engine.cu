@@ -1066,27 +1066,64 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
         }
         char msg[256] = {0};
         const size_t budget = std::min<size_t>(ctx->scratch_budget, 1ull << 30);
-        rc = rzw_optimize(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p, budget,
-                          ctx->stream, msg, sizeof msg, &ctx->launches);
+        rc = obs->use_harmonic_polishing
+                 ? rzw_optimize(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p, budget,
+                                ctx->stream, msg, sizeof msg, &ctx->launches)
+                 : rzw_optimize_each(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p,
+                                     budget, ctx->stream, msg, sizeof msg, &ctx->launches);
         if (rc) return fail(ctx, rc, "%s", msg);
         return AB_OK;
     }
-    std::vector<PolishIn> in((size_t) n);
-    for (long long k = 0; k < n; k++) in[k] = PolishIn{cands[k].r, cands[k].z, cands[k].numharm, 0};
+    // -noharmpolish (src/accel_utils.c:585-611): max_rz_arr for each harmonic
+    // on its own at (r h, z h); results gathered back per candidate below
+    const bool each = !obs->use_harmonic_polishing;
+    std::vector<PolishIn> in;
+    std::vector<long long> owner;
+    for (long long k = 0; k < n; k++) {
+        if (!each) {
+            in.push_back(PolishIn{cands[k].r, cands[k].z, cands[k].numharm, 0});
+            continue;
+        }
+        for (int ii = 0; ii < cands[k].numharm; ii++) {
+            in.push_back(PolishIn{cands[k].r * (ii + 1), cands[k].z * (ii + 1), 1, 1});
+            owner.push_back(k);
+        }
+    }
+    const long long nin = (long long) in.size();
+    if (nin > (1 << 24)) return fail(ctx, AB_ERR_ARG, "too many harmonics to polish");
+    std::vector<ab_polished> single(each ? (size_t) nin : 0);
+    ab_polished *hout = each ? single.data() : out;
     DevBuf<PolishIn> din;
     DevBuf<ab_polished> dout;
-    cudaError_t e = din.ensure((size_t) n);
-    if (e == cudaSuccess) e = dout.ensure((size_t) n);
+    cudaError_t e = din.ensure((size_t) nin);
+    if (e == cudaSuccess) e = dout.ensure((size_t) nin);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(din.p, in.data(), sizeof(PolishIn) * n, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = launch_polish(dfft, obs->numbins, obs->lobin, din.p, (int) n, dout.p, ctx->stream);
+        e = cudaMemcpyAsync(din.p, in.data(), sizeof(PolishIn) * nin, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = launch_polish(dfft, obs->numbins, obs->lobin, din.p, (int) nin, dout.p, ctx->stream);
     if (e == cudaSuccess) ctx->launches++;
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(out, dout.p, sizeof(ab_polished) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpyAsync(hout, dout.p, sizeof(ab_polished) * nin, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     din.release();
     dout.release();
     if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "candidate polishing failed: %s", cudaGetErrorString(e));
+    if (each) {
+        for (long long k = 0; k < n; k++) {
+            memset(&out[k], 0, sizeof out[k]);
+            out[k].numharm = cands[k].numharm;
+        }
+        std::vector<int> seen((size_t) n, 0);
+        for (long long q = 0; q < nin; q++) {
+            const long long k = owner[q];
+            const int ii = seen[k]++;
+            out[k].pows[ii] = single[q].pows[0];
+            out[k].hirs[ii] = single[q].hirs[0];      // r + lobin of the harmonic's own optimum
+            out[k].hizs[ii] = single[q].hizs[0];
+            out[k].hiws[ii] = 0.0;
+            out[k].derivs[ii] = single[q].derivs[0];
+        }
+    }
     return AB_OK;
 }
 

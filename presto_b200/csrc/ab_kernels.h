@@ -136,7 +136,8 @@ size_t tc_corr_smem(int nks_max);
 // candidate polishing (optimize_accelcand for acceleration searches)
 struct PolishIn {
     double r, z;
-    int numharm, pad;
+    int numharm;
+    int mode;                   // 0: max_rz_arr_harmonics, 1: max_rz_arr (one harmonic)
 };
 cudaError_t launch_polish(const float2 *data, long long numdata, long long lobin, const PolishIn *in,
                           int n, ab_polished *out, cudaStream_t st);
@@ -163,12 +164,14 @@ cudaError_t launch_rzw_jobs(const RzwJob *jobs, int njobs, const float2 *data, l
                             const double2 *tw, float2 *resp, double2 *acc, const long long *out_j,
                             float2 *out_amp, cudaStream_t st);
 // Per candidate c: harmonics' local powers from the amplitudes
-// amp[lp_off[c * 32 + h] ...] (lp_n of them; mean over NUMLOCPOWAVG = 20),
-// the float sum over harmonics of |vol|^2 / locpow in the reference's order
-// (volume amplitudes at amp[vol_off[c] + h * RZW_VOL + cell]) and the first
-// cell of the highest sum: best[c] = cell index.
+// amp[lp_off[c * 32 + h] ...] (lp_n of them; mean over NUMLOCPOWAVG = 20;
+// lp_n < 0: 1, raw powers), the float sum over harmonics of |vol|^2 / locpow
+// in the reference's order (volume amplitudes at amp[vol_off[c] + h * ncell +
+// cell]) and the first cell of the highest sum: best[c] = cell index,
+// bestval[c] (if not null) = that sum.
 cudaError_t launch_rzw_sum(const float2 *amp, const int *numharm, const int *vol_off,
-                           const int *lp_off, const int *lp_n, int ncand, int *best, cudaStream_t st);
+                           const int *lp_off, const int *lp_n, int ncell, int ncand, int *best,
+                           float *bestval, cudaStream_t st);
 // max_rzw_arr_harmonics for every candidate (host planning + the two
 // kernels above): data is the device spectrum of numdata bins, tw the FP64
 // table exp(-2 pi i m / 2^RZW_NMAX_LOG2), budget the response scratch per
@@ -176,6 +179,11 @@ cudaError_t launch_rzw_sum(const float2 *amp, const int *numharm, const int *vol
 int rzw_optimize(const float2 *data, long long numdata, long long lobin, const ab_cand *cands,
                  long long n, ab_polished *out, const double2 *tw, size_t budget, cudaStream_t st,
                  char *err, size_t errlen, long long *launches);
+// -noharmpolish: max_rzw_arr (src/maximize_rzw.c:3-52) for every harmonic
+// of every candidate, each on its own.
+int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, const ab_cand *cands,
+                      long long n, ab_polished *out, const double2 *tw, size_t budget,
+                      cudaStream_t st, char *err, size_t errlen, long long *launches);
 
 // time-series input path: realfft and deredden
 constexpr int AB_DERED_MAXW = 1024;     // longest de-reddening block

@@ -84,6 +84,7 @@ struct PolishSmem {
     double term[PL_MAXH];
     float locpow[PL_MAXH];
     double val;
+    int raw;                    // max_rz_arr: one harmonic, raw power (-noharmpolish)
 };
 
 // Amplitudes of items [0, n) (all threads).
@@ -153,13 +154,14 @@ __device__ double eval_harmonics(const float2 *data, long long numdata, int nh, 
     for (int ii = warp; ii < nh; ii += PL_WARPS) {
         const int n = ii + 1;
         const float2 a = warp_rz_interp(data, numdata, r * n, zs * PL_ZSCALE * n, kernhw, lane);
-        if (lane == 0) s.term[ii] = powerf2(a) / (double) s.locpow[ii];
+        if (lane == 0) s.term[ii] = s.raw ? powerf2(a) : powerf2(a) / (double) s.locpow[ii];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double total = 0.0;
         for (int ii = 0; ii < nh; ii++) total += s.term[ii];
-        s.val = isfinite(total) ? -total : 0.0;
+        // power_call_rz (src/maximize_rz.c:10-23) for one raw power
+        s.val = s.raw ? -total : (isfinite(total) ? -total : 0.0);
     }
     __syncthreads();
     const double v = s.val;
@@ -264,7 +266,8 @@ __global__ void __launch_bounds__(PL_THREADS) k_polish_rz(const float2 *data, lo
     __shared__ PolishSmem s;
     const PolishIn c = in[blockIdx.x];
     ab_polished &o = out[blockIdx.x];
-    const int nh = c.numharm < 1 ? 1 : (c.numharm > PL_MAXH ? PL_MAXH : c.numharm);
+    const int nh = c.mode == 1 ? 1 : (c.numharm < 1 ? 1 : (c.numharm > PL_MAXH ? PL_MAXH : c.numharm));
+    if (threadIdx.x == 0) s.raw = c.mode == 1;
     const double rin = c.r - (double) lobin, zin = c.z;
     local_powers(data, numdata, rin, zin, nh, s);
     double x[2] = {rin, zin / PL_ZSCALE};

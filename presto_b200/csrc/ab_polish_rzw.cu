@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(RZW_THREADS) k_rzw_jobs(const RzwJob *jobs, co
 // operation rounded on its own as the reference's scalar code rounds it.
 __global__ void __launch_bounds__(256) k_rzw_sum(const float2 *amp, const int *numharm,
                                                  const int *vol_off, const int *lp_off,
-                                                 const int *lp_n, int *best)
+                                                 const int *lp_n, int ncell, int *best,
+                                                 float *bestval)
 {
     __shared__ float s_locpow[AB_POLISH_MAX_HARM];
     __shared__ float s_p[256];
@@ -193,21 +194,23 @@ __global__ void __launch_bounds__(256) k_rzw_sum(const float2 *amp, const int *n
     const int c = blockIdx.x, nh = numharm[c];
     if ((int) threadIdx.x < nh) {
         const int h = threadIdx.x;
+        const int n = lp_n[c * AB_POLISH_MAX_HARM + h];
         const float2 *a = amp + lp_off[c * AB_POLISH_MAX_HARM + h];
         double sum = 0.0;
-        for (int m = 0; m < lp_n[c * AB_POLISH_MAX_HARM + h]; m++)
+        for (int m = 0; m < n; m++)
             sum = __dadd_rn(sum, __dadd_rn(__dmul_rn((double) a[m].x, (double) a[m].x),
                                            __dmul_rn((double) a[m].y, (double) a[m].y)));
-        s_locpow[h] = (float) (sum / 20.0);
+        // n < 0: raw powers (max_rzw_arr); x / 1 is x
+        s_locpow[h] = n < 0 ? 1.0f : (float) (sum / 20.0);
     }
     __syncthreads();
     float bp = 0.0f;
-    int bi = RZW_VOL;                       // none above zero yet
+    int bi = ncell;                         // none above zero yet
     const float2 *vol = amp + vol_off[c];
-    for (int cell = threadIdx.x; cell < RZW_VOL; cell += blockDim.x) {
+    for (int cell = threadIdx.x; cell < ncell; cell += blockDim.x) {
         float ps = 0.0f;
         for (int h = 0; h < nh; h++) {
-            const float2 v = vol[h * RZW_VOL + cell];
+            const float2 v = vol[h * ncell + cell];
             const float p = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
             ps = __fadd_rn(ps, __fdiv_rn(p, s_locpow[h]));
         }
@@ -230,7 +233,10 @@ __global__ void __launch_bounds__(256) k_rzw_sum(const float2 *amp, const int *n
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) best[c] = s_i[0] == RZW_VOL ? 0 : s_i[0];
+    if (threadIdx.x == 0) {
+        best[c] = s_i[0] == ncell ? 0 : s_i[0];
+        if (bestval) bestval[c] = s_i[0] == ncell ? 0.0f : s_p[0];
+    }
 }
 
 }  // namespace
@@ -249,10 +255,11 @@ cudaError_t launch_rzw_jobs(const RzwJob *jobs, int njobs, const float2 *data, l
 }
 
 cudaError_t launch_rzw_sum(const float2 *amp, const int *numharm, const int *vol_off,
-                           const int *lp_off, const int *lp_n, int ncand, int *best, cudaStream_t st)
+                           const int *lp_off, const int *lp_n, int ncell, int ncand, int *best,
+                           float *bestval, cudaStream_t st)
 {
     if (ncand <= 0) return cudaSuccess;
-    k_rzw_sum<<<ncand, 256, 0, st>>>(amp, numharm, vol_off, lp_off, lp_n, best);
+    k_rzw_sum<<<ncand, 256, 0, st>>>(amp, numharm, vol_off, lp_off, lp_n, ncell, best, bestval);
     return cudaGetLastError();
 }
 
@@ -553,7 +560,8 @@ int rzw_optimize(const float2 *data, long long numdata, long long lobin, const a
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_lpn, lp_n.data(), sizeof(int) * lp_n.size(), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
-            e = launch_rzw_sum((const float2 *) damp.p, d_nh, d_vol, d_lpo, d_lpn, (int) n, d_best, st);
+            e = launch_rzw_sum((const float2 *) damp.p, d_nh, d_vol, d_lpo, d_lpn, RZW_VOL, (int) n,
+                               d_best, nullptr, st);
         if (e == cudaSuccess) ++*launches;
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(best.data(), d_best, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
@@ -632,6 +640,169 @@ int rzw_optimize(const float2 *data, long long numdata, long long lobin, const a
             o.hizs[ii] = s.zout * (ii + 1);
             o.hiws[ii] = s.wout * (ii + 1);
         }
+    }
+    return AB_OK;
+}
+
+}  // namespace ab
+
+namespace ab {
+
+// -noharmpolish on a jerk search: max_rzw_arr (src/maximize_rzw.c:3-52) for
+// each harmonic of each candidate on its own, at (r h - lobin, z h, w h):
+// a 9 x 9 x 24 volume (z +- ACCEL_DZ, w +- ACCEL_DW, r from (int) r - 1 in
+// 1/8 bins) of raw powers, its first highest cell, and get_derivs3d there
+// with the local power taken at the starting point
+// (src/accel_utils.c:585-597).
+int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, const ab_cand *cands,
+                      long long n, ab_polished *out, const double2 *tw, size_t budget,
+                      cudaStream_t st, char *err, size_t errlen, long long *launches)
+{
+    constexpr int numz = 2 * kInterpFac + 1, ncell = numz * numz * kNumR;
+    struct Entry {
+        long long k;
+        int ii;
+        double rin, zin, win;
+        long long startbin;
+        int lp_off, lp_n, d_idx[5];
+    };
+    std::vector<Entry> es;
+    for (long long k = 0; k < n; k++)
+        for (int ii = 0; ii < cands[k].numharm; ii++) {
+            Entry e{};
+            e.k = k;
+            e.ii = ii;
+            e.rin = cands[k].r * (ii + 1) - (double) lobin;
+            e.zin = cands[k].z * (ii + 1);
+            e.win = cands[k].w * (ii + 1);
+            es.push_back(e);
+        }
+    const long long ne = (long long) es.size();
+    if (ne > (1 << 24)) {
+        snprintf(err, errlen, "too many harmonics to polish");
+        return AB_ERR_ARG;
+    }
+    Plan pv;
+    pv.numdata = numdata;
+    std::vector<int> nh((size_t) ne, 1), vol_off((size_t) ne);
+    std::vector<int> lp_off((size_t) ne * AB_POLISH_MAX_HARM, 0), lp_n((size_t) ne * AB_POLISH_MAX_HARM, -1);
+    for (long long q = 0; q < ne; q++) {
+        Entry &e = es[q];
+        e.startbin = (long long) (int) e.rin - 1;
+        const double zlo = e.zin - kAccelDZ, zhi = e.zin + kAccelDZ;
+        const double wlo = e.win - kAccelDW, whi = e.win + kAccelDW;
+        const double dz = (zhi - zlo) / (numz - 1), dw = (whi - wlo) / (numz - 1);
+        const double maxz = (fabs(zlo) < fabs(zhi)) ? zhi : zlo;
+        const double maxw = (fabs(wlo) < fabs(whi)) ? whi : wlo;
+        const int hw = w_halfwidth(maxz, maxw, false);
+        vol_off[q] = pv.outputs();
+        for (int iw = 0; iw < numz; iw++)
+            for (int jz = 0; jz < numz; jz++) {
+                const double z = zlo + jz * dz, w = wlo + iw * dw;
+                pv.open(fabs(w) < 1E-4 ? 0 : 1, 0.0, z, w, kRzwNb, hw, e.startbin - hw, 0);
+                for (int kk = 1; kk < kNumR; kk++) pv.add_output(kk);
+            }
+    }
+    if (pv.bad) {
+        snprintf(err, errlen, "%s", pv.msg);
+        return AB_ERR_ARG;
+    }
+    DevMem djobs, dresp, dacc, dj, damp, dsmall;
+    cudaError_t e = run_plan(pv, data, tw, budget, djobs, dresp, dacc, dj, damp, st, launches);
+    std::vector<int> best((size_t) ne, 0);
+    std::vector<float> bestval((size_t) ne, 0.0f);
+    const size_t small = sizeof(int) * ((size_t) ne * (4 + 2 * AB_POLISH_MAX_HARM));
+    if (e == cudaSuccess) e = dsmall.ensure(small);
+    if (e == cudaSuccess) {
+        int *d = (int *) dsmall.p;
+        int *d_nh = d, *d_vol = d + ne, *d_lpo = d + 2 * ne, *d_lpn = d_lpo + ne * AB_POLISH_MAX_HARM;
+        int *d_best = d_lpn + ne * AB_POLISH_MAX_HARM;
+        float *d_val = reinterpret_cast<float *>(d_best + ne);
+        e = cudaMemcpyAsync(d_nh, nh.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_vol, vol_off.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_lpo, lp_off.data(), sizeof(int) * lp_off.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_lpn, lp_n.data(), sizeof(int) * lp_n.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = launch_rzw_sum((const float2 *) damp.p, d_nh, d_vol, d_lpo, d_lpn, ncell, (int) ne,
+                               d_best, d_val, st);
+        if (e == cudaSuccess) ++*launches;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(best.data(), d_best, sizeof(int) * ne, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(bestval.data(), d_val, sizeof(float) * ne, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) {
+        snprintf(err, errlen, "jerk polishing (volumes): %s", cudaGetErrorString(e));
+        return AB_ERR_CUDA;
+    }
+    // the optimum, the starting point's local power and the derivatives
+    Plan pd;
+    pd.numdata = numdata;
+    const double h = 0.003, twoh = 0.006, twohsqrd = 0.000036;
+    std::vector<double> rout((size_t) ne), zout((size_t) ne), wout((size_t) ne);
+    for (long long q = 0; q < ne; q++) {
+        Entry &en = es[q];
+        const int cell = best[q], wind = cell / (numz * kNumR), zind = (cell / kNumR) % numz;
+        const int rind = cell % kNumR;
+        rout[q] = en.startbin + rind * 0.5 / (double) kInterpFac;
+        zout[q] = en.zin - kAccelDZ + zind * 2 / (double) kInterpFac;
+        wout[q] = en.win - kAccelDW + wind * 20 / (double) kInterpFac;
+        en.lp_off = pd.localpower(en.rin, en.zin, en.win, &en.lp_n);
+        const int hw = w_halfwidth(zout[q], wout[q], true);
+        double f = rout[q] - twoh;
+        for (int p = 0; p < 5; p++, f += h) en.d_idx[p] = pd.point(f, zout[q], wout[q], hw, false);
+    }
+    if (pd.bad) {
+        snprintf(err, errlen, "%s", pd.msg);
+        return AB_ERR_ARG;
+    }
+    e = run_plan(pd, data, tw, budget, djobs, dresp, dacc, dj, damp, st, launches);
+    std::vector<float2> amp(pd.js.size());
+    if (e == cudaSuccess && !amp.empty())
+        e = cudaMemcpyAsync(amp.data(), damp.p, sizeof(float2) * amp.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        snprintf(err, errlen, "jerk polishing (derivatives): %s", cudaGetErrorString(e));
+        return AB_ERR_CUDA;
+    }
+    for (long long k = 0; k < n; k++) {
+        memset(&out[k], 0, sizeof out[k]);
+        out[k].numharm = cands[k].numharm;
+    }
+    for (long long q = 0; q < ne; q++) {
+        const Entry &en = es[q];
+        ab_polished &o = out[en.k];
+        double sum = 0.0;
+        for (int m = 0; m < en.lp_n; m++) {
+            const float2 a = amp[en.lp_off + m];
+            sum += (double) a.x * a.x + (double) a.y * a.y;
+        }
+        const float locpow = (float) (sum / 20.0);
+        double pwr[5], phs[5];
+        for (int p = 0; p < 5; p++) {
+            const int idx = en.d_idx[p];
+            const float2 a = idx >= 0 ? amp[idx] : make_float2(0.f, 0.f);
+            pwr[p] = (double) a.x * a.x + (double) a.y * a.y;
+            phs[p] = radian_phase(a.x, a.y);
+        }
+        for (int p = 0; p < 4; p++)
+            if (fabs(phs[p + 1] - phs[p]) > kPi) phs[p + 1] -= kTwoPi;
+        ab_rderivs &d = o.derivs[en.ii];
+        d.pow = pwr[2];
+        d.phs = phs[2];
+        d.dpow = (pwr[3] - pwr[1]) / twoh;
+        d.dphs = (phs[3] - phs[1]) / twoh;
+        d.d2pow = (pwr[4] - 2.0 * pwr[2] + pwr[0]) / twohsqrd;
+        d.d2phs = (phs[4] - 2.0 * phs[2] + phs[0]) / twohsqrd;
+        d.locpow = locpow;
+        o.pows[en.ii] = bestval[q];
+        o.hirs[en.ii] = rout[q] + (double) lobin;
+        o.hizs[en.ii] = zout[q];
+        o.hiws[en.ii] = wout[q];
     }
     return AB_OK;
 }

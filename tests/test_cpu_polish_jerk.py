@@ -143,3 +143,21 @@ def test_acceleration_branch_unchanged(oracle):
     for k in ("pows", "hirs", "hizs", "derivs"):
         np.testing.assert_array_equal(a[k], b[k])
     assert not np.any(b["hiws"])
+
+
+def test_max_rzw_arr_single_harmonic(oracle, jerk_case):
+    """max_rzw_arr (the -noharmpolish path): a 9 x 9 x 24 grid, z +- 2 and
+    w +- 20 around the start; started within half of that from the injected
+    (r, z, w) it recovers them within one step (1/8 bin, 0.5, 5)."""
+    ft, cands = jerk_case
+    rng = np.random.default_rng(77)
+    for numharm, r, z, w, *_ in cands:
+        if numharm != 1:
+            continue
+        rs, zs, ws = r + rng.uniform(-0.4, 0.4), z + rng.uniform(-1, 1), w + rng.uniform(-10, 10)
+        p, ro, zo, wo, rd = oracle.max_rzw_arr(ft, rs, zs, ws)
+        assert abs(ro - r) <= 0.125 and abs(zo - z) <= 0.5 and abs(wo - w) <= 5.0, (ro - r, zo - z, wo - w)
+        assert 0.95 <= p / THEO_POW <= 1.05
+        # the grid: r from (int) rs - 1 in 1/8 bins, z and w from the start
+        assert abs((ro - (int(rs) - 1)) * 8 - round((ro - (int(rs) - 1)) * 8)) < 1e-9
+        assert abs((zo - (zs - 2.0)) / 0.5 - round((zo - (zs - 2.0)) / 0.5)) < 1e-9

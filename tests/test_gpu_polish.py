@@ -92,3 +92,30 @@ def test_device_polish_search_candidates(ctx, ablib, oracle):
     dev = ctx.optimize_cands(obs, fft, cands)
     orc = oracle.optimize_cands(fft, obs.lobin, [(c[2], c[3], c[4]) for c in cands], nthreads=8)
     _agree(dev, orc, "search")
+
+
+def test_device_noharmpolish_accel(ctx, ablib, oracle):
+    """-noharmpolish: max_rz_arr for every harmonic on its own at (r n, z n)
+    (src/accel_utils.c:598-611), device against the oracle's max_rz_arr."""
+    fails = []
+    for z in HARM_Z_VALUES:
+        ft = harmonic_signal(R_HARM, z, 3, 1.0, 4321)
+        obs = ablib.obs_init(ablib.make_params(N, DT, ft.size, zmax=100, wmax=0, numharm=4,
+                                               noharmpolish=True))
+        assert obs.use_harmonic_polishing == 0
+        dr, dz = HARM_OFFSETS[1]
+        dev = ctx.optimize_cands(obs, ft, [(0.0, 0.0, 3, R_HARM + dr, z + dz, 0.0)])[0]
+        for ii in range(3):
+            n = ii + 1
+            p, ro, zo, rd = oracle.max_rz_arr(ft, (R_HARM + dr) * n, (z + dz) * n)
+            ok = (abs(dev["hirs"][ii] - ro) <= 2e-3 and abs(dev["hizs"][ii] - zo) <= 1e-2 and
+                  abs(dev["pows"][ii] - p) <= 1e-3 * p and
+                  # local power: relative, or against the peak (the 20 points sit at
+                  # integer offsets from each side's optimum, which differ by ~1e-4
+                  # bins, so a strong tone's leakage into them differs), as _agree
+                  abs(dev["derivs"][ii][6] - rd.locpow) <= 1e-3 * rd.locpow + 1e-6 * p)
+            if not ok:
+                fails.append(f"z={z} n={n} r {dev['hirs'][ii]!r} {ro!r} z {dev['hizs'][ii]!r} {zo!r} "
+                             f"pow {dev['pows'][ii]!r} {p!r} locpow {dev['derivs'][ii][6]!r} "
+                             f"{rd.locpow!r}")
+    assert not fails, fails

@@ -115,3 +115,25 @@ def test_device_rzw_search_candidates(ctx, ablib, oracle):
     orc = oracle.optimize_cands_w(ft, obs.lobin, [(c[2], c[3], c[4], c[5]) for c in top], jerk=True,
                                   nthreads=os.cpu_count() or 1)
     _agree(dev, orc, "search")
+
+
+def test_device_noharmpolish_jerk(ctx, ablib, oracle, jerk_case):
+    """-noharmpolish: max_rzw_arr for every harmonic on its own
+    (src/accel_utils.c:585-597), device against the oracle: the same grid
+    cell, the volume's maximum power as the harmonic's power, derivatives
+    with the starting point's local power."""
+    ft, cands = jerk_case
+    obs = ablib.obs_init(ablib.make_params(N, DT, ft.size, zmax=100, wmax=300, numharm=4,
+                                           noharmpolish=True))
+    assert obs.use_harmonic_polishing == 0
+    sel = [c for c in cands if c[0] <= 2]
+    dev = ctx.optimize_cands(obs, ft, [(0.0, 0.0, c[0], c[4], c[5], c[6]) for c in sel])
+    for c, d in zip(sel, dev):
+        for ii in range(c[0]):
+            n = ii + 1
+            p, ro, zo, wo, rd = oracle.max_rzw_arr(ft, c[4] * n, c[5] * n, c[6] * n)
+            assert (d["hirs"][ii], d["hizs"][ii], d["hiws"][ii]) == (ro, zo, wo), (c, ii)
+            assert abs(d["pows"][ii] - p) <= 1e-5 * p
+            dd = d["derivs"][ii]
+            assert abs(dd[0] - rd.pow) <= 1e-4 * rd.pow
+            assert abs(dd[6] - rd.locpow) <= 1e-4 * rd.locpow
