@@ -24,7 +24,7 @@
 namespace ab {
 namespace {
 
-constexpr int PL_THREADS = 256;
+constexpr int PL_THREADS = 512;
 constexpr int PL_WARPS = PL_THREADS / 32;
 constexpr int PL_MAXH = AB_POLISH_MAX_HARM;
 constexpr int PL_LOCPOW = 20;                 // NUMLOCPOWAVG, include/presto.h:99
@@ -37,17 +37,27 @@ __device__ __forceinline__ int z_halfwidth(double z, bool highacc)   // src/resp
     return (int) (0.5 * 1.1 * fabs(z)) + (highacc ? 48 : 16);
 }
 
-// rz_interp at (r, z) with kernel half-width hw, by one warp.
-__device__ float2 warp_rz_interp(const float2 *data, long long numdata, double r, double z, int hw,
-                                 int lane)
+// rz_interp (src/rzinterp.c:144-232) at (r, z) with kernel half-width hw,
+// shared by P warps: this lane of warp part sums kernel points lane + 32 (part
+// + P k) in FP64.  The lanes' and parts' sums add up to the amplitude; the
+// exact-bin cases come from lane 0 of part 0 alone.
+__device__ double2 rz_interp_part(const float2 *data, long long numdata, double r, double z, int hw,
+                                  int part, int P, int lane)
 {
-    if (r > numdata - 1.0 || r < 0.0) return make_float2(0.f, 0.f);
+    if (r > numdata - 1.0 || r < 0.0) return make_double2(0.0, 0.0);
     double dint;
     const double frac = modf(r, &dint);
     const long long intfreq = (long long) dint;
     if (fabs(z) < 1E-4) {
-        if (frac < 1E-5) return data[intfreq];
-        if ((1.0 - frac) < 1E-5) return data[intfreq + 1];
+        const bool first = part == 0 && lane == 0;
+        if (frac < 1E-5) {
+            const float2 v = data[intfreq];
+            return first ? make_double2(v.x, v.y) : make_double2(0.0, 0.0);
+        }
+        if ((1.0 - frac) < 1E-5) {
+            const float2 v = data[intfreq + 1];
+            return first ? make_double2(v.x, v.y) : make_double2(0.0, 0.0);
+        }
     }
     const int numkern = 2 * hw;
     long long lodata = intfreq - hw, loresp = 0;
@@ -59,19 +69,32 @@ __device__ float2 warp_rz_interp(const float2 *data, long long numdata, double r
     const long long hiresp = (hidata > numdata - 1) ? numkern - hidata + numdata - 1 : numkern;
     const long long nsum = hiresp - loresp;
     double ar = 0.0, ai = 0.0;
-    for (long long ii = lane; ii < nsum; ii += 32) {
+    for (long long ii = lane + 32 * part; ii < nsum; ii += 32 * P) {
         const double2 pv = z_resp_point(frac, 1, z, numkern, (int) (loresp + ii));
         const float pr = (float) pv.x, pim = (float) pv.y;      // the reference's response is float
         const float2 d = data[lodata + ii];
         ar += (double) d.x * (double) pr + (double) __fmul_rn(d.y, pim);
         ai += (double) d.y * (double) pr - (double) pim * (double) d.x;
     }
+    return make_double2(ar, ai);
+}
+
+__device__ __forceinline__ double2 warp_sum(double2 v)
+{
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
-        ar += __shfl_xor_sync(0xffffffffu, ar, o);
-        ai += __shfl_xor_sync(0xffffffffu, ai, o);
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
     }
-    return make_float2((float) ar, (float) ai);
+    return v;
+}
+
+// rz_interp by one warp.
+__device__ float2 warp_rz_interp(const float2 *data, long long numdata, double r, double z, int hw,
+                                 int lane)
+{
+    const double2 v = warp_sum(rz_interp_part(data, numdata, r, z, hw, 0, 1, lane));
+    return make_float2((float) v.x, (float) v.y);
 }
 
 __device__ __forceinline__ double powerf2(float2 a) { return (double) a.x * a.x + (double) a.y * a.y; }
@@ -83,6 +106,7 @@ struct PolishSmem {
     int cnt[PL_MAXH];
     double term[PL_MAXH];
     float locpow[PL_MAXH];
+    double2 part[PL_MAXH];      // per-warp partial amplitudes of one evaluation
     double val;
     int raw;                    // max_rz_arr: one harmonic, raw power (-noharmpolish)
 };
@@ -150,16 +174,28 @@ __device__ void local_powers(const float2 *data, long long numdata, double r, do
 __device__ double eval_harmonics(const float2 *data, long long numdata, int nh, int kernhw, double r,
                                  double zs, PolishSmem &s)
 {
+    // P warps per harmonic (all warps busy for few harmonics)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int ii = warp; ii < nh; ii += PL_WARPS) {
-        const int n = ii + 1;
-        const float2 a = warp_rz_interp(data, numdata, r * n, zs * PL_ZSCALE * n, kernhw, lane);
-        if (lane == 0) s.term[ii] = s.raw ? powerf2(a) : powerf2(a) / (double) s.locpow[ii];
+    const int P = nh >= PL_WARPS ? 1 : PL_WARPS / nh;
+    for (int w = warp; w < nh * P; w += PL_WARPS) {
+        const int ii = w / P, n = ii + 1;
+        const double2 v = warp_sum(rz_interp_part(data, numdata, r * n, zs * PL_ZSCALE * n, kernhw,
+                                                  w - ii * P, P, lane));
+        if (lane == 0) s.part[w] = v;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double total = 0.0;
-        for (int ii = 0; ii < nh; ii++) total += s.term[ii];
+        for (int ii = 0; ii < nh; ii++) {
+            double ar = 0.0, ai = 0.0;
+            for (int q = 0; q < P; q++) {
+                ar += s.part[ii * P + q].x;
+                ai += s.part[ii * P + q].y;
+            }
+            const float2 a = make_float2((float) ar, (float) ai);
+            s.term[ii] = s.raw ? powerf2(a) : powerf2(a) / (double) s.locpow[ii];
+            total += s.term[ii];
+        }
         // power_call_rz (src/maximize_rz.c:10-23) for one raw power
         s.val = s.raw ? -total : (isfinite(total) ? -total : 0.0);
     }
