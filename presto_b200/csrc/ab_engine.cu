@@ -697,22 +697,40 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             // the item upload is reused by the next pass: wait before overwriting
             CK(cudaStreamSynchronize(ctx->stream));
         }
-        CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(unsigned), ctx->stream));
-        if (count > 0) {
-            BlockBatch bb{ctx->startr.p + first, first, (int) count, 0};
-            HitBuf hb{ctx->keys.p, ctx->pows.p, ctx->count.p, ctx->hit_cap};
+        // the sums run in chunks of blocks through the ring of hit sets, so the
+        // host replays chunk k while the device sums the chunks after it
+        const long long nch = std::min<long long>(8, std::max<long long>(1, count / 32));
+        const long long csz = (count + nch - 1) / nch;
+        int k = 0;
+        for (long long c0 = first; count > 0 && c0 < first + count; c0 += csz, k++) {
+            const int nb = (int) std::min<long long>(csz, first + count - c0);
+            const int set = k % ab_ctx::kHitSets;
+            HitSet h = hitset(ctx, set);
+            CK(cudaMemsetAsync(h.count, 0, sizeof(unsigned), ctx->stream));
+            BlockBatch bb{ctx->startr.p + c0, c0, nb, 0};
+            HitBuf hb{h.keys, h.pows, h.count, ctx->hit_cap};
+            const bool dump = dbg_block >= c0 && dbg_block < c0 + nb;
             tick(ctx, 3, true);
             cudaError_t e = launch_harmsum_inmem(sc, bb, ctx->fullplane.p, hb,
-                                                 dbg_block >= 0 ? ctx->dbg.p : nullptr,
-                                                 (int) (dbg_block - first), ctx->stream);
+                                                 dump ? ctx->dbg.p : nullptr,
+                                                 dump ? (int) (dbg_block - c0) : -1, ctx->stream);
             tick(ctx, 3, false);
             ctx->launches++;
             if (e != cudaSuccess)
                 return fail(ctx, AB_ERR_CUDA, "harmonic sum launch failed: %s", cudaGetErrorString(e));
+            rc = close_hitset(ctx, obs, set);
+            if (rc) return rc;
+            if (k >= ab_ctx::kHitSets - 1) {
+                rc = drain_hitset(ctx, obs, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, list,
+                                  replay_ms);
+                if (rc) return rc;
+            }
         }
-        rc = close_hitset(ctx, obs, 0);
-        if (rc) return rc;
-        return drain_hitset(ctx, obs, 0, list, replay_ms);
+        for (int d = std::max(0, k - (ab_ctx::kHitSets - 1)); d < k; d++) {
+            rc = drain_hitset(ctx, obs, d % ab_ctx::kHitSets, list, replay_ms);
+            if (rc) return rc;
+        }
+        return AB_OK;
     }
 
     // standard mode: batches of blocks, each correlated for every bank, then
