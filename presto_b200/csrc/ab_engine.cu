@@ -669,33 +669,53 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         } else {
             CK(ctx->xhat.ensure((size_t) std::max<long long>(nall, 1) * bs.xhat_per_block));
         }
-        CorrPlan plan;
-        std::vector<TcItem> tplan;
+        // both passes' work items are built first and uploaded once, each pass
+        // reading its own part, so the passes follow each other on the stream
+        CorrPlan plan[2];
+        std::vector<TcItem> tplan[2];
+        size_t ioff[2] = {0, 0}, itotal = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            const long long nb = pass == 0 ? npre : nmain;
+            ioff[pass] = itotal;
+            if (nb == 0) continue;
+            if (tcp) {
+                build_tc_plan(ctx->cur_bank->tc, bs, (int) nb, 0, 1, tplan[pass]);
+                itotal += tplan[pass].size();
+            } else {
+                build_corr_plan(bs, sc, (int) nb, 0, 1, plan[pass]);
+                itotal += plan[pass].items.size();
+            }
+        }
+        if (tcp) {
+            CK(ctx->titems.ensure(std::max<size_t>(itotal, 1)));
+            for (int pass = 0; pass < 2; pass++)
+                if (!tplan[pass].empty())
+                    CK(cudaMemcpyAsync(ctx->titems.p + ioff[pass], tplan[pass].data(),
+                                       sizeof(TcItem) * tplan[pass].size(), cudaMemcpyHostToDevice,
+                                       ctx->stream));
+        } else {
+            CK(ctx->items.ensure(std::max<size_t>(itotal, 1)));
+            for (int pass = 0; pass < 2; pass++)
+                if (!plan[pass].items.empty())
+                    CK(cudaMemcpyAsync(ctx->items.p + ioff[pass], plan[pass].items.data(),
+                                       sizeof(CorrItem) * plan[pass].items.size(),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+        }
         for (int pass = 0; pass < 2; pass++) {
             long long nb = pass == 0 ? npre : nmain;
             if (nb == 0) continue;
             BlockBatch bb{ctx->startr.p + (pass == 0 ? nmain : 0), 0, (int) nb, pass == 0};
             if (tcp) {
-                build_tc_plan(ctx->cur_bank->tc, bs, (int) nb, 0, 1, tplan);
-                CK(ctx->titems.ensure(tplan.size()));
-                CK(cudaMemcpyAsync(ctx->titems.p, tplan.data(), sizeof(TcItem) * tplan.size(),
-                                   cudaMemcpyHostToDevice, ctx->stream));
-                rc = run_tc(ctx, sc, bb, dfft, 0, 1, ctx->titems.p, (int) tplan.size(), nullptr, 0,
-                            ctx->fullplane.p);
+                rc = run_tc(ctx, sc, bb, dfft, 0, 1, ctx->titems.p + ioff[pass], (int) tplan[pass].size(),
+                            nullptr, 0, ctx->fullplane.p);
                 if (rc) return rc;
-                CK(cudaStreamSynchronize(ctx->stream));
                 continue;
             }
             rc = run_prep(ctx, sc, bb, dfft, 0, 1);
             if (rc) return rc;
-            build_corr_plan(bs, sc, (int) nb, 0, 1, plan);
-            CK(ctx->items.ensure(plan.items.size()));
-            CK(cudaMemcpyAsync(ctx->items.p, plan.items.data(), sizeof(CorrItem) * plan.items.size(),
-                               cudaMemcpyHostToDevice, ctx->stream));
-            rc = run_corr(ctx, sc, bb, plan, ctx->items.p, nullptr, 0, ctx->fullplane.p);
+            rc = run_corr(ctx, sc, bb, plan[pass], ctx->items.p + ioff[pass], nullptr, 0,
+                          ctx->fullplane.p);
             if (rc) return rc;
-            // the item upload is reused by the next pass: wait before overwriting
-            CK(cudaStreamSynchronize(ctx->stream));
         }
         // the sums run in chunks of blocks through the ring of hit sets, so the
         // host replays chunk k while the device sums the chunks after it
