@@ -75,7 +75,9 @@ typedef struct {
     float nph, sigma;
     float powcut[6];
     long long numindep[6];
-    int use_harmonic_polishing;   /* 0 with -noharmpolish (src/accel_utils.c:1489-1494) */
+    int noharmpolish;             /* 1: -noharmpolish, each harmonic polished alone
+                                     (use_harmonic_polishing = 0, src/accel_utils.c:1489-1494);
+                                     0, the default, in a zero-filled ab_obs */
 } ab_obs;
 
 /* accelcand search fields (include/accel.h:83-95). */

@@ -131,7 +131,7 @@ int orc_obs_init(const orc_params *p, orc_obs *obs)
     obs->numbins = p->numbins;
     obs->nph = p->nph > 0 ? p->nph : 0.0f;
     obs->norm_type = (p->nph > 0 || !p->locpowP) ? 0 : 1;     /* src/accel_utils.c:1598-1620 */
-    obs->use_harmonic_polishing = !p->noharmpolishP;
+    obs->noharmpolish = p->noharmpolishP ? 1 : 0;
     obs->lobin = p->lobin;
     if (obs->lobin > 0) {
         obs->nph = 0.0f;

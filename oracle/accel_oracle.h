@@ -58,7 +58,7 @@ typedef struct {
     float nph, sigma;
     float powcut[6];
     long long numindep[6];
-    int use_harmonic_polishing;   /* src/accel_utils.c:1489-1494 */
+    int noharmpolish;             /* 1: -noharmpolish (src/accel_utils.c:1489-1494) */
 } orc_obs;
 
 /* One plane (ffdotpows, include/accel.h:120-130), powers[w][z][r]. */

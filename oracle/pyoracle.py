@@ -34,7 +34,7 @@ class Obs(C.Structure):
                 ("wlo", C.c_double), ("whi", C.c_double), ("dw", C.c_double),
                 ("nph", C.c_float), ("sigma", C.c_float),
                 ("powcut", C.c_float * 6), ("numindep", C.c_longlong * 6),
-                ("use_harmonic_polishing", C.c_int)]
+                ("noharmpolish", C.c_int)]
 
 
 class FFDot(C.Structure):

@@ -1104,7 +1104,7 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
         }
         char msg[256] = {0};
         const size_t budget = std::min<size_t>(ctx->scratch_budget, 1ull << 30);
-        rc = obs->use_harmonic_polishing
+        rc = !obs->noharmpolish
                  ? rzw_optimize(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p, budget,
                                 ctx->stream, msg, sizeof msg, &ctx->launches)
                  : rzw_optimize_each(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p,
@@ -1114,7 +1114,7 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
     }
     // -noharmpolish (src/accel_utils.c:585-611): max_rz_arr for each harmonic
     // on its own at (r h, z h); results gathered back per candidate below
-    const bool each = !obs->use_harmonic_polishing;
+    const bool each = obs->noharmpolish != 0;
     std::vector<PolishIn> in;
     std::vector<long long> owner;
     for (long long k = 0; k < n; k++) {

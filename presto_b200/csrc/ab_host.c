@@ -222,7 +222,7 @@ int ab_obs_init(const ab_params *p, ab_obs *obs)        /* src/accel_utils.c:159
     /* -photon takes precedence; otherwise -locpow selects the local-power
      * normalisation (src/accel_utils.c:1598-1620) */
     obs->norm_type = (p->nph > 0.0f || !p->locpowP) ? 0 : 1;
-    obs->use_harmonic_polishing = !p->noharmpolishP;
+    obs->noharmpolish = p->noharmpolishP ? 1 : 0;
     obs->lobin = p->lobin;
     if (obs->lobin > 0) {
         obs->nph = 0.0f;

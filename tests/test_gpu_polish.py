@@ -102,7 +102,7 @@ def test_device_noharmpolish_accel(ctx, ablib, oracle):
         ft = harmonic_signal(R_HARM, z, 3, 1.0, 4321)
         obs = ablib.obs_init(ablib.make_params(N, DT, ft.size, zmax=100, wmax=0, numharm=4,
                                                noharmpolish=True))
-        assert obs.use_harmonic_polishing == 0
+        assert obs.noharmpolish == 1
         dr, dz = HARM_OFFSETS[1]
         dev = ctx.optimize_cands(obs, ft, [(0.0, 0.0, 3, R_HARM + dr, z + dz, 0.0)])[0]
         for ii in range(3):

@@ -125,7 +125,7 @@ def test_device_noharmpolish_jerk(ctx, ablib, oracle, jerk_case):
     ft, cands = jerk_case
     obs = ablib.obs_init(ablib.make_params(N, DT, ft.size, zmax=100, wmax=300, numharm=4,
                                            noharmpolish=True))
-    assert obs.use_harmonic_polishing == 0
+    assert obs.noharmpolish == 1
     sel = [c for c in cands if c[0] <= 2]
     dev = ctx.optimize_cands(obs, ft, [(0.0, 0.0, c[0], c[4], c[5], c[6]) for c in sel])
     for c, d in zip(sel, dev):
