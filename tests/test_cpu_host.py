@@ -149,3 +149,15 @@ def test_fourier_amplitudes_and_copy(ablib):
     assert np.array_equal(dst_pw[:src_pw.size], src_pw)
     small = F(0, 0, 0, 0, 0, 0, dst_pw.ctypes.data_as(C.POINTER(C.c_float)), 5)
     assert ablib.lib().ab_copy_ffdotpows(C.byref(src), C.byref(small)) == -4
+
+
+@pytest.mark.parametrize("bad", [dict(numharm=3), dict(numharm=64), dict(zmax=-2), dict(N=0),
+                                 dict(lobin=1 << 20), dict(wmax=-20)])
+def test_obs_init_rejects_bad_options(ablib, bad):
+    """The reference exits on these (src/accel_utils.c:1467-1487, clig ranges); the
+    C ABI returns AB_ERR_ARG and the Python mirror raises."""
+    kw = dict(N=1 << 18, zmax=50, numharm=8)
+    kw.update(bad)
+    N = kw.pop("N")
+    with pytest.raises(ablib.AccelError):
+        ablib.obs_init(ablib.make_params(N, 64e-6, max(N // 2, 1), **kw))
