@@ -7,8 +7,12 @@
 namespace ab {
 
 // ======================================================================
-// FP64 Fresnel integrals (power series / Lentz continued fraction for
-// erfc((1-i) sqrt(pi)/2 x), Numerical Recipes 2ed section 6.9).
+// FP64 Fresnel integrals: power series for x <= 1.8, Lentz continued
+// fraction for erfc((1-i) sqrt(pi)/2 x) up to 5.5 (Numerical Recipes 2ed
+// section 6.9), and above that the auxiliary functions' asymptotic series
+// (Abramowitz & Stegun 7.3.27-28; C and S from f and g by 7.3.9-10), whose
+// terms fall below 1e-18 within about a dozen steps there (3.6e-14 absolute
+// against Cephes' fresnl over 5.5..40).
 // ======================================================================
 __device__ __forceinline__ void fresnel64(double xin, double *s, double *c)
 {
@@ -31,6 +35,22 @@ __device__ __forceinline__ void fresnel64(double xin, double *s, double *c)
         }
         C = sc;
         S = ss;
+    } else if (x >= 5.5) {
+        const double px2 = M_PI * x * x, t = 1.0 / (px2 * px2);
+        double f = 1.0, g = 1.0, c = 1.0, d = 1.0;
+        for (int m = 1; m < 40; m++) {
+            c *= -(double) ((4 * m - 3) * (4 * m - 1)) * t;
+            d *= -(double) ((4 * m - 1) * (4 * m + 1)) * t;
+            f += c;
+            g += d;
+            if (fabs(c) < 1e-18 && fabs(d) < 1e-18) break;
+        }
+        f /= M_PI * x;
+        g /= M_PI * M_PI * x * x * x;
+        double sp, cp;
+        sincospi(0.5 * x * x, &sp, &cp);           // sin, cos(pi x^2 / 2)
+        C = 0.5 + f * sp - g * cp;
+        S = 0.5 - f * cp - g * sp;
     } else {
         const double fpmin = 1e-300;
         double px2 = M_PI * x * x;
