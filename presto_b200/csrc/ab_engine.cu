@@ -9,8 +9,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ab_host.h"
@@ -570,10 +574,92 @@ static int close_hitset(ab_ctx *ctx, const ab_obs *obs, int i)
     return AB_OK;
 }
 
-// Waits for hit set i, appends its hits to the context's host copy and, if
-// list is given, replays them (they all belong to blocks after those of any
-// earlier set, so set-by-set replay is the reference's visit order).
-static int drain_hitset(ab_ctx *ctx, const ab_obs *obs, int i, ab_list *list, double *replay_ms)
+// Replays the batches' threshold crossings into the candidate list on a
+// thread of its own, batch after batch in the order they are handed over (the
+// reference's visit order), while the search keeps launching batches: the
+// device never waits for the list.  The worker alone writes the list and the
+// context's host copy of the hits until finish() has joined it.
+struct Replayer {
+    struct Batch {
+        std::vector<unsigned long long> keys;
+        std::vector<float> pows, sigs;
+    };
+    ab_ctx *ctx;
+    const ab_obs *obs;
+    ab_list *list;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Batch> q;
+    bool closing = false;
+    int rc = AB_OK;
+    double ms = 0.0;
+    std::thread th;
+
+    Replayer(ab_ctx *c, const ab_obs *o, ab_list *l) : ctx(c), obs(o), list(l)
+    {
+        th = std::thread([this] { run(); });
+    }
+    ~Replayer() { finish(); }
+    void push(Batch &&b)
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            q.push_back(std::move(b));
+        }
+        cv.notify_one();
+    }
+    int finish()
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            closing = true;
+        }
+        cv.notify_one();
+        if (th.joinable()) th.join();
+        return rc;
+    }
+    void run()
+    {
+        for (;;) {
+            Batch b;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                cv.wait(lock, [this] { return closing || !q.empty(); });
+                if (q.empty()) return;
+                b = std::move(q.front());
+                q.pop_front();
+            }
+            const long long n = (long long) b.keys.size();
+            if (rc == AB_OK) {
+                const double t0 = now_ms();
+                const int r = ab_replay_hits(obs, b.keys.data(), b.pows.data(), b.sigs.data(), n,
+                                             ctx->hstart.data(), ab_num_blocks(obs), list);
+                ms += now_ms() - t0;
+                if (r) rc = r;
+            }
+            keep_hits(ctx, b.keys, b.pows, b.sigs);
+        }
+    }
+    // the context's copy of the search's hits (ab_last_hits); bounded: past
+    // 2^24 only the latest batches are kept
+    static void keep_hits(ab_ctx *ctx, const std::vector<unsigned long long> &k,
+                          const std::vector<float> &p, const std::vector<float> &sg)
+    {
+        if (ctx->hkeys.size() + k.size() > (size_t) 1 << 24) {
+            ctx->hkeys.clear();
+            ctx->hpows.clear();
+            ctx->hsigs.clear();
+            ctx->hits_truncated = true;
+        }
+        ctx->hkeys.insert(ctx->hkeys.end(), k.begin(), k.end());
+        ctx->hpows.insert(ctx->hpows.end(), p.begin(), p.end());
+        ctx->hsigs.insert(ctx->hsigs.end(), sg.begin(), sg.end());
+    }
+};
+
+// Waits for hit set i and copies its hits to the host, freeing the set for
+// the next batch; hands them to the replayer (or, without a list, keeps them).
+static int drain_hitset(ab_ctx *ctx, int i, Replayer *rp)
 {
     CK(cudaEventSynchronize(ctx->batch_done[i]));
     unsigned n = ctx->hcount[i];
@@ -584,32 +670,17 @@ static int drain_hitset(ab_ctx *ctx, const ab_obs *obs, int i, ab_list *list, do
     }
     if (n == 0) return AB_OK;
     HitSet h = hitset(ctx, i);
-    if (ctx->hkeys.size() + n > (size_t) 1 << 24) {
-        // keep host memory bounded: the replay only needs this batch
-        ctx->hkeys.clear();
-        ctx->hpows.clear();
-        ctx->hsigs.clear();
-        ctx->hits_truncated = true;
-    }
-    size_t old = ctx->hkeys.size();
-    ctx->hkeys.resize(old + n);
-    ctx->hpows.resize(old + n);
-    ctx->hsigs.resize(old + n);
-    CK(cudaMemcpyAsync(ctx->hkeys.data() + old, h.keys, sizeof(unsigned long long) * n,
-                       cudaMemcpyDeviceToHost, ctx->cstream));
-    CK(cudaMemcpyAsync(ctx->hpows.data() + old, h.pows, sizeof(float) * n, cudaMemcpyDeviceToHost,
+    Replayer::Batch b;
+    b.keys.resize(n);
+    b.pows.resize(n);
+    b.sigs.resize(n);
+    CK(cudaMemcpyAsync(b.keys.data(), h.keys, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost,
                        ctx->cstream));
-    CK(cudaMemcpyAsync(ctx->hsigs.data() + old, h.sigs, sizeof(float) * n, cudaMemcpyDeviceToHost,
-                       ctx->cstream));
+    CK(cudaMemcpyAsync(b.pows.data(), h.pows, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->cstream));
+    CK(cudaMemcpyAsync(b.sigs.data(), h.sigs, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->cstream));
     CK(cudaStreamSynchronize(ctx->cstream));
-    if (list) {
-        double t0 = now_ms();
-        int rc = ab_replay_hits(obs, ctx->hkeys.data() + old, ctx->hpows.data() + old,
-                                ctx->hsigs.data() + old, n, ctx->hstart.data(),
-                                ab_num_blocks(obs), list);
-        if (replay_ms) *replay_ms += now_ms() - t0;
-        if (rc) return fail(ctx, rc, "hit replay failed");
-    }
+    if (rp) rp->push(std::move(b));
+    else Replayer::keep_hits(ctx, b.keys, b.pows, b.sigs);
     return AB_OK;
 }
 
@@ -645,6 +716,15 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     ctx->hpows.clear();
     ctx->hsigs.clear();
     ctx->hits_truncated = false;
+    // with a list: the replay runs on its own thread (joined on every return)
+    std::unique_ptr<Replayer> rp(list ? new Replayer(ctx, obs, list) : nullptr);
+    auto finish_replay = [&]() -> int {
+        if (!rp) return AB_OK;
+        const int r = rp->finish();
+        if (replay_ms) *replay_ms += rp->ms;
+        if (r) return fail(ctx, r, "hit replay failed");
+        return AB_OK;
+    };
     const int nstage = obs->numharmstages;
     const size_t dbg_floats = (size_t) nstage * sc.numws * sc.numz * obs->corr_uselen;
     if (dbg_block >= 0) CK(ctx->dbg.ensure(dbg_floats));
@@ -741,16 +821,15 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             rc = close_hitset(ctx, obs, set);
             if (rc) return rc;
             if (k >= ab_ctx::kHitSets - 1) {
-                rc = drain_hitset(ctx, obs, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, list,
-                                  replay_ms);
+                rc = drain_hitset(ctx, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, rp.get());
                 if (rc) return rc;
             }
         }
         for (int d = std::max(0, k - (ab_ctx::kHitSets - 1)); d < k; d++) {
-            rc = drain_hitset(ctx, obs, d % ab_ctx::kHitSets, list, replay_ms);
+            rc = drain_hitset(ctx, d % ab_ctx::kHitSets, rp.get());
             if (rc) return rc;
         }
-        return AB_OK;
+        return finish_replay();
     }
 
     // standard mode: batches of blocks, each correlated for every bank, then
@@ -836,16 +915,15 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         rc = close_hitset(ctx, obs, set);
         if (rc) return rc;
         if (k >= ab_ctx::kHitSets - 1) {
-            rc = drain_hitset(ctx, obs, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, list,
-                              replay_ms);
+            rc = drain_hitset(ctx, (k - (ab_ctx::kHitSets - 1)) % ab_ctx::kHitSets, rp.get());
             if (rc) return rc;
         }
     }
     for (int d = std::max(0, k - (ab_ctx::kHitSets - 1)); d < k; d++) {
-        rc = drain_hitset(ctx, obs, d % ab_ctx::kHitSets, list, replay_ms);
+        rc = drain_hitset(ctx, d % ab_ctx::kHitSets, rp.get());
         if (rc) return rc;
     }
-    return AB_OK;
+    return finish_replay();
 }
 
 static int fetch_hits(ab_ctx *ctx, long long *nhits)
