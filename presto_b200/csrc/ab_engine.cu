@@ -1182,12 +1182,20 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
         }
         char msg[256] = {0};
         const size_t budget = std::min<size_t>(ctx->scratch_budget, 1ull << 30);
-        rc = !obs->noharmpolish
-                 ? rzw_optimize(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p, budget,
-                                ctx->stream, msg, sizeof msg, &ctx->launches)
-                 : rzw_optimize_each(dfft, obs->numbins, obs->lobin, cands, n, out, ctx->tw_rzw.p,
-                                     budget, ctx->stream, msg, sizeof msg, &ctx->launches);
-        if (rc) return fail(ctx, rc, "%s", msg);
+        // candidates in groups of at most 4096 harmonics bound each plan's host
+        // memory (about 7000 volume outputs per harmonic)
+        for (long long c0 = 0; c0 < n;) {
+            long long c1 = c0, nh = 0;
+            while (c1 < n && (c1 == c0 || nh + cands[c1].numharm <= 4096)) nh += cands[c1++].numharm;
+            rc = !obs->noharmpolish
+                     ? rzw_optimize(dfft, obs->numbins, obs->lobin, cands + c0, c1 - c0, out + c0,
+                                    ctx->tw_rzw.p, budget, ctx->stream, msg, sizeof msg, &ctx->launches)
+                     : rzw_optimize_each(dfft, obs->numbins, obs->lobin, cands + c0, c1 - c0, out + c0,
+                                         ctx->tw_rzw.p, budget, ctx->stream, msg, sizeof msg,
+                                         &ctx->launches);
+            if (rc) return fail(ctx, rc, "%s", msg);
+            c0 = c1;
+        }
         return AB_OK;
     }
     // -noharmpolish (src/accel_utils.c:585-611): max_rz_arr for each harmonic

@@ -488,6 +488,14 @@ int rzw_optimize(const float2 *data, long long numdata, long long lobin, const a
                  long long n, ab_polished *out, const double2 *tw, size_t budget, cudaStream_t st,
                  char *err, size_t errlen, long long *launches)
 {
+    // every output of the plan is indexed by int: bound the call's volume
+    long long nharm = 0;
+    for (long long c = 0; c < n; c++) nharm += cands[c].numharm;
+    if (nharm * (long long) (RZW_VOL + 64) > (1LL << 27)) {
+        snprintf(err, errlen, "%lld harmonics to polish in one call: at most %lld", nharm,
+                 (1LL << 27) / (RZW_VOL + 64));
+        return AB_ERR_ARG;
+    }
     std::vector<CandState> cs((size_t) n);
     Plan pv;
     pv.numdata = numdata;
@@ -678,8 +686,9 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
             es.push_back(e);
         }
     const long long ne = (long long) es.size();
-    if (ne > (1 << 24)) {
-        snprintf(err, errlen, "too many harmonics to polish");
+    if (ne * (long long) (ncell + 64) > (1LL << 27)) {
+        snprintf(err, errlen, "%lld harmonics to polish in one call: at most %lld", ne,
+                 (1LL << 27) / (ncell + 64));
         return AB_ERR_ARG;
     }
     Plan pv;
