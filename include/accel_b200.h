@@ -26,6 +26,8 @@
  *   ab_power_for_sigma      power_for_sigma           src/characteristics.c:549-559
  *   ab_gen_response         gen_w_response/gen_z_response/gen_r_response
  *                                                     src/responses.c:159-418
+ *   ab_write_accelfile      output_fundamentals +     src/accel_utils.c:666-966
+ *                           output_harmonics
  */
 #ifndef ACCEL_B200_H
 #define ACCEL_B200_H
@@ -341,6 +343,27 @@ typedef struct {
 int ab_calc_props(const ab_rderivs *d, double r, double z, double w, ab_fourierprops *out);
 int ab_calc_rzwerrs(const ab_fourierprops *props, double T, ab_rzwerrs *out);
 int ab_cand_props(const ab_cand *cands, const ab_polished *pol, long long n, ab_fourierprops *out);
+
+/* The text candidate file <root>_ACCEL_<zmax>[_JERK_<wmax>]: the
+ * fundamentals table (output_fundamentals, src/accel_utils.c:666-841) and
+ * the harmonics table (output_harmonics, src/accel_utils.c:844-966) of n
+ * sorted, polished candidates (out of ab_optimize_cands), with the .inf at
+ * inf_path appended as the reference's "cat <root>.inf >>" does (NULL or an
+ * unreadable file: nothing appended).  Notes are the candidates' own
+ * (compare_rzw_cands, src/accel_utils.c:105-134); the pulsar-catalogue notes
+ * of an observation with a telescope name are not made.  AB_ERR_ARG where
+ * the reference exits (a power or local power ~ 0, T <= 0, a value
+ * nice_output_2 cannot format) or the file cannot be written; nothing is
+ * written then.
+ *   ab_nice_output_1 / ab_nice_output_2  nice_output_1 / nice_output_2
+ *   (src/output.c:6-210) into out[outlen]: val(err) with a one- or two-digit
+ *   error, left-justified for len == 0, else right-justified to len; the
+ *   string length, or AB_ERR_ARG (no room, or nice_output_2's undefined
+ *   case). */
+int ab_write_accelfile(const char *path, const ab_obs *obs, const ab_cand *cands,
+                       const ab_polished *pol, long long n, const char *inf_path);
+int ab_nice_output_1(char *out, size_t outlen, double val, double err, int len);
+int ab_nice_output_2(char *out, size_t outlen, double val, double err, int len);
 
 /* The time-series input of create_accelobs (.dat files,
  * src/accel_utils.c:1516-1563) on the device:

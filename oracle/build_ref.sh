@@ -1,9 +1,13 @@
 #!/bin/sh
 # Compiles the parts of the reference's accelsearch path that build from the
 # reference's own source files with no external library, into oracle/_ref/.
-# Only src/fresnl.c (Cephes Fresnel integrals, used by gen_z_response at
-# src/responses.c:291-292) qualifies: every other hot-path file includes
-# ransomfft.h -> fftw3.h, or needs GSL / glib, none of which exist here.
+# src/fresnl.c (Cephes Fresnel integrals, used by gen_z_response at
+# src/responses.c:291-292) qualifies as is.  src/output.c (nice_output_1 /
+# nice_output_2, the value(error) format of the ACCEL text file) needs only
+# FFTW's type names through include/presto.h, which refshim/fftw3.h declares;
+# the library exports just those two functions, and --gc-sections drops the
+# file's other functions with their references to the rest of libpresto.
+# Every other hot-path file calls FFTW, GSL or glib, none of which exist here.
 # Nothing from the reference is copied into the repository; the objects land
 # in oracle/_ref/, which git ignores.
 set -e
@@ -17,3 +21,10 @@ fi
 mkdir -p "$OUT"
 $( [ -x /usr/bin/gcc ] && echo /usr/bin/gcc || echo gcc ) -O2 -g -fPIC -shared -o "$OUT/libref_fresnl.so" "$REF/src/fresnl.c" -lm
 echo "built $OUT/libref_fresnl.so from $REF/src/fresnl.c"
+CC=$( [ -x /usr/bin/gcc ] && echo /usr/bin/gcc || echo gcc )
+echo 'REF { global: nice_output_1; nice_output_2; local: *; };' > "$OUT/output.map"
+$CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" -I "$REF/include" \
+    -c "$REF/src/output.c" -o "$OUT/output.o"
+$CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/output.map" -o "$OUT/libref_output.so" \
+    "$OUT/output.o" -lm
+echo "built $OUT/libref_output.so from $REF/src/output.c"

@@ -433,3 +433,251 @@ def deredden(fft, startwidth=6, endwidth=200, endfreq=None, T=1.0):
     if n < 0:
         raise ValueError("deredden failed")
     return y
+
+
+# ---- the ACCEL text candidate file ------------------------------------------
+# output_fundamentals / output_harmonics (src/accel_utils.c:666-966),
+# compare_rzw_cands (src/accel_utils.c:105-134), center_string
+# (src/accel_utils.c:629-643) and nice_output_1 / nice_output_2
+# (src/output.c:6-210), restated in Python.  Python's % operator formats
+# these conversions as C's printf does and math.* calls the C library.
+import math  # noqa: E402
+
+DBLCORRECT = 1e-14
+SOL = 299792458.0
+
+
+class RzwErrs(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("p", "pd", "pdd", "f", "fd", "fdd")] + \
+               [(n, C.c_float) for n in ("perr", "pderr", "pdderr", "ferr", "fderr", "fdderr")]
+
+
+def ref_output_lib():
+    """The reference's own src/output.c built by build_ref.sh, or None."""
+    path = os.path.join(HERE, "_ref", "libref_output.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    for f in (L.nice_output_1, L.nice_output_2):
+        f.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_int]
+        f.restype = C.c_int
+    return L
+
+
+def _cint(x):
+    """C's (int) of a double on x86-64: truncation, INT_MIN when out of range."""
+    t = int(x)
+    return t if -2 ** 31 <= t < 2 ** 31 else -2 ** 31
+
+
+def _p(prec):
+    return prec if prec >= 0 else 6          # C: a negative '*' precision is omitted
+
+
+def _fin(s, length):
+    return s if length == 0 else "%*s" % (length, s)
+
+
+def nice_output_1(val, err, length=0):
+    """val(err), one error digit (src/output.c:6-111)."""
+    ee = 0 if abs(err) == 0.0 else math.floor(math.log10(abs(err)))
+    ev = _cint(math.floor(abs(err) * math.pow(10.0, -ee) + DBLCORRECT + 0.5))
+    if ev == 10:
+        ev, ee = 1, ee + 1
+    rv = math.pow(10.0, ee) * math.floor(val * math.pow(10.0, -ee) + 0.5)
+    nint = 1 if abs(val) == 0.0 else (math.ceil(math.log10(abs(val))) or 1)
+    nfrac = -ee
+    prec = nint + nfrac
+    oexp = 0 if abs(rv) == 0.0 else math.floor(math.log10(abs(rv)))
+    mant = rv * math.pow(10.0, -oexp)
+    if abs(1.0 - mant) < DBLCORRECT or abs(-1.0 - mant) < DBLCORRECT:
+        prec += 1
+    sm = -abs(mant) if rv < 0.0 else abs(mant)
+    if oexp >= 0 and ee > 0 and oexp > ee:
+        s = "% .*f(%d)x10^%d" % (_p(prec - 1), sm, ev, oexp)
+    elif oexp >= 0 and ee > 0 and oexp == ee:
+        s = "% d(%d)x10^%d" % (_cint(sm), ev, oexp)
+    elif oexp < -4 and oexp >= ee:
+        s = "% .*f(%d)x10^%d" % (_p(prec - 1), sm, ev, oexp)
+    elif oexp < ee and ee != 0:
+        s = "% d(%d)x10^%d" % (_cint(sm + DBLCORRECT), ev, ee)
+    elif nfrac == 0 and abs(rv) < 1.0e-15:
+        s = "% d(%d)" % (_cint(abs(rv)), ev)
+    elif abs(rv) <= DBLCORRECT and ee < -5:
+        s = "0.0(%d)x10^%d" % (ev, ee + 1)
+    else:
+        s = "% .*f(%d)" % (_p(nfrac), rv, ev)
+    return _fin(s, length)
+
+
+def nice_output_2(val, err, length=0):
+    """val(err), two error digits (src/output.c:114-210); None where the
+    reference exits."""
+    ee = 0 if abs(err) == 0.0 else math.floor(math.log10(abs(err)))
+    ev = _cint(math.floor(abs(err) * math.pow(10.0, -ee + 1) + DBLCORRECT + 0.5))
+    if ev == 100:
+        ev, ee = 10, ee + 1
+    rv = math.pow(10.0, ee - 1) * math.floor(val * math.pow(10.0, -ee + 1) + 0.5)
+    oexp = 0 if rv == 0.0 else math.floor(math.log10(abs(rv)))
+    vexp = 0 if val == 0.0 else math.floor(math.log10(abs(val)))
+    mant = rv * math.pow(10.0, -oexp)
+    hi, lo = ev // 10, ev % 10
+    if oexp < -4:
+        k = oexp - ee + 1
+        if k < 2:
+            m, x = (mant / 10, oexp + 1) if k == 0 else (mant, oexp)
+            s = "% .1f(%d.%d)x10^%d" % (m, hi, lo, x)
+        else:
+            s = "% .*f(%.2d)x10^%d" % (k, mant, ev, oexp)
+    elif ee - vexp > 1 and ee not in (0, 1):
+        s = "0.0(%d.%d)x10^%d" % (hi, lo, ee)
+    elif ee == 0:
+        s = "% .1f(%d.%d)" % (abs(rv) if abs(rv) < 0.1 else rv, hi, lo)
+    elif ee < 0:
+        if abs(rv) * math.pow(10.0, -ee + 1) < 0.1:
+            rv = abs(rv)
+        if abs(rv) <= DBLCORRECT and ee < -4:
+            s = "0.0(%d.%d)x10^%d" % (hi, lo, ee)
+        else:
+            s = "% .*f(%.2d)" % (-ee + 1, rv, ev)
+    elif ee == oexp:
+        s = "% d(%.2d)" % (_cint(rv), ev) if ee == 1 else "% .1f(%d.%d)x10^%d" % (mant, hi, lo, ee)
+    elif ee - oexp == 1:
+        m = abs(mant) if abs(mant) < 0.99999999999999 else mant
+        s = "% .1f(%d.%d)x10^%d" % (m / 10.0, hi, lo, ee)
+    elif ee > 1 and oexp > 1 and ee - oexp <= -1:
+        s = "% .*f(%.2d)x10^%d" % (oexp - ee + 1, mant, ev, oexp)
+    elif ee == 1 and oexp > 0:
+        s = "% d(%.2d)" % (_cint(rv), ev)
+    else:
+        return None
+    return _fin(s, length)
+
+
+def _centre(s, width):
+    if len(s) >= width:
+        return s[:width]
+    left = (width - len(s)) // 2
+    return " " * left + s + " " * (width - left - len(s))
+
+
+def _props(derivs, r, z, w):
+    out = FourierProps()
+    if _polish_lib().orc_calc_props(RDerivs(*[float(v) for v in derivs]), r, z, w,
+                                    C.byref(out)):
+        raise ValueError("calc_props: power or local power ~ 0")
+    return out
+
+
+def _rzwerrs(props, T):
+    L = _polish_lib()
+    L.orc_calc_rzwerrs.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    out = RzwErrs()
+    if L.orc_calc_rzwerrs(C.addressof(props), T, C.addressof(out)):
+        raise ValueError("calc_rzwerrs: T <= 0")
+    return out
+
+
+def _table_head(widths, t1, t2, skip):
+    cols = [k for k in range(len(widths)) if k not in skip]
+    lines = []
+    for cells in ([_centre(t1[k], widths[k]) for k in cols],
+                  [_centre(t2[k], widths[k]) for k in cols]):
+        lines.append("  ".join(cells) + "\n")
+    lines.append("--".join("-" * widths[k] for k in cols) + "\n")
+    return "".join(lines)
+
+
+def accelfile_text(T, nph, numw, cands, polished, inf_bytes=b""):
+    """The reference's text candidate file for sorted, polished candidates
+    ((power, sigma, numharm, r, z, w) and dicts of pows/hirs/hizs/hiws/derivs)
+    of an observation of T seconds; nph > 0 for -photon; numw > 0 for a jerk
+    search.  Returns bytes; notes are those of a telescope "None" run."""
+    def ve(val, err, digits, width):
+        s = nice_output_1(val, err) if digits == 1 else nice_output_2(val, err)
+        if s is None:
+            raise ValueError("nice_output_2: undefined condition")
+        return _centre(s, width)
+
+    sig = lib(64).orc_candidate_sigma
+    sig.restype = C.c_double
+    sig.argtypes = [C.c_double, C.c_int, C.c_double]
+    f32 = np.float32
+    props = []
+    for c, p in zip(cands, polished):
+        pr = _props(p["derivs"][0], c[3], c[4], c[5])
+        pr.rerr = float(f32(0.5) / f32(c[2]))
+        pr.zerr = float(f32(2.0) / f32(c[2]))
+        pr.werr = float(f32(20.0) / f32(c[2]))
+        props.append(pr)
+    n = len(cands)
+    notes = [" " * 20 for _ in range(n)]
+    for i in range(n):
+        for j in range(n):
+            if i == j:
+                continue
+            if (abs(props[i].r - props[j].r) < 15.0 and abs(props[i].z - props[j].z) > 1.0
+                    and props[i].pow > props[j].pow):
+                if notes[j] == " " * 20:
+                    notes[j] = ("SL? of Cand %d" % (i + 1))[:20]
+                continue
+            for k in range(1, 61):
+                if (abs(props[i].r - props[j].r / k) < float(f32(props[j].rerr) * f32(3))
+                        and abs(props[i].z - props[j].z / k) < float(f32(props[j].zerr) * f32(2))
+                        and notes[j] == " " * 20):
+                    notes[j] = ("H %d of Cand %d" % (k, i + 1))[:20]
+                    break
+    out = []
+    fw = [4, 5, 6, 8, 4, 16, 15, 15, 15, 11, 11, 15, 20]
+    out.append(_table_head(fw, ["", "", "Summed", "Coherent", "Num", "Period", "Frequency",
+                                "FFT 'r'", "Freq Deriv", "FFT 'z'", "FFT 'w'", "Accel", ""],
+                           ["Cand", "Sigma", "Power", "Power", "Harm", "(ms)", "(Hz)", "(bin)",
+                            "(Hz/s)", "(bins)", "(bins)", "(m/s^2)", "Notes"],
+                           () if numw else (10,)))
+    for i, (c, p) in enumerate(zip(cands, polished)):
+        er = _rzwerrs(props[i], T)
+        phs0 = float(p["derivs"][0][1])
+        cr = ci = 0.0
+        for h in range(c[2]):
+            d = [float(v) for v in p["derivs"][h]]
+            amp = math.sqrt(d[0] / nph) if nph > 0.0 else math.sqrt(d[0] / d[6])
+            corr = phs0 - math.fmod((h + 1.0) * phs0, 2.0 * math.pi)
+            cr += amp * math.cos(d[1] + corr)
+            ci += amp * math.sin(d[1] + corr)
+        cells = [_centre("%-4d" % (i + 1), 4), _centre("%.2f" % c[1], 5),
+                 _centre("%.2f" % c[0], 6), _centre("%.2f" % (cr * cr + ci * ci), 8),
+                 _centre("%d" % c[2], 4), ve(er.p * 1000.0, er.perr * 1000.0, 1, 16),
+                 ve(er.f, er.ferr, 1, 15), ve(props[i].r, props[i].rerr, 2, 15),
+                 ve(er.fd, er.fderr, 1, 15), ve(props[i].z, props[i].zerr, 2, 11)]
+        if numw:
+            cells.append(ve(props[i].w, props[i].werr, 2, 11))
+        cells.append(ve(props[i].z * SOL / (T * T * er.f), props[i].zerr * SOL / (T * T * er.f),
+                        2, 15))
+        out.append("  ".join(cells) + "    " + notes[i].split("\0")[0] + "\n")
+    out.append("\n\n")
+    hw = [5, 4, 5, 15, 11, 18, 13, 12, 9, 12, 9, 12, 10, 10, 20]
+    out.append(_table_head(hw, ["", "", "", "Power /", "Raw", "FFT 'r'", "Pred 'r'", "FFT 'z'",
+                                "Pred 'z'", "FFT 'w'", "Pred 'w'", "Phase", "Centroid", "Purity",
+                                ""],
+                           ["Cand", "Harm", "Sigma", "NumPhot" if nph > 0.0 else "Loc Pow",
+                            "Power", "(bin)", "(bin)", "(bins)", "(bins)", "(bins)", "(bins)",
+                            "(rad)", "(0-1)", "<p> = 1", "Notes"],
+                           () if numw else (9, 10)))
+    for i, (c, p) in enumerate(zip(cands, polished)):
+        for h in range(c[2]):
+            d = [float(v) for v in p["derivs"][h]]
+            if nph > 0.0:
+                d[6] = nph
+            hp = _props(d, float(p["hirs"][h]), float(p["hizs"][h]), float(p["hiws"][h]))
+            cells = [_centre(" %-4d" % (i + 1) if h == 0 else "     ", 5),
+                     _centre("%-4d" % (h + 1), 4), _centre("%.2f" % sig(hp.pow, 1, 1.0), 5),
+                     ve(hp.pow, hp.powerr, 2, 15), _centre("%.3g" % hp.rawpow, 11),
+                     ve(hp.r, hp.rerr, 2, 18), _centre("%.2f" % (c[3] * (h + 1)), 13),
+                     ve(hp.z, hp.zerr, 2, 12), _centre("%.2f" % (c[4] * (h + 1)), 9)]
+            if numw:
+                cells += [ve(hp.w, hp.werr, 2, 12), _centre("%.2f" % (c[5] * (h + 1)), 9)]
+            cells += [ve(hp.phs, hp.phserr, 2, 12), ve(hp.cen, hp.cenerr, 2, 10),
+                      ve(hp.pur, hp.purerr, 2, 10)]
+            out.append("  ".join(cells) + "    " + " " * 20 + "\n")
+    out.append("\n\n")
+    return "".join(out).encode() + inf_bytes

@@ -36,6 +36,7 @@ EXPORTS = [
     "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
     "ab_get_fourier_amplitudes", "ab_optimize_cands", "ab_realfft", "ab_deredden",
     "ab_series_to_fft", "ab_calc_props", "ab_calc_rzwerrs", "ab_cand_props",
+    "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2",
 ]
 
 COST_SLOTS = 16
@@ -162,6 +163,10 @@ def lib():
     L.ab_calc_props.argtypes = [C.POINTER(RDerivs), d, d, d, C.POINTER(FourierProps)]
     L.ab_calc_rzwerrs.argtypes = [C.POINTER(FourierProps), d, C.POINTER(RzwErrs)]
     L.ab_cand_props.argtypes = [C.POINTER(Cand), C.POINTER(Polished), ll, C.POINTER(FourierProps)]
+    L.ab_write_accelfile.argtypes = [C.c_char_p, C.POINTER(Obs), C.POINTER(Cand),
+                                     C.POINTER(Polished), ll, C.c_char_p]
+    L.ab_nice_output_1.argtypes = [C.c_char_p, C.c_size_t, d, d, i]
+    L.ab_nice_output_2.argtypes = L.ab_nice_output_1.argtypes
     L.ab_realfft.argtypes = [vp, vp, ll, i, vp, i]
     L.ab_deredden.argtypes = [vp, vp, ll, i, i, d, d, i]
     L.ab_series_to_fft.argtypes = [vp, vp, ll, d, i, vp, i]
@@ -311,18 +316,37 @@ def calc_rzwerrs(props, T):
     return out
 
 
+def _cand_arrays(cands, polished):
+    """ctypes arrays of (power, sigma, numharm, r, z, w) candidates and their
+    polishing dicts (Context.optimize_cands)."""
+    n = len(cands)
+    if len(polished) != n:
+        raise AccelError(f"{n} candidates but {len(polished)} polished records")
+    arr = (Cand * max(n, 1))(*[Cand(c[0], c[1], c[2], c[3], c[4], c[5]) for c in cands])
+    pol = (Polished * max(n, 1))()
+    for k, p in enumerate(polished):
+        h = len(p["pows"])
+        if h > POLISH_MAX_HARM:
+            raise AccelError(f"{h} harmonics: at most {POLISH_MAX_HARM}")
+        pol[k].numharm = h
+        zeros = np.zeros(h)
+        pows, hirs, hizs, hiws = (p.get(key, zeros) for key in ("pows", "hirs", "hizs", "hiws"))
+        for j in range(h):
+            pol[k].pows[j] = float(pows[j])
+            pol[k].hirs[j] = float(hirs[j])
+            pol[k].hizs[j] = float(hizs[j])
+            pol[k].hiws[j] = float(hiws[j])
+            pol[k].derivs[j] = RDerivs(*[float(v) for v in p["derivs"][j]])
+    return arr, pol
+
+
 def cand_props(cands, polished):
     """The .cand file's records (src/accelsearch.c:261-272): per candidate
     (power, sigma, numharm, r, z, w) and its polishing (a dict from
     Context.optimize_cands), the fundamental's fourierprops at the search's
     r, z, w with the errors set to ACCEL_DR, ACCEL_DZ, ACCEL_DW / numharm."""
     n = len(cands)
-    arr = (Cand * max(n, 1))(*[Cand(c[0], c[1], c[2], c[3], c[4], c[5]) for c in cands])
-    pol = (Polished * max(n, 1))()
-    for k, p in enumerate(polished):
-        pol[k].numharm = len(p["pows"])
-        for h in range(len(p["pows"])):
-            pol[k].derivs[h] = RDerivs(*[float(v) for v in p["derivs"][h]])
+    arr, pol = _cand_arrays(cands, polished)
     out = (FourierProps * max(n, 1))()
     rc = lib().ab_cand_props(arr, pol, n, out)
     if rc:
@@ -336,6 +360,39 @@ def write_candfile(path, props):
     arr = (FourierProps * len(props))(*props)
     with open(path, "wb") as f:
         f.write(bytes(arr))
+
+
+def accel_filenames(rootname, obs):
+    """The output names of src/accel_utils.c:1667-1682 (text, .cand and
+    .txtcand) from the search's -zmax and -wmax as create_accelobs rounds them
+    up (to multiples of 2 and 20); _JERK_ only when the search has w planes."""
+    base = f"{rootname}_ACCEL_{int(round(obs.zhi))}"
+    if obs.numw:
+        base += f"_JERK_{int(round(obs.whi))}"
+    return dict(accel=base, cand=base + ".cand", txtcand=base + ".txtcand")
+
+
+def write_accelfile(path, obs, cands, polished, inf_path=None):
+    """The text candidate file (output_fundamentals + output_harmonics,
+    src/accel_utils.c:666-966) of sorted, polished candidates, with the .inf
+    at inf_path appended."""
+    n = len(cands)
+    arr, pol = _cand_arrays(cands, polished)
+    rc = lib().ab_write_accelfile(os.fsencode(path), C.byref(obs), arr, pol, n,
+                                  os.fsencode(inf_path) if inf_path else None)
+    if rc:
+        raise AccelError(f"ab_write_accelfile: {ERRORS.get(rc, rc)}")
+
+
+def nice_output(val, err, digits=1, length=0):
+    """nice_output_1 / nice_output_2 (src/output.c:6-210): val(err) with a
+    one- or two-digit error."""
+    buf = C.create_string_buffer(512)
+    f = lib().ab_nice_output_1 if digits == 1 else lib().ab_nice_output_2
+    rc = f(buf, 512, float(val), float(err), int(length))
+    if rc < 0:
+        raise AccelError(f"nice_output_{digits}({val!r}, {err!r}): no format")
+    return buf.value.decode()
 
 
 def read_candfile(path):
@@ -673,12 +730,16 @@ class AccelSearch:
         obs = self.obs(N, dt, fft.size)
         return self.ctx.search(obs, fft)
 
-    def run(self, fft, N, dt, harmremove=True, candfile=None):
+    def run(self, fft, N, dt, harmremove=True, candfile=None, rootname=None):
         """The whole of src/accelsearch.c:155-284 for one spectrum: the search,
         sort_accelcands, eliminate_harmonics (numharm > 1 unless harmremove
         is False, as -noharmremove), optimize_accelcand of every candidate on
         the device, and the fundamentals' .cand records (written to candfile
-        when given).  Returns dict(cands, polished, props)."""
+        when given).  With rootname, the reference's output files too:
+        <rootname>_ACCEL_<zmax>[_JERK_<wmax>] (text, with <rootname>.inf
+        appended when it exists), its .cand and an empty .txtcand work file
+        (src/accel_utils.c:1667-1685); with no candidates only the .txtcand,
+        as the reference.  Returns dict(cands, polished, props, obs)."""
         fft = np.ascontiguousarray(fft, dtype=np.complex64)
         obs = self.obs(N, dt, fft.size)
         cands = self.ctx.search(obs, fft)
@@ -691,4 +752,12 @@ class AccelSearch:
             props = cand_props(cands, polished)
             if candfile:
                 write_candfile(candfile, props)
-        return dict(cands=cands, polished=polished, props=props)
+        if rootname:
+            names = accel_filenames(rootname, obs)
+            open(names["txtcand"], "w").close()
+            if cands:
+                inf = rootname + ".inf"
+                write_accelfile(names["accel"], obs, cands, polished,
+                                inf if os.path.exists(inf) else None)
+                write_candfile(names["cand"], props)
+        return dict(cands=cands, polished=polished, props=props, obs=obs)

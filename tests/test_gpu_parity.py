@@ -328,6 +328,33 @@ def test_accelsearch_run_writes_cand_file(ctx, ablib, tmp_path):
     assert [(p.r, p.z, p.sig) for p in back] == [(p.r, p.z, p.sig) for p in props]
 
 
+def test_accelsearch_run_writes_reference_files(ctx, ablib, oracle, tmp_path):
+    """AccelSearch.run(rootname=...): <root>_ACCEL_<zmax> (text, the .inf
+    appended), its .cand and the empty .txtcand work file
+    (src/accel_utils.c:1667-1685); the text file is the oracle's restatement
+    of output_fundamentals + output_harmonics of the same candidates,
+    byte for byte."""
+    N = 1 << 19
+    fft = synth.cfg1_spectrum(N=N, amp=0.05)
+    root = str(tmp_path / "cfg1_DM0.00")
+    inf = (b" Number of bins in the time series      =  524288     \n"
+           b" Width of each time series bin (sec)    =  6.4e-05\n")
+    with open(root + ".inf", "wb") as f:
+        f.write(inf)
+    res = ablib.AccelSearch(zmax=200, numharm=8, sigma=2.0, ctx=ctx).run(fft, N, DT,
+                                                                          rootname=root)
+    obs = res["obs"]
+    assert res["cands"]
+    names = ablib.accel_filenames(root, obs)
+    assert names["accel"].endswith("cfg1_DM0.00_ACCEL_200")
+    assert os.path.getsize(names["txtcand"]) == 0
+    assert os.path.getsize(names["cand"]) == 88 * len(res["cands"])
+    got = open(names["accel"], "rb").read()
+    want = oracle.accelfile_text(obs.T, float(obs.nph), obs.numw, res["cands"], res["polished"],
+                                 inf)
+    assert got == want
+
+
 def test_wrapping_bank_matches_oracle(ctx, ablib, oracle):
     """zmax=100, wmax=200, numharm=16: the reference's 192-point FFT for the
     1/16 harmonic is one sample shorter than the span its valid cells read, so
