@@ -28,3 +28,23 @@ $CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" -I "$REF
 $CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/output.map" -o "$OUT/libref_output.so" \
     "$OUT/output.o" -lm
 echo "built $OUT/libref_output.so from $REF/src/output.c"
+# The polishing interpolators and candidate properties: src/characteristics.c
+# (calc_props, calc_rzwerrs, get_localpower3d, get_derivs3d), src/rzinterp.c,
+# src/rzwinterp.c, src/responses.c, src/fresnl.c and src/vectors.c, unmodified,
+# linked with refshim/refshim.c (malloc-backed fftwf_malloc/free and an FP64
+# forward realfft standing in for FFTW).
+cat > "$OUT/polish.map" <<'MAP'
+REF { global: calc_props; calc_rzwerrs; get_localpower3d; get_derivs3d; rz_interp;
+      rzw_interp; gen_r_response; gen_z_response; gen_w_response; r_resp_halfwidth;
+      z_resp_halfwidth; w_resp_halfwidth; vect_free; local: *; };
+MAP
+POBJ=""
+for f in characteristics rzinterp rzwinterp responses fresnl vectors; do
+    $CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" -I "$REF/include" \
+        -c "$REF/src/$f.c" -o "$OUT/p_$f.o"
+    POBJ="$POBJ $OUT/p_$f.o"
+done
+$CC -O2 -g -fPIC -c "$HERE/refshim/refshim.c" -o "$OUT/p_refshim.o"
+$CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/polish.map" -Wl,-z,defs \
+    -o "$OUT/libref_polish.so" $POBJ "$OUT/p_refshim.o" -lm
+echo "built $OUT/libref_polish.so from $REF/src/{characteristics,rzinterp,rzwinterp,responses,fresnl,vectors}.c"

@@ -393,6 +393,48 @@ def optimize_cands(fft, lobin, cands, nthreads=1):
                  derivs=der[k, :nh[k]]) for k in range(n)]
 
 
+def ref_polish_lib():
+    """The reference's src/characteristics.c, rzinterp.c, rzwinterp.c,
+    responses.c, fresnl.c and vectors.c built by build_ref.sh (FFTW replaced by
+    oracle/refshim/refshim.c), or None.  Its functions exit() on arguments the
+    reference rejects: call them with valid ones only."""
+    path = os.path.join(HERE, "_ref", "libref_polish.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    d, i, vp = C.c_double, C.c_int, C.c_void_p
+    L.gen_r_response.restype = vp
+    L.gen_r_response.argtypes = [d, i, i]
+    L.gen_z_response.restype = vp
+    L.gen_z_response.argtypes = [d, i, d, i]
+    L.gen_w_response.restype = vp
+    L.gen_w_response.argtypes = [d, i, d, d, i]
+    L.vect_free.argtypes = [vp]
+    L.z_resp_halfwidth.argtypes = [d, i]
+    L.w_resp_halfwidth.argtypes = [d, d, i]
+    L.rz_interp.argtypes = [vp, C.c_long, d, d, i, vp]
+    L.rzw_interp.argtypes = [vp, C.c_long, d, d, d, i, vp]
+    L.get_localpower3d.restype = d
+    L.get_localpower3d.argtypes = [vp, C.c_long, d, d, d]
+    L.get_derivs3d.argtypes = [vp, C.c_long, d, d, d, d, C.POINTER(RDerivs)]
+    L.calc_props.argtypes = [RDerivs, d, d, d, C.POINTER(FourierProps)]
+    L.calc_rzwerrs.argtypes = [C.c_void_p, d, C.c_void_p]
+    return L
+
+
+def ref_response(L, kind, numbetween, numkern, z=0.0, w=0.0, roffset=0.0):
+    """gen_r/z/w_response of the reference build, copied out and freed."""
+    if kind == "r":
+        p = L.gen_r_response(roffset, numbetween, numkern)
+    elif kind == "z":
+        p = L.gen_z_response(roffset, numbetween, z, numkern)
+    else:
+        p = L.gen_w_response(roffset, numbetween, z, w, numkern)
+    out = np.ctypeslib.as_array((C.c_float * (2 * numkern)).from_address(p)).copy()
+    L.vect_free(p)
+    return out.view(np.complex64)
+
+
 # ---- time-series input path (series_oracle.c) ------------------------------
 def _series_lib():
     L = lib(64)

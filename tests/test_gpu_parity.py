@@ -77,6 +77,23 @@ def test_responses_match_oracle(ctx, oracle, z, w):
     assert np.max(np.abs(dev - orc)) <= 2e-6 * np.max(np.abs(orc))
 
 
+@pytest.mark.parametrize("kind,nb,z,w", [("r", 2, 0.0, 0.0), ("z", 2, 3.0, 0.0),
+                                         ("z", 2, -600.0, 0.0), ("z", 16, 5.0, 0.0),
+                                         ("w", 2, 0.0, 40.0), ("w", 16, 5.0, 40.0),
+                                         ("w", 2, -60.0, 200.0), ("w", 2, 100.0, -300.0)])
+def test_responses_match_reference_build(ctx, oracle, kind, nb, z, w):
+    """The device's responses against the reference's own gen_*_response
+    (src/responses.c, built unmodified into oracle/_ref when the reference
+    tree was present; FFTW stood in for by an FP64 realfft)."""
+    ref = oracle.ref_polish_lib()
+    if ref is None:
+        pytest.skip("no reference build in oracle/_ref")
+    numkern = 2 * nb * (32 if kind == "r" else ref.w_resp_halfwidth(z, w, 0))
+    want = oracle.ref_response(ref, kind, nb, numkern, z=z, w=w)
+    dev = ctx.gen_response(kind, nb, numkern, z=z, w=w)
+    assert np.max(np.abs(dev - want)) <= 2e-6 * np.max(np.abs(want))
+
+
 def test_fundamental_templates_match_oracle(ctx, oracle, ablib, case):
     """Device templates against the oracle's: at the reference's fftlen when
     the device uses it, else the oracle's response placed (centre at index 0,
