@@ -219,6 +219,22 @@ int ab_candlist_insert(ab_candlist *l, float power, float sigma, int numharm,
 int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd,
                         int numharm, ab_candlist *list);
 
+/* The .txtcand work file: search_ffdotpows writes one line per candidate an
+ * insertion adds, "%-7.2f  %-7.4f  %-2d  %-14.4f  %-14.9f  %-10.4f %-10.4f"
+ * of power, sigma, numharm, r, r / T, z, w (src/accel_utils.c:1443-1447),
+ * in search order, for .fft input.
+ *   ab_set_worklog      on != 0: later ab_search calls record those lines;
+ *   ab_last_worklog     the last ab_search's lines: *len bytes; up to
+ *                       cap - 1 of them copied to out, NUL-terminated;
+ *   ab_candlist_set_worklog / ab_candlist_worklog  the same for a list that
+ *                       ab_search_ffdotpows / ab_candlist_insert fill (T the
+ *                       observation's length, s); the second returns the
+ *                       length and copies as ab_last_worklog does. */
+int ab_set_worklog(ab_ctx *ctx, int on);
+int ab_last_worklog(ab_ctx *ctx, char *out, size_t cap, size_t *len);
+int ab_candlist_set_worklog(ab_candlist *l, int on, double T);
+long long ab_candlist_worklog(const ab_candlist *l, char *out, size_t cap);
+
 /* Stage sums of one block of the last ab_search configuration, for parity
  * checks: out[stage][numws][numzs][numrs] after each stage. */
 int ab_block_stage_sums(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft_host,

@@ -28,23 +28,50 @@ $CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" -I "$REF
 $CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/output.map" -o "$OUT/libref_output.so" \
     "$OUT/output.o" -lm
 echo "built $OUT/libref_output.so from $REF/src/output.c"
-# The polishing interpolators and candidate properties: src/characteristics.c
-# (calc_props, calc_rzwerrs, get_localpower3d, get_derivs3d), src/rzinterp.c,
-# src/rzwinterp.c, src/responses.c, src/fresnl.c and src/vectors.c, unmodified,
-# linked with refshim/refshim.c (malloc-backed fftwf_malloc/free and an FP64
-# forward realfft standing in for FFTW).
+# The accelsearch program itself: src/accelsearch.c, its command-line parser
+# and the libpresto files it links (src/meson.build:56-58, -DUSEMMAP, with
+# the project-wide -DUSE_FFTW_MALLOC), unmodified, linked against stand-ins of
+# our own for the third-party libraries that are not in this image
+# (refshim/refshim_fftw.c: FFTW's plans over an FP64 mixed-radix transform;
+# refshim_glib.c: GSList; refshim_gsl.c: CDFs from oracle/accel_oracle.c,
+# median, vectors, nmsimplex2, no random numbers; refshim_erfa.c: angle
+# conversions).  oracle/_ref/accelsearch runs like the installed program
+# (telescope "None (Artificial Data Set)" .inf files; no -zaplist).
+# libref_polish.so exports the polishing primitives, responses and candidate
+# properties from the same objects.
+OBJ="$OUT/obj"
+mkdir -p "$OBJ"
+PRESTO_SRC="accelsearch accelsearch_cmd accel_utils zapping characteristics responses fresnl
+    vectors corr_prep corr_routines correlations fftcalls fastffts median misc_utils ioinf
+    chkio maximize_rz maximize_rzw rzinterp rzwinterp output birdzap datadir database read_fft
+    transpose sorter"
+AOBJ=""
+for f in $PRESTO_SRC; do
+    $CC -O2 -g -fPIC -fopenmp -ffunction-sections -fdata-sections -DUSEMMAP -DUSE_FFTW_MALLOC \
+        -DPRESTO_DATADIR='"/nonexistent"' -w -I "$HERE/refshim" -I "$REF/include" \
+        -c "$REF/src/$f.c" -o "$OBJ/$f.o"
+    AOBJ="$AOBJ $OBJ/$f.o"
+done
+SOBJ=""
+for f in refshim_fftw refshim_glib refshim_gsl refshim_erfa; do
+    $CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" \
+        -c "$HERE/refshim/$f.c" -o "$OBJ/$f.o"
+    SOBJ="$SOBJ $OBJ/$f.o"
+done
+$CC -O2 -g -fPIC -ffunction-sections -fdata-sections -DORC_REAL=double \
+    -c "$HERE/accel_oracle.c" -o "$OBJ/orc_stats.o"
+$CC -fopenmp -Wl,--gc-sections -o "$OUT/accelsearch" $AOBJ $SOBJ "$OBJ/orc_stats.o" -lm
+echo "built $OUT/accelsearch from $REF/src/accelsearch.c and the libpresto sources it links"
 cat > "$OUT/polish.map" <<'MAP'
 REF { global: calc_props; calc_rzwerrs; get_localpower3d; get_derivs3d; rz_interp;
       rzw_interp; gen_r_response; gen_z_response; gen_w_response; r_resp_halfwidth;
       z_resp_halfwidth; w_resp_halfwidth; vect_free; local: *; };
 MAP
 POBJ=""
-for f in characteristics rzinterp rzwinterp responses fresnl vectors; do
-    $CC -O2 -g -fPIC -ffunction-sections -fdata-sections -I "$HERE/refshim" -I "$REF/include" \
-        -c "$REF/src/$f.c" -o "$OUT/p_$f.o"
-    POBJ="$POBJ $OUT/p_$f.o"
+for f in characteristics rzinterp rzwinterp responses fresnl vectors fastffts fftcalls misc_utils \
+         datadir chkio transpose; do
+    POBJ="$POBJ $OBJ/$f.o"
 done
-$CC -O2 -g -fPIC -c "$HERE/refshim/refshim.c" -o "$OUT/p_refshim.o"
-$CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/polish.map" -Wl,-z,defs \
-    -o "$OUT/libref_polish.so" $POBJ "$OUT/p_refshim.o" -lm
-echo "built $OUT/libref_polish.so from $REF/src/{characteristics,rzinterp,rzwinterp,responses,fresnl,vectors}.c"
+$CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/polish.map" -Wl,-z,defs \
+    -o "$OUT/libref_polish.so" $POBJ $SOBJ "$OBJ/orc_stats.o" -lm
+echo "built $OUT/libref_polish.so from the same objects"

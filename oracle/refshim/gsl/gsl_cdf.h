@@ -1,7 +1,5 @@
-/* Declaration-only stand-in for GSL's gsl_cdf.h: src/characteristics.c
- * includes it, and the functions oracle/build_ref.sh exports from that file
- * (calc_props, calc_rzwerrs, get_localpower3d, get_derivs3d) call none of
- * these.  Test infrastructure only. */
+/* Stand-in for GSL's gsl_cdf.h (src/characteristics.c), implemented by
+ * oracle/refshim/refshim_gsl.c.  Test infrastructure only. */
 #ifndef REFSHIM_GSL_CDF_H
 #define REFSHIM_GSL_CDF_H
 double gsl_cdf_chisq_Q(double x, double nu);

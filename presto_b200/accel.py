@@ -36,7 +36,8 @@ EXPORTS = [
     "ab_fund_to_ffdotplane_trans", "ab_inmem_add_ffdotpows_trans", "ab_copy_ffdotpows",
     "ab_get_fourier_amplitudes", "ab_optimize_cands", "ab_realfft", "ab_deredden",
     "ab_series_to_fft", "ab_calc_props", "ab_calc_rzwerrs", "ab_cand_props",
-    "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2",
+    "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
+    "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog",
 ]
 
 COST_SLOTS = 16
@@ -163,6 +164,11 @@ def lib():
     L.ab_calc_props.argtypes = [C.POINTER(RDerivs), d, d, d, C.POINTER(FourierProps)]
     L.ab_calc_rzwerrs.argtypes = [C.POINTER(FourierProps), d, C.POINTER(RzwErrs)]
     L.ab_cand_props.argtypes = [C.POINTER(Cand), C.POINTER(Polished), ll, C.POINTER(FourierProps)]
+    L.ab_set_worklog.argtypes = [vp, i]
+    L.ab_last_worklog.argtypes = [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.ab_candlist_set_worklog.argtypes = [vp, i, d]
+    L.ab_candlist_worklog.restype = ll
+    L.ab_candlist_worklog.argtypes = [vp, C.c_char_p, C.c_size_t]
     L.ab_write_accelfile.argtypes = [C.c_char_p, C.POINTER(Obs), C.POINTER(Cand),
                                      C.POINTER(Polished), ll, C.c_char_p]
     L.ab_nice_output_1.argtypes = [C.c_char_p, C.c_size_t, d, d, i]
@@ -493,6 +499,20 @@ class Context:
         self._check(self.L.ab_last_cands(self.ptr, cands, n.value, C.byref(n)), "ab_last_cands")
         return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in cands[:n.value]]
 
+    def set_worklog(self, on=True):
+        """Record the .txtcand work-file lines of later searches
+        (search_ffdotpows, src/accel_utils.c:1443-1447)."""
+        self._check(self.L.ab_set_worklog(self.ptr, int(bool(on))), "ab_set_worklog")
+
+    def last_worklog(self):
+        """The .txtcand text of the last search (set_worklog on)."""
+        n = C.c_size_t()
+        self._check(self.L.ab_last_worklog(self.ptr, None, 0, C.byref(n)), "ab_last_worklog")
+        buf = C.create_string_buffer(n.value + 1)
+        self._check(self.L.ab_last_worklog(self.ptr, buf, n.value + 1, C.byref(n)),
+                    "ab_last_worklog")
+        return buf.raw[:n.value].decode()
+
     def last_hits(self):
         n = C.c_longlong()
         self.L.ab_last_hits(self.ptr, None, None, None, None, None, None, 0, C.byref(n))
@@ -682,6 +702,18 @@ class CandList:
         self.L.ab_candlist_get(self.ptr, arr, n)
         return [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in arr[:n]]
 
+    def set_worklog(self, on, T):
+        """Record the .txtcand line of every candidate an insertion adds (T the
+        observation's length, s)."""
+        if self.L.ab_candlist_set_worklog(self.ptr, int(bool(on)), float(T)):
+            raise AccelError("ab_candlist_set_worklog: T must be > 0")
+
+    def worklog(self):
+        n = self.L.ab_candlist_worklog(self.ptr, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        self.L.ab_candlist_worklog(self.ptr, buf, n + 1)
+        return buf.raw[:n].decode()
+
     def __del__(self):
         try:
             self.L.ab_candlist_free(self.ptr)
@@ -737,12 +769,20 @@ class AccelSearch:
         the device, and the fundamentals' .cand records (written to candfile
         when given).  With rootname, the reference's output files too:
         <rootname>_ACCEL_<zmax>[_JERK_<wmax>] (text, with <rootname>.inf
-        appended when it exists), its .cand and an empty .txtcand work file
-        (src/accel_utils.c:1667-1685); with no candidates only the .txtcand,
-        as the reference.  Returns dict(cands, polished, props, obs)."""
+        appended when it exists), its .cand and the .txtcand work file, one
+        line per candidate insertion during the search (src/accel_utils.c:
+        1443-1447, 1667-1685); with no candidates only the .txtcand, as the
+        reference.  Returns dict(cands, polished, props, obs)."""
         fft = np.ascontiguousarray(fft, dtype=np.complex64)
         obs = self.obs(N, dt, fft.size)
-        cands = self.ctx.search(obs, fft)
+        if rootname:
+            self.ctx.set_worklog(True)
+        try:
+            cands = self.ctx.search(obs, fft)
+            worklog = self.ctx.last_worklog() if rootname else ""
+        finally:
+            if rootname:
+                self.ctx.set_worklog(False)
         polished, props = [], []
         if cands:
             cands = sort_cands(cands)
@@ -754,7 +794,8 @@ class AccelSearch:
                 write_candfile(candfile, props)
         if rootname:
             names = accel_filenames(rootname, obs)
-            open(names["txtcand"], "w").close()
+            with open(names["txtcand"], "w") as f:
+                f.write(worklog)
             if cands:
                 inf = rootname + ".inf"
                 write_accelfile(names["accel"], obs, cands, polished,

@@ -131,6 +131,8 @@ struct ab_ctx {
     std::vector<float> hpows;
     std::vector<double> hstart;
     std::vector<ab_cand> last_cands;
+    int worklog_on = 0;                 // record the .txtcand lines of each ab_search
+    std::string last_worklog;
     unsigned overflow_need = 0;              // hits one batch wanted beyond hit_cap
     bool hits_truncated = false;             // host copy holds only the latest batches
 
@@ -1414,6 +1416,8 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
     ab_list *l = nullptr;
     for (int attempt = 0;; attempt++) {
         l = ab_list_new();
+        if (!l) return fail(ctx, AB_ERR_NOMEM, "candidate list");
+        if (ctx->worklog_on) ab_list_worklog(l, 1, obs->T);
         ctx->overflow_need = 0;
         rc = search_core(ctx, obs, dfft, first_block, max_blocks, -1, l, &replay_ms);
         if (!rc) rc = check_device_error(ctx);
@@ -1443,6 +1447,11 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
     long long n = ab_list_get(l, nullptr, 0);
     ctx->last_cands.resize((size_t) n);
     ab_list_get(l, ctx->last_cands.data(), n);
+    {
+        size_t wlen = 0;
+        const char *wtext = ab_list_worklog_text(l, &wlen);
+        ctx->last_worklog.assign(wtext, wlen);
+    }
     ab_list_free(l);
     if (cands)
         for (long long i = 0; i < n && i < maxcands; i++) cands[i] = ctx->last_cands[i];
@@ -1729,9 +1738,49 @@ int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd,
         double rr = (ffd->rlo + ri * (double) AB_DR) / (double) numharm;
         double zz = (ffd->zlo + zi * (double) AB_DZ) / (double) numharm;
         double ww = (ffd->wlo + wi * (double) AB_DW) / (double) numharm;
-        ab_list_insert(list, pw, sig, numharm, rr, zz, ww);
+        if (ab_list_insert(list, pw, sig, numharm, rr, zz, ww) < 0)
+            return fail(ctx, AB_ERR_NOMEM, "candidate list");
     }
     return AB_OK;
+}
+
+int ab_set_worklog(ab_ctx *ctx, int on)
+{
+    if (!ctx) return AB_ERR_ARG;
+    ctx->worklog_on = on ? 1 : 0;
+    return AB_OK;
+}
+
+int ab_last_worklog(ab_ctx *ctx, char *out, size_t cap, size_t *len)
+{
+    if (!ctx || !len) return AB_ERR_ARG;
+    *len = ctx->last_worklog.size();
+    if (out && cap) {
+        const size_t k = std::min(cap - 1, ctx->last_worklog.size());
+        memcpy(out, ctx->last_worklog.data(), k);
+        out[k] = '\0';
+    }
+    return AB_OK;
+}
+
+int ab_candlist_set_worklog(ab_candlist *l, int on, double T)
+{
+    if (!l || (on && !(T > 0.0))) return AB_ERR_ARG;
+    ab_list_worklog(l, on, T);
+    return AB_OK;
+}
+
+long long ab_candlist_worklog(const ab_candlist *l, char *out, size_t cap)
+{
+    if (!l) return AB_ERR_ARG;
+    size_t len = 0;
+    const char *t = ab_list_worklog_text(l, &len);
+    if (out && cap) {
+        const size_t k = len < cap - 1 ? len : cap - 1;
+        memcpy(out, t, k);
+        out[k] = '\0';
+    }
+    return (long long) len;
 }
 
 int ab_gen_response(ab_ctx *ctx, double roffset, int numbetween, double z, double w, int numkern,

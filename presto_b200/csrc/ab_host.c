@@ -516,6 +516,12 @@ struct ab_list {
     double *seg;                        /* max-of-r segment tree (unordered walks) */
     long long segsz;
     int seg_dirty;
+    /* the work-file lines of search_ffdotpows (src/accel_utils.c:1443-1447),
+       one per candidate that an insertion adds, when wlog_on */
+    int wlog_on;
+    double wlog_T;
+    char *wlog;
+    size_t wlen, wcap;
 };
 
 ab_list *ab_list_new(void)
@@ -530,7 +536,40 @@ void ab_list_free(ab_list *l)
     if (!l) return;
     free(l->c);
     free(l->seg);
+    free(l->wlog);
     free(l);
+}
+
+void ab_list_worklog(ab_list *l, int on, double T)
+{
+    l->wlog_on = on;
+    l->wlog_T = T;
+}
+
+const char *ab_list_worklog_text(const ab_list *l, size_t *len)
+{
+    *len = l->wlen;
+    return l->wlog ? l->wlog : "";
+}
+
+static int wlog_line(ab_list *l, float power, float sigma, int numharm, double rr, double zz,
+                     double ww)
+{
+    char b[160];
+    const int k = snprintf(b, sizeof b, "%-7.2f  %-7.4f  %-2d  %-14.4f  %-14.9f  %-10.4f %-10.4f\n",
+                           power, sigma, numharm, rr, rr / l->wlog_T, zz, ww);
+    if (k < 0) return -1;
+    if (l->wlen + (size_t) k + 1 > l->wcap) {
+        size_t cap = l->wcap ? l->wcap : 4096;
+        while (cap < l->wlen + (size_t) k + 1) cap *= 2;
+        char *p = (char *) realloc(l->wlog, cap);
+        if (!p) return -1;
+        l->wlog = p;
+        l->wcap = cap;
+    }
+    memcpy(l->wlog + l->wlen, b, (size_t) k + 1);
+    l->wlen += (size_t) k;
+    return 0;
 }
 
 /* Segment tree over the array positions holding max(r); answers "first
@@ -666,6 +705,7 @@ int ab_list_insert(ab_list *l, float power, float sigma, int numharm,
     if (l->n == 0) {
         set_cand(&l->c[0], power, sigma, numharm, rr, zz, ww);
         l->n = 1;
+        if (l->wlog_on && wlog_line(l, power, sigma, numharm, rr, zz, ww)) return -1;
         return 1;
     }
     long long t = find_stop(l, rr);
@@ -697,6 +737,7 @@ int ab_list_insert(ab_list *l, float power, float sigma, int numharm,
         long long at = (t == l->n - 1 && c[t].r < rr - AB_CLOSEST_R) ? l->n : t;
         insert_at(l, at, power, sigma, numharm, rr, zz, ww);
     }
+    if (added && l->wlog_on && wlog_line(l, power, sigma, numharm, rr, zz, ww)) return -1;
     return added;
 }
 

@@ -81,6 +81,10 @@ void      ab_list_free(ab_list *l);
 int       ab_list_insert(ab_list *l, float power, float sigma, int numharm,
                          double rr, double zz, double ww);
 long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout);
+/* work-file log: on != 0 records the reference's .txtcand line (T = the
+ * observation's length, s) for every candidate an insertion adds */
+void      ab_list_worklog(ab_list *l, int on, double T);
+const char *ab_list_worklog_text(const ab_list *l, size_t *len);
 int       ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows,
                          float *sigs, long long nhits, const double *startr_tab,
                          long long ntab, ab_list *l);

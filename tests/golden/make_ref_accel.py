@@ -1,0 +1,96 @@
+"""Runs the reference's own accelsearch program on seeded synthetic spectra and
+keeps its output files as fixtures under tests/golden/ref_accel/<case>/.
+
+The program is src/accelsearch.c with the libpresto files it links, compiled
+unmodified into oracle/_ref/accelsearch by oracle/build_ref.sh; FFTW, GSL,
+glib and ERFA, which this image lacks, are replaced by stand-ins written for
+this repository (oracle/refshim/).  Run here, where the reference tree is;
+the fixtures travel with the repository.
+
+Per case: the .fft input is presto_b200.synth's seeded spectrum (its SHA-256
+is recorded so that a test can confirm it regenerated the same input), the
+.inf is a telescope "None (Artificial Data Set)" observation, and the
+program's three outputs are kept: <root>_ACCEL_<zmax>[_JERK_<wmax>] (text),
+.cand (fourierprops records) and .txtcand (one line per candidate insertion
+during the search), with its command line in manifest.json.
+"""
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+OUT = os.path.join(HERE, "ref_accel")
+PROG = os.path.join(ROOT, "oracle", "_ref", "accelsearch")
+DT = 64e-6
+
+# name: (N, seed, pulsars, accelsearch options)
+CASES = {
+    "std": (1 << 17, 11, [dict(r=1500.3, z=12.0, harms=[(0.08, 0.3), (0.05, 1.0), (0.03, 2.0)])],
+            ["-zmax", "60", "-wmax", "0", "-numharm", "4"]),
+    "inmem": (1 << 17, 12, [dict(r=2222.7, z=-20.0, harms=[(0.06, 0.1)] * 6)],
+              ["-zmax", "60", "-numharm", "8"]),
+    "jerk": (1 << 16, 13, [dict(r=900.2, z=6.0, w=25.0, harms=[(0.12, 0.0), (0.06, 0.5)])],
+             ["-zmax", "20", "-wmax", "40", "-numharm", "2"]),
+    "std_locpow": (1 << 17, 14,
+                   [dict(r=1700.6, z=-9.0, harms=[(0.08, 0.2), (0.05, 0.9)])],
+                   ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-locpow"]),
+    "noharmpolish": (1 << 17, 11,
+                     [dict(r=1500.3, z=12.0, harms=[(0.08, 0.3), (0.05, 1.0), (0.03, 2.0)])],
+                     ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-noharmpolish"]),
+}
+
+
+def inf_text(name, N, dt):
+    return (f" Data file name without suffix          =  {name}\n"
+            f" Telescope used                         =  None (Artificial Data Set)\n"
+            f" Number of bins in the time series      =  {N:<11.0f}\n"
+            f" Width of each time series bin (sec)    =  {dt:.15g}\n"
+            f" Any breaks in the data? (1 yes, 0 no)  =  0\n"
+            f" Data analyzed by                       =  synthetic\n"
+            f" Any additional notes:\n"
+            f"    seeded synthetic spectrum\n")
+
+
+def spectrum(N, seed, pulsars):
+    sys.path.insert(0, ROOT)
+    from presto_b200 import synth
+    return synth.spectrum(synth.time_series(N, seed, pulsars)).astype(np.complex64)
+
+
+def main():
+    if not os.path.exists(PROG):
+        subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh")], check=True)
+    manifest = {}
+    for name, (N, seed, pulsars, opts) in CASES.items():
+        fft = spectrum(N, seed, pulsars)
+        with tempfile.TemporaryDirectory() as tmp:
+            root = os.path.join(tmp, name)
+            fft.tofile(root + ".fft")
+            with open(root + ".inf", "w") as f:
+                f.write(inf_text(name, N, DT))
+            r = subprocess.run([PROG] + opts + [name + ".fft"], cwd=tmp, capture_output=True,
+                               text=True, timeout=600)
+            if r.returncode:
+                raise RuntimeError(f"{name}: accelsearch exited {r.returncode}\n{r.stdout[-2000:]}")
+            dst = os.path.join(OUT, name)
+            shutil.rmtree(dst, ignore_errors=True)
+            os.makedirs(dst)
+            outs = sorted(f for f in os.listdir(tmp) if "_ACCEL_" in f)
+            for f in outs:
+                shutil.copy(os.path.join(tmp, f), dst)
+        manifest[name] = dict(N=N, seed=seed, dt=DT, pulsars=pulsars, options=opts,
+                              fft_sha256=hashlib.sha256(fft.tobytes()).hexdigest(), files=outs)
+        print(name, outs)
+    with open(os.path.join(OUT, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
