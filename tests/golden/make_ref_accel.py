@@ -41,6 +41,10 @@ CASES = {
     "std_locpow": (1 << 17, 14,
                    [dict(r=1700.6, z=-9.0, harms=[(0.08, 0.2), (0.05, 0.9)])],
                    ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-locpow"]),
+    # the plain search the benchmarks quote on the CPU-runnable size: N = 2^20,
+    # f = 123.4 Hz, z = 40, A = 0.05 (presto_b200.synth.cfg1_spectrum), in memory
+    "cfg1": (1 << 20, 1000, [dict(r=123.4 * (1 << 20) * DT, z=40.0, w=0.0, harms=[(0.05, 0.0)])],
+             ["-zmax", "200", "-numharm", "8"]),
     "noharmpolish": (1 << 17, 11,
                      [dict(r=1500.3, z=12.0, harms=[(0.08, 0.3), (0.05, 1.0), (0.03, 2.0)])],
                      ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-noharmpolish"]),
