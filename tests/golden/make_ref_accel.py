@@ -7,6 +7,9 @@ glib and ERFA, which this image lacks, are replaced by stand-ins written for
 this repository (oracle/refshim/).  Run here, where the reference tree is;
 the fixtures travel with the repository.
 
+Usage: python tests/golden/make_ref_accel.py [case ...] (all cases when none
+is named; the manifest keeps the other cases' entries).
+
 Per case: the .fft input is presto_b200.synth's seeded spectrum (its SHA-256
 is recorded so that a test can confirm it regenerated the same input), the
 .inf is a telescope "None (Artificial Data Set)" observation, and the
@@ -45,6 +48,12 @@ CASES = {
     # f = 123.4 Hz, z = 40, A = 0.05 (presto_b200.synth.cfg1_spectrum), in memory
     "cfg1": (1 << 20, 1000, [dict(r=123.4 * (1 << 20) * DT, z=40.0, w=0.0, harms=[(0.05, 0.0)])],
              ["-zmax", "200", "-numharm", "8"]),
+    # the larger search's parameters (zmax 600, 16 harmonics, standard mode) on
+    # N = 2^20: presto_b200.synth.cfg2_spectrum's three 8-harmonic pulsars
+    "cfg2s": (1 << 20, 2000, "cfg2", ["-zmax", "600", "-numharm", "16"]),
+    # -photon: Poisson counts at 4 per bin, 10 % modulated at r = 3100.4, z = 15;
+    # the spectrum is the raw transform, so nph = its DC term
+    "photon": (1 << 16, 15, "photon", ["-zmax", "40", "-numharm", "2", "-photon"]),
     "noharmpolish": (1 << 17, 11,
                      [dict(r=1500.3, z=12.0, harms=[(0.08, 0.3), (0.05, 1.0), (0.03, 2.0)])],
                      ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-noharmpolish"]),
@@ -63,16 +72,33 @@ def inf_text(name, N, dt):
 
 
 def spectrum(N, seed, pulsars):
+    """pulsars: injected signals, "cfg2" for synth.cfg2_spectrum's draw, or
+    "photon" for photon counts (raw transform, PRESTO's packing)"""
     sys.path.insert(0, ROOT)
     from presto_b200 import synth
+    if pulsars == "cfg2":
+        return synth.cfg2_spectrum(N=N, dt=DT, seed=seed)[0].astype(np.complex64)
+    if pulsars == "photon":
+        rng = np.random.default_rng(seed)
+        u = np.arange(N) / N
+        rate = 4.0 * (1.0 + 0.1 * np.cos(2.0 * np.pi * u * (3100.4 - 7.5 + 7.5 * u)))
+        x = rng.poisson(rate).astype(np.float32)
+        f = np.fft.rfft(x.astype(np.float64))
+        out = f[:N // 2].astype(np.complex64)
+        out[0] = complex(f[0].real, f[N // 2].real)
+        return out
     return synth.spectrum(synth.time_series(N, seed, pulsars)).astype(np.complex64)
 
 
 def main():
     if not os.path.exists(PROG):
         subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh")], check=True)
-    manifest = {}
+    mpath = os.path.join(OUT, "manifest.json")
+    manifest = json.load(open(mpath)) if os.path.exists(mpath) else {}
+    only = set(sys.argv[1:])
     for name, (N, seed, pulsars, opts) in CASES.items():
+        if only and name not in only:
+            continue
         fft = spectrum(N, seed, pulsars)
         with tempfile.TemporaryDirectory() as tmp:
             root = os.path.join(tmp, name)
@@ -80,7 +106,7 @@ def main():
             with open(root + ".inf", "w") as f:
                 f.write(inf_text(name, N, DT))
             r = subprocess.run([PROG] + opts + [name + ".fft"], cwd=tmp, capture_output=True,
-                               text=True, timeout=600)
+                               text=True, timeout=3600)
             if r.returncode:
                 raise RuntimeError(f"{name}: accelsearch exited {r.returncode}\n{r.stdout[-2000:]}")
             dst = os.path.join(OUT, name)
@@ -92,8 +118,8 @@ def main():
         manifest[name] = dict(N=N, seed=seed, dt=DT, pulsars=pulsars, options=opts,
                               fft_sha256=hashlib.sha256(fft.tobytes()).hexdigest(), files=outs)
         print(name, outs)
-    with open(os.path.join(OUT, "manifest.json"), "w") as f:
-        json.dump(manifest, f, indent=1)
+    with open(mpath, "w") as f:
+        json.dump(dict(sorted(manifest.items())), f, indent=1)
 
 
 if __name__ == "__main__":

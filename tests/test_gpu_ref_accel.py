@@ -4,7 +4,8 @@ src/accelsearch.c and the libpresto files it links, compiled unmodified, with
 FFTW / GSL / glib replaced by stand-ins written for this repository).
 
 Per case (acceleration search in standard and in-memory mode, jerk search,
--locpow, -noharmpolish), on the same seeded spectrum (its SHA-256 checked):
+-locpow, -noharmpolish, -photon, and the benchmark configurations' search
+parameters on N = 2^20), on the same seeded spectrum (its SHA-256 checked):
 * .txtcand: the same candidate insertions in the same order (numharm, r, z, w
   equal; power and sigma within the plane tolerance);
 * .cand: the same candidates in the same order, r, z, w equal, the
@@ -57,6 +58,8 @@ def _opts(options):
             kw["locpow"] = True
         elif o == "-noharmpolish":
             kw["noharmpolish"] = True
+        elif o == "-photon":
+            kw["photon"] = True          # the spectrum's DC term, set by the caller
         else:
             raise ValueError(o)
     return kw
@@ -110,7 +113,10 @@ def run(request, ctx, ablib, tmp_path_factory):
     root = str(tmp / name)
     with open(root + ".inf", "w") as f:
         f.write(mk.inf_text(name, case["N"], case["dt"]))
-    s = ablib.AccelSearch(ctx=ctx, sigma=2.0, **_opts(case["options"]))
+    kw = _opts(case["options"])
+    if kw.get("photon"):
+        kw["photon"] = float(fft[0].real)                # -photon: nph = fft[0].r
+    s = ablib.AccelSearch(ctx=ctx, sigma=2.0, **kw)
     res = s.run(fft, case["N"], case["dt"], rootname=root)
     names = ablib.accel_filenames(root, res["obs"])
     mine = {k: open(v, "rb").read() for k, v in names.items()}
