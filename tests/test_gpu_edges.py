@@ -17,7 +17,7 @@ def test_noise_search_at_high_sigma_is_empty(ctx, ablib):
     assert ctx.search(obs, ft) == []
     assert ctx.optimize_cands(obs, ft, []) == []
     res = ablib.AccelSearch(zmax=20, numharm=4, sigma=30.0, ctx=ctx).run(ft, N, DT)
-    assert res == dict(cands=[], polished=[], props=[])
+    assert (res["cands"], res["polished"], res["props"]) == ([], [], [])
 
 
 @pytest.mark.parametrize("inmem", [False, True])

@@ -347,8 +347,8 @@ def test_accelsearch_run_writes_cand_file(ctx, ablib, tmp_path):
 
 def test_accelsearch_run_writes_reference_files(ctx, ablib, oracle, tmp_path):
     """AccelSearch.run(rootname=...): <root>_ACCEL_<zmax> (text, the .inf
-    appended), its .cand and the empty .txtcand work file
-    (src/accel_utils.c:1667-1685); the text file is the oracle's restatement
+    appended), its .cand and the .txtcand work file (src/accel_utils.c:
+    1443-1447, 1667-1685); the text file is the oracle's restatement
     of output_fundamentals + output_harmonics of the same candidates,
     byte for byte."""
     N = 1 << 19
@@ -364,8 +364,15 @@ def test_accelsearch_run_writes_reference_files(ctx, ablib, oracle, tmp_path):
     assert res["cands"]
     names = ablib.accel_filenames(root, obs)
     assert names["accel"].endswith("cfg1_DM0.00_ACCEL_200")
-    assert os.path.getsize(names["txtcand"]) == 0
     assert os.path.getsize(names["cand"]) == 88 * len(res["cands"])
+    # .txtcand: one line per candidate an insertion added, in search order; every
+    # final candidate was added at some point with its own (numharm, r, z)
+    lines = [ln.split() for ln in open(names["txtcand"]).read().splitlines()]
+    assert lines and all(len(f) == 7 for f in lines)
+    added = {(int(f[2]), float(f[3]), float(f[5])) for f in lines}
+    unsorted = ablib.AccelSearch(zmax=200, numharm=8, sigma=2.0, ctx=ctx)(fft, N, DT)
+    for c in unsorted:
+        assert (c[2], float("%.4f" % c[3]), float("%.4f" % c[4])) in added, c
     got = open(names["accel"], "rb").read()
     want = oracle.accelfile_text(obs.T, float(obs.nph), obs.numw, res["cands"], res["polished"],
                                  inf)
