@@ -9,16 +9,16 @@
  *       and returns the middle value, or the mean of the two middle values
  *       in double for even n;
  *   gsl_vector_*            plain stride-1 vectors;
- *   nmsimplex2              GSL's Nelder-Mead variant as its manual and
- *       source describe it: an initial simplex x0, x0 + step_i e_i;
- *       per iteration reflect the worst vertex through the centre of all
- *       vertices (try_corner_move coefficient -1), expand (-2) when the
- *       reflection is the new best, else contract that vertex (0.5) or the
- *       whole simplex towards the best vertex; the centre and the squared
- *       size (mean squared distance of the vertices from the centre) kept up
- *       to date incrementally, recomputed after a whole contraction; norms
- *       as the reference BLAS dnrm2.  Floating-point order follows that
- *       description; iterates agree with GSL's to rounding;
+ *   nmsimplex2              Nelder & Mead (1965) as GSL's manual documents
+ *       its nmsimplex2 minimiser: an initial simplex x0, x0 + step_i e_i;
+ *       each iteration reflects the worst vertex through the centroid of the
+ *       others, expands when the reflection beats the best vertex, else
+ *       contracts that vertex halfway or, failing that, shrinks the simplex
+ *       towards the best vertex; the size is the RMS distance of the vertices
+ *       from their centroid, updated incrementally as vertices change and
+ *       recomputed after a shrink (the manual's distinction from nmsimplex);
+ *       vector norms as the reference BLAS dnrm2 (scaled sum of squares).
+ *       Iterates agree with GSL's only to rounding;
  *   gsl_rng / gsl_ran       not provided: birdie zapping (-zaplist) exits. */
 #include <math.h>
 #include <stdio.h>
@@ -137,14 +137,14 @@ static double feval(gsl_multimin_function *f, const double *x, size_t n)
     return f->f(&v, f->params);
 }
 
-static void compute_center(nm2_state *s)
+static void centroid_of(nm2_state *s)
 {
     memset(s->center, 0, sizeof(double) * s->n);
     for (size_t i = 0; i < s->P; i++) axpy(1.0, s->x1 + i * s->n, s->center, s->n);
     for (size_t j = 0; j < s->n; j++) s->center[j] *= 1.0 / (double) s->P;
 }
 
-static double compute_size(nm2_state *s)
+static double rms_size(nm2_state *s)
 {
     double ss = 0.0;
     for (size_t i = 0; i < s->P; i++) {
@@ -157,8 +157,10 @@ static double compute_size(nm2_state *s)
     return sqrt(ss / (double) s->P);
 }
 
-/* corner moved by coeff about the centre of all vertices */
-static double corner_move(nm2_state *s, gsl_multimin_function *f, double coeff, size_t corner,
+/* the vertex `corner` moved along the line through the centroid of all
+   vertices: coeff -1 reflects it through the centroid of the others, -2
+   expands, 0.5 contracts it halfway towards that centroid */
+static double trial_point(nm2_state *s, gsl_multimin_function *f, double coeff, size_t corner,
                           double *xc)
 {
     const double P = (double) s->P;
@@ -170,7 +172,10 @@ static double corner_move(nm2_state *s, gsl_multimin_function *f, double coeff, 
     return feval(f, xc, s->n);
 }
 
-static void update_point(nm2_state *s, size_t i, const double *x, double val)
+/* replaces vertex i, keeping the centroid and the squared size current
+   without a full recomputation (the property that distinguishes nmsimplex2
+   from nmsimplex in GSL's manual) */
+static void replace_vertex(nm2_state *s, size_t i, const double *x, double val)
 {
     const double P = (double) s->P;
     double *xo = s->x1 + i * s->n;
@@ -187,7 +192,9 @@ static void update_point(nm2_state *s, size_t i, const double *x, double val)
     s->y1[i] = val;
 }
 
-static int contract_by_best(nm2_state *s, gsl_multimin_function *f, size_t best)
+/* every vertex but the best moves halfway towards it; centroid and size
+   are recomputed */
+static int shrink_to_best(nm2_state *s, gsl_multimin_function *f, size_t best)
 {
     int status = GSL_SUCCESS;
     for (size_t i = 0; i < s->P; i++) {
@@ -197,8 +204,8 @@ static int contract_by_best(nm2_state *s, gsl_multimin_function *f, size_t best)
         s->y1[i] = feval(f, s->x1 + i * s->n, s->n);
         if (!isfinite(s->y1[i])) status = GSL_EBADFUNC;
     }
-    compute_center(s);
-    compute_size(s);
+    centroid_of(s);
+    rms_size(s);
     return status;
 }
 
@@ -252,8 +259,8 @@ int gsl_multimin_fminimizer_set(gsl_multimin_fminimizer *m, gsl_multimin_functio
         memcpy(s->x1 + (i + 1) * n, s->xc, sizeof(double) * n);
         s->y1[i + 1] = val;
     }
-    compute_center(s);
-    m->size = compute_size(s);
+    centroid_of(s);
+    m->size = rms_size(s);
     return GSL_SUCCESS;
 }
 
@@ -279,28 +286,28 @@ int gsl_multimin_fminimizer_iterate(gsl_multimin_fminimizer *m)
         }
     }
     (void) s_hi;
-    const double val = corner_move(s, f, -1.0, hi, s->xc);
+    const double val = trial_point(s, f, -1.0, hi, s->xc);
     if (isfinite(val) && val < s->y1[lo]) {
-        const double val2 = corner_move(s, f, -2.0, hi, s->xc2);
-        if (isfinite(val2) && val2 < s->y1[lo]) update_point(s, hi, s->xc2, val2);
-        else update_point(s, hi, s->xc, val);
+        const double val2 = trial_point(s, f, -2.0, hi, s->xc2);
+        if (isfinite(val2) && val2 < s->y1[lo]) replace_vertex(s, hi, s->xc2, val2);
+        else replace_vertex(s, hi, s->xc, val);
     } else if (!isfinite(val) || val > ds_hi) {
-        if (isfinite(val) && val <= s->y1[hi]) update_point(s, hi, s->xc, val);
-        const double val2 = corner_move(s, f, 0.5, hi, s->xc2);
+        if (isfinite(val) && val <= s->y1[hi]) replace_vertex(s, hi, s->xc, val);
+        const double val2 = trial_point(s, f, 0.5, hi, s->xc2);
         if (isfinite(val2) && val2 <= s->y1[hi]) {
-            update_point(s, hi, s->xc2, val2);
-        } else if (contract_by_best(s, f, lo) != GSL_SUCCESS) {
+            replace_vertex(s, hi, s->xc2, val2);
+        } else if (shrink_to_best(s, f, lo) != GSL_SUCCESS) {
             return GSL_FAILURE;
         }
     } else {
-        update_point(s, hi, s->xc, val);
+        replace_vertex(s, hi, s->xc, val);
     }
     size_t best = 0;
     for (size_t i = 1; i < s->P; i++)
         if (s->y1[i] < s->y1[best]) best = i;
     memcpy(m->x->data, s->x1 + best * s->n, sizeof(double) * s->n);
     m->fval = s->y1[best];
-    m->size = s->S2 > 0 ? sqrt(s->S2) : compute_size(s);
+    m->size = s->S2 > 0 ? sqrt(s->S2) : rms_size(s);
     return GSL_SUCCESS;
 }
 
