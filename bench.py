@@ -32,6 +32,16 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes moved per byte of f-fdot planes, from one ncu capture of each
+# kernel on the zmax=600 numharm=16 search at N=2^20 (one batch of 49 blocks,
+# 1.87 GB of planes): the 4096-point correlation launch read 0.17 GB and wrote
+# 1.81 GB for its 1.84 GB of planes (profiles/k_corr_4096_accelsearch_zmax600_
+# N2e20.md); the harmonic sum read 2.22 GB of the batch's 1.87 GB (profiles/
+# k_harmsum_std5_accelsearch_zmax600_N2e20.md).  Both move bytes in proportion
+# to the planes, so full-size launches scale by their plane bytes.
+CORR_DRAM_PER_PLANE_BYTE = (0.17 + 1.81) / 1.84
+HARMSUM_DRAM_PER_PLANE_BYTE = 2.22 / 1.87
+
 WORKLOADS = {
     "cfg2": dict(N=1 << 23, dt=64e-6, zmax=600, wmax=None, numharm=16, sigma=2.0,
                  desc="accelsearch N=2^23 dt=64us zmax=600 numharm=16 sigma=2; "
@@ -306,6 +316,14 @@ def run_ours(args):
     # ---- roofline of the dominant kernel (correlation) ----
     corr_ms_per_search = kms[2] / args.steps
     harm_ms = kms[3] / args.steps
+    # DRAM traffic per launch, standard mode: each kernel's measured DRAM bytes
+    # per byte of f-fdot planes (one ncu capture each on the zmax=600 numharm=16
+    # search at N=2^20) times this search's plane bytes per launch
+    corr_traffic = harm_traffic = None
+    if not obs.inmem and not tc and kn[2] and kn[3]:
+        planes = counts["harmsum_min_bytes"] * args.steps
+        corr_traffic = CORR_DRAM_PER_PLANE_BYTE * planes / kn[2]
+        harm_traffic = HARMSUM_DRAM_PER_PLANE_BYTE * planes / kn[3]
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -328,7 +346,10 @@ def run_ours(args):
         fp32_peak = measured_fp32_peak(ctx)
         roof = {"bound": "fp32", "kernel": "k_corr (template correlation)",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp32_peak, "traffic": None,
+                "frac": achieved / fp32_peak, "traffic": corr_traffic,
+                "traffic_unit": "DRAM bytes per launch (average over the search's correlation "
+                                "launches), scaled from profiles/k_corr_4096_accelsearch_zmax600"
+                                "_N2e20.md by plane bytes" if corr_traffic else None,
                 "flops_per_search": counts["corr_flops"],
                 "kernel_ms_per_search": corr_ms_per_search,
                 "peak_source": "measured in-run FP32 FMA loop (MEASURED_PEAKS.json "
@@ -360,6 +381,10 @@ def run_ours(args):
                                  "peak": hbm, "unit": "GB/s",
                                  "frac": counts["harmsum_min_bytes"] / (harm_ms / 1e3) / 1e9 / hbm,
                                  "bytes": "planes read once (the fused kernel's minimum)",
+                                 "traffic": harm_traffic,
+                                 "traffic_unit": "DRAM bytes per launch, scaled from profiles/"
+                                                 "k_harmsum_std5_accelsearch_zmax600_N2e20.md by "
+                                                 "plane bytes" if harm_traffic else None,
                                  "unfused_equivalent_gbs":
                                      counts["harmsum_bytes"] / (harm_ms / 1e3) / 1e9,
                                  "kernel_ms_per_search": harm_ms},
