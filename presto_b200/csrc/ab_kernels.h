@@ -158,7 +158,9 @@ struct RzwJob {
     long long acc_off;                      // double2 offset of the accumulator (npts > RZW_PMAX)
     int mode;                               // 0: z response, 1: w response, 2: copy a bin
     int nb, numkern, npts;
-    int nout, out_off;
+    int nout, out_off;                      // amplitudes out_amp[out_off .. + nout)
+    int j_off;                              // their correlation offsets out_j[j_off .. + nout),
+                                            // shared by the jobs of one volume
 };
 cudaError_t launch_rzw_jobs(const RzwJob *jobs, int njobs, const float2 *data, long long numdata,
                             const double2 *tw, float2 *resp, double2 *acc, const long long *out_j,

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(RZW_THREADS) k_rzw_jobs(const RzwJob *jobs, co
     __syncthreads();                        // the response is visible to the whole CTA
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int o = warp; o < jb.nout; o += nwarp) {
-        const long long j = out_j[jb.out_off + o];
+        const long long j = out_j[jb.j_off + o];
         const long long i0 = j >= 0 ? (j + nb - 1) / nb : -((-j) / nb);
         const long long i1 = (numkern - 1 + j) / nb;
         double ar = 0.0, ai = 0.0;
@@ -297,11 +297,26 @@ long long next2(long long x)
 struct Plan {
     long long numdata = 0;
     std::vector<RzwJob> jobs;
-    std::vector<long long> js;              // output offsets j, one per output
+    std::vector<long long> js;              // correlation offsets j of the outputs
+    long long namp = 0;                     // amplitudes (outputs) so far
     bool bad = false;
     char msg[200] = {0};
 
-    int outputs() const { return (int) js.size(); }
+    int outputs() const { return (int) namp; }
+
+    static long long chirp_points(double z, double w, int numkern, int nb)
+    {
+        // gen_w_response's num_pts_wdat (src/responses.c:381-382)
+        return next2(6LL * ab_resp_halfwidth(z, w) + 200 + numkern / nb);
+    }
+    void check_chirp(const RzwJob &jb)
+    {
+        if (jb.npts > RZW_NMAX || (jb.npts / 4) * jb.nb < jb.numkern / 2) {
+            bad = true;
+            snprintf(msg, sizeof msg, "response (z %.1f, w %.1f) needs %d chirp samples, "
+                     "above %lld", jb.z, jb.w, jb.npts, RZW_NMAX);
+        }
+    }
 
     // A new job (mode 0 / 1) with its first output.
     void open(int mode, double roffset, double z, double w, int nb, int hw, long long beginbin,
@@ -316,19 +331,32 @@ struct Plan {
         jb.numkern = 2 * nb * hw;
         jb.beginbin = beginbin;
         jb.out_off = outputs();
+        jb.j_off = (int) js.size();
         jb.nout = 0;
         if (mode == 1) {
-            // gen_w_response's num_pts_wdat (src/responses.c:381-382)
-            const long long npts = next2(6LL * ab_resp_halfwidth(z, w) + 200 + jb.numkern / nb);
-            if (npts > RZW_NMAX || (npts / 4) * nb < jb.numkern / 2) {
-                bad = true;
-                snprintf(msg, sizeof msg, "response (z %.1f, w %.1f) needs %lld chirp samples, "
-                         "above %lld", z, w, npts, RZW_NMAX);
-            }
-            jb.npts = (int) npts;
+            const long long npts = chirp_points(z, w, jb.numkern, nb);
+            jb.npts = (int) std::min<long long>(npts, 1LL << 30);
+            check_chirp(jb);
         }
         jobs.push_back(jb);
         add_output(j);
+    }
+    // A job with another response (mode, z, w) over the same data window and
+    // the same outputs as job `like` (the cells of one volume row).
+    void open_like(int like, int mode, double z, double w)
+    {
+        RzwJob jb = jobs[(size_t) like];
+        jb.mode = mode;
+        jb.z = z;
+        jb.w = w;
+        jb.npts = 0;
+        if (mode == 1) {
+            jb.npts = (int) std::min<long long>(chirp_points(z, w, jb.numkern, jb.nb), 1LL << 30);
+            check_chirp(jb);
+        }
+        jb.out_off = outputs();
+        namp += jb.nout;
+        jobs.push_back(jb);
     }
     void add_output(long long j)
     {
@@ -338,8 +366,13 @@ struct Plan {
             snprintf(msg, sizeof msg, "correlation offset %lld outside a %d-point response", j,
                      jb.numkern);
         }
+        if (jb.j_off + jb.nout != (int) js.size() || jb.out_off + jb.nout != namp) {
+            bad = true;                     // a shared list can not grow
+            snprintf(msg, sizeof msg, "jerk polishing plan: output appended to a shared list");
+        }
         js.push_back(j);
         jb.nout++;
+        namp++;
     }
     void copy_bin(long long bin)
     {
@@ -347,9 +380,11 @@ struct Plan {
         jb.mode = 2;
         jb.beginbin = bin;
         jb.out_off = outputs();
+        jb.j_off = (int) js.size();
         jb.nout = 1;
         jobs.push_back(jb);
         js.push_back(0);
+        namp++;
     }
 
     // rzw_interp at r with kern_half_width hw (src/rzwinterp.c:145-228, and
@@ -442,7 +477,7 @@ cudaError_t run_plan(Plan &plan, const float2 *data, const double2 *tw, size_t b
                      long long *launches)
 {
     cudaError_t e = dj.ensure(sizeof(long long) * plan.js.size());
-    if (e == cudaSuccess) e = damp.ensure(sizeof(float2) * plan.js.size());
+    if (e == cudaSuccess) e = damp.ensure(sizeof(float2) * (size_t) plan.namp);
     if (e == cudaSuccess && !plan.js.empty())
         e = cudaMemcpyAsync(dj.p, plan.js.data(), sizeof(long long) * plan.js.size(),
                             cudaMemcpyHostToDevice, st);
@@ -537,11 +572,19 @@ int rzw_optimize(const float2 *data, long long numdata, long long lobin, const a
             const double maxz = (fabs(zlo) < fabs(zhi)) ? zhi : zlo;
             const double maxw = (fabs(wlo) < fabs(whi)) ? whi : wlo;
             const int hw = w_halfwidth(maxz, maxw, false);
+            // every cell of the volume reads the same 24 output offsets
+            int first = -1;
             for (int ii = 0; ii < kNumZ; ii++)
                 for (int jj = 0; jj < kNumZ; jj++) {
                     const double z = zlo + jj * dz, w = wlo + ii * dw;
-                    pv.open(fabs(w) < 1E-4 ? 0 : 1, 0.0, z, w, kRzwNb, hw, lobin_h - hw, rind[0]);
+                    const int mode = fabs(w) < 1E-4 ? 0 : 1;
+                    if (first >= 0) {
+                        pv.open_like(first, mode, z, w);
+                        continue;
+                    }
+                    pv.open(mode, 0.0, z, w, kRzwNb, hw, lobin_h - hw, rind[0]);
                     for (int kk = 1; kk < kNumR; kk++) pv.add_output(rind[kk]);
+                    first = (int) pv.jobs.size() - 1;
                 }
         }
     }
@@ -606,7 +649,7 @@ int rzw_optimize(const float2 *data, long long numdata, long long lobin, const a
         return AB_ERR_ARG;
     }
     e = run_plan(pd, data, tw, budget, djobs, dresp, dacc, dj, damp, st, launches);
-    std::vector<float2> amp(pd.js.size());
+    std::vector<float2> amp((size_t) pd.namp);
     if (e == cudaSuccess && !amp.empty())
         e = cudaMemcpyAsync(amp.data(), damp.p, sizeof(float2) * amp.size(), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -705,11 +748,18 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
         const double maxw = (fabs(wlo) < fabs(whi)) ? whi : wlo;
         const int hw = w_halfwidth(maxz, maxw, false);
         vol_off[q] = pv.outputs();
+        int first = -1;
         for (int iw = 0; iw < numz; iw++)
             for (int jz = 0; jz < numz; jz++) {
                 const double z = zlo + jz * dz, w = wlo + iw * dw;
-                pv.open(fabs(w) < 1E-4 ? 0 : 1, 0.0, z, w, kRzwNb, hw, e.startbin - hw, 0);
+                const int mode = fabs(w) < 1E-4 ? 0 : 1;
+                if (first >= 0) {
+                    pv.open_like(first, mode, z, w);
+                    continue;
+                }
+                pv.open(mode, 0.0, z, w, kRzwNb, hw, e.startbin - hw, 0);
                 for (int kk = 1; kk < kNumR; kk++) pv.add_output(kk);
+                first = (int) pv.jobs.size() - 1;
             }
     }
     if (pv.bad) {
@@ -770,7 +820,7 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
         return AB_ERR_ARG;
     }
     e = run_plan(pd, data, tw, budget, djobs, dresp, dacc, dj, damp, st, launches);
-    std::vector<float2> amp(pd.js.size());
+    std::vector<float2> amp((size_t) pd.namp);
     if (e == cudaSuccess && !amp.empty())
         e = cudaMemcpyAsync(amp.data(), damp.p, sizeof(float2) * amp.size(), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
