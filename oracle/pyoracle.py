@@ -395,8 +395,9 @@ def optimize_cands(fft, lobin, cands, nthreads=1):
 
 def ref_polish_lib():
     """The reference's src/characteristics.c, rzinterp.c, rzwinterp.c,
-    responses.c, fresnl.c and vectors.c built by build_ref.sh (FFTW replaced by
-    oracle/refshim/refshim.c), or None.  Its functions exit() on arguments the
+    responses.c, fresnl.c, vectors.c and the libpresto files they call
+    (realfft, fftwcall), built by build_ref.sh against the FFTW / GSL stand-ins
+    of oracle/refshim/, or None.  Its functions exit() on arguments the
     reference rejects: call them with valid ones only."""
     path = os.path.join(HERE, "_ref", "libref_polish.so")
     if not os.path.exists(path):

@@ -1,8 +1,9 @@
 """The oracle and the product's host functions against the reference's own
 code, compiled here from its unmodified sources by oracle/build_ref.sh
 (src/characteristics.c, rzinterp.c, rzwinterp.c, responses.c, fresnl.c,
-vectors.c; FFTW's allocator and realfft supplied by oracle/refshim/refshim.c,
-an FP64 stand-in for FFTW).  Skipped when the reference tree is absent.
+vectors.c with the reference's own realfft and fftwcall, over the FFTW / GSL
+stand-ins of oracle/refshim/: FFTW's plans run an FP64 transform).  Skipped
+when the reference tree is absent.
 
 * gen_r_response / gen_z_response / gen_w_response (src/responses.c:159-418)
   against the oracle's restatements: within 2e-6 of the response's peak (the
