@@ -161,3 +161,26 @@ def test_obs_init_rejects_bad_options(ablib, bad):
     N = kw.pop("N")
     with pytest.raises(ablib.AccelError):
         ablib.obs_init(ablib.make_params(N, 64e-6, max(N // 2, 1), **kw))
+
+
+def test_candlist_worklog_lines_for_added_candidates_only():
+    """search_ffdotpows writes a .txtcand line only when insert_new_accelcand
+    adds or replaces (src/accel_utils.c:1443-1447): "%-7.2f  %-7.4f  %-2d
+    %-14.4f  %-14.9f  %-10.4f %-10.4f" of power, sigma, numharm, r, r/T, z, w."""
+    import presto_b200 as pb
+    T = 67.108864
+    lst = pb.CandList()
+    lst.set_worklog(True, T)
+    assert lst.insert(30.0, 5.0, 1, 1000.0, 2.0, 0.0) == 1      # new
+    assert lst.insert(20.0, 4.0, 2, 1005.0, 4.0, 0.0) == 0      # weaker, within 15 bins
+    assert lst.insert(40.0, 6.5, 2, 1007.5, -6.0, 20.0) == 1    # stronger: replaces
+    assert lst.insert(12.0, 2.5, 4, 3000.25, 1.5, 0.0) == 1     # new, far away
+    lines = lst.worklog().splitlines()
+    want = ["%-7.2f  %-7.4f  %-2d  %-14.4f  %-14.9f  %-10.4f %-10.4f" % a for a in (
+        (30.0, 5.0, 1, 1000.0, 1000.0 / T, 2.0, 0.0),
+        (40.0, 6.5, 2, 1007.5, 1007.5 / T, -6.0, 20.0),
+        (12.0, 2.5, 4, 3000.25, 3000.25 / T, 1.5, 0.0))]
+    assert lines == want
+    assert [c[3] for c in lst.get()] == [1007.5, 3000.25]
+    with pytest.raises(pb.AccelError):
+        lst.set_worklog(True, 0.0)
