@@ -75,3 +75,17 @@ done
 $CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/polish.map" -Wl,-z,defs \
     -o "$OUT/libref_polish.so" $POBJ $SOBJ "$OBJ/orc_stats.o" -lm
 echo "built $OUT/libref_polish.so from the same objects"
+# oracle/refdrv.c over the same objects (all but the program's main): the
+# reference's own create_accelobs / create_subharminfos / subharm_fderivs_vol
+# for plane-level checks
+echo 'REF { global: refdrv_open; refdrv_close; refdrv_geometry; refdrv_plane; local: *; };' \
+    > "$OUT/accel.map"
+$CC -O2 -g -fPIC -fopenmp -ffunction-sections -fdata-sections -DUSEMMAP -DUSE_FFTW_MALLOC \
+    -w -I "$HERE/refshim" -I "$REF/include" -c "$HERE/refdrv.c" -o "$OBJ/refdrv.o"
+LOBJ=""
+for f in $PRESTO_SRC; do
+    [ "$f" = accelsearch ] || LOBJ="$LOBJ $OBJ/$f.o"
+done
+$CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/accel.map" -Wl,-z,defs \
+    -o "$OUT/libref_accel.so" "$OBJ/refdrv.o" $LOBJ $SOBJ "$OBJ/orc_stats.o" -lm
+echo "built $OUT/libref_accel.so (oracle/refdrv.c over the reference objects)"

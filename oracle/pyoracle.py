@@ -423,6 +423,32 @@ def ref_polish_lib():
     return L
 
 
+def ref_accel_lib():
+    """oracle/refdrv.c over the reference's own objects (build_ref.sh): its
+    create_accelobs / create_subharminfos / subharm_fderivs_vol, or None."""
+    path = os.path.join(HERE, "_ref", "libref_accel.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    L.refdrv_open.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+    L.refdrv_geometry.argtypes = [C.POINTER(C.c_double)]
+    L.refdrv_plane.restype = C.c_longlong
+    L.refdrv_plane.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                               C.c_longlong, C.POINTER(C.c_longlong)]
+    return L
+
+
+def ref_plane(L, numharm, harmnum, lo, hi):
+    """(meta dict, powers [numws][numzs][numrs]) of the reference's
+    subharm_fderivs_vol for the search refdrv_open set up."""
+    meta = (C.c_longlong * 6)()
+    n = L.refdrv_plane(numharm, harmnum, lo, hi, None, 0, meta)
+    out = np.zeros(n, np.float32)
+    L.refdrv_plane(numharm, harmnum, lo, hi, out.ctypes.data, n, meta)
+    m = dict(zip(("rlo", "zlo", "wlo", "numrs", "numzs", "numws"), [int(v) for v in meta]))
+    return m, out.reshape(m["numws"], m["numzs"], m["numrs"])
+
+
 def ref_response(L, kind, numbetween, numkern, z=0.0, w=0.0, roffset=0.0):
     """gen_r/z/w_response of the reference build, copied out and freed."""
     if kind == "r":
