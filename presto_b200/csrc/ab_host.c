@@ -555,10 +555,10 @@ const char *ab_list_worklog_text(const ab_list *l, size_t *len)
 static int wlog_line(ab_list *l, float power, float sigma, int numharm, double rr, double zz,
                      double ww)
 {
-    char b[160];
+    char b[2048];                   /* %f of doubles up to 1e308 fits */
     const int k = snprintf(b, sizeof b, "%-7.2f  %-7.4f  %-2d  %-14.4f  %-14.9f  %-10.4f %-10.4f\n",
                            power, sigma, numharm, rr, rr / l->wlog_T, zz, ww);
-    if (k < 0) return -1;
+    if (k < 0 || (size_t) k >= sizeof b) return -1;
     if (l->wlen + (size_t) k + 1 > l->wcap) {
         size_t cap = l->wcap ? l->wcap : 4096;
         while (cap < l->wlen + (size_t) k + 1) cap *= 2;
