@@ -145,7 +145,7 @@ def cpu_sample(name, threads, budget_s=20.0, first_block=200):
     t_two = time.perf_counter() - t0 - t_setup
     per_block = max(t_two / max(done, 1), 1e-6)
     more = int(max(0, (budget_s - 2 * t_setup - t_two) / per_block))
-    more = min(more, 64)
+    more = min(max(more, 8), 64)            # at least 8 blocks (~0.3 s): a steadier per-block time
     if more > 0 and not obs.inmem:
         t0 = time.perf_counter()
         _, _, done2 = po.accelsearch(p, fft, nthreads=threads, first_block=first_block,
