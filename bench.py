@@ -135,22 +135,23 @@ def cpu_sample(name, threads, budget_s=20.0, first_block=200):
     obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
                                      numharm=w["numharm"], sigma=w["sigma"]))
     counts = pb.algorithmic_counts(obs)
-    t0 = time.perf_counter()
-    po.accelsearch(p, fft, nthreads=threads, first_block=first_block, max_blocks=0, prec=32)
-    t_setup = time.perf_counter() - t0
+    # the oracle times its template banks and its block loop itself; in memory
+    # every block up to the sample is computed (the plane needs all rows), so
+    # the sample starts at block 0 there
+    if obs.inmem:
+        first_block = 0
     nb = 2
-    t0 = time.perf_counter()
     _, _, done = po.accelsearch(p, fft, nthreads=threads, first_block=first_block, max_blocks=nb,
                                 prec=32)
-    t_two = time.perf_counter() - t0 - t_setup
-    per_block = max(t_two / max(done, 1), 1e-6)
-    more = int(max(0, (budget_s - 2 * t_setup - t_two) / per_block))
-    more = min(max(more, 8), 64)            # at least 8 blocks (~0.3 s): a steadier per-block time
+    t_setup, t_blocks = po.last_timing(32)
+    per_block = max(t_blocks / max(done, 1), 1e-6)
+    more = int(max(0, (budget_s - 2 * t_setup - t_blocks) / per_block))
+    more = min(max(more, 8), 64)            # at least 8 blocks (~0.3 s)
     if more > 0 and not obs.inmem:
-        t0 = time.perf_counter()
         _, _, done2 = po.accelsearch(p, fft, nthreads=threads, first_block=first_block,
                                      max_blocks=more, prec=32)
-        per_block = (time.perf_counter() - t0 - t_setup) / max(done2, 1)
+        t_setup, t_blocks = po.last_timing(32)
+        per_block = t_blocks / max(done2, 1)
         nb = done2
     t_search = t_setup + per_block * counts["blocks"]
     desc = (f"oracle port FP32 (scalar mixed-radix FFT, not FFTW), {threads} threads: template "

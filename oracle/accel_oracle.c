@@ -9,6 +9,7 @@
 #include "accel_oracle.h"
 
 #include <math.h>
+#include <time.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1133,6 +1134,23 @@ void orc_search_ffdotpows(const orc_ffdot *ffd, int numharm, const orc_obs *obs,
 /* ======================================================================
  * Full search: src/accelsearch.c:161-224
  * ==================================================================== */
+/* wall seconds of the last orc_accelsearch: template banks, then the block
+   loop (timing for the CPU baseline, which needs no subtraction) */
+static double g_t_setup, g_t_blocks;
+
+static double wall_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+void orc_last_timing(double *setup_s, double *blocks_s)
+{
+    *setup_s = g_t_setup;
+    *blocks_s = g_t_blocks;
+}
+
 long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthreads,
                           long long first_block, long long max_blocks,
                           orc_cand *cands, long long maxcands,
@@ -1147,6 +1165,7 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
     (void) nthreads;
 #endif
     if (numhits) *numhits = 0;
+    const double t0 = wall_s();
     const int stages = obs.numharmstages;
     orc_bank **banks = (orc_bank **) calloc(64, sizeof(orc_bank *));
     banks[0] = orc_bank_create(&obs, 1, 1);
@@ -1160,6 +1179,8 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
     const int rstep = obs.rstep;
     orc_list *l = orc_list_new();
     double startr, lastr, nextr;
+    const double t1 = wall_s();
+    g_t_setup = t1 - t0;
     if (obs.inmem) {
         startr = 8;
         while (startr < obs.rlo) {
@@ -1210,6 +1231,7 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
         startr = nextr;
         block++;
     }
+    g_t_blocks = wall_s() - t1;
     if (numblocks_done) *numblocks_done = done;
     long long nc = orc_list_get(l, cands, maxcands);
     orc_list_free(l);

@@ -134,6 +134,7 @@ void orc_inmem_add_ffdotpows(orc_ffdot *fund, const orc_obs *obs, const float *p
  * order when hits != NULL.  max_blocks < 0 means all blocks; otherwise only
  * blocks [first_block, first_block + max_blocks) of the main loop are
  * searched (bounded CPU samples).  Returns number of candidates or < 0. */
+void orc_last_timing(double *setup_s, double *blocks_s);
 long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthreads,
                           long long first_block, long long max_blocks,
                           orc_cand *cands, long long maxcands,

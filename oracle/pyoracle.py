@@ -228,6 +228,14 @@ def accelsearch(p, fft, nthreads=1, first_block=0, max_blocks=-1, maxcands=10000
     return cl, hl, nb.value
 
 
+def last_timing(prec=64):
+    """(template-bank seconds, block-loop seconds) of the last accelsearch."""
+    L = lib(prec)
+    a, b = C.c_double(), C.c_double()
+    L.orc_last_timing(C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
 def ref_fresnel_lib():
     """The reference's own fresnl.c built by build_ref.sh, or None."""
     path = os.path.join(HERE, "_ref", "libref_fresnl.so")
