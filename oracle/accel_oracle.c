@@ -5,6 +5,15 @@
  * reference's behaviour; every routine cites the reference file:line that
  * it restates.  ORC_REAL selects the arithmetic of the plane generation
  * (double: FP64 oracle, float: FP32 like FFTW single precision).
+ *
+ * Pinned against the reference's own code, compiled from its unmodified
+ * sources by oracle/build_ref.sh over stand-ins for FFTW / GSL / glib: the
+ * f-fdot planes (tests/test_cpu_ref_planes.py, within 3.7e-7 of power + mean
+ * power), the response generators, interpolators and candidate properties
+ * (tests/test_cpu_ref_pins.py), and the reference program's output files
+ * (tests/golden/ref_accel/, checked against the device).  What stays
+ * unpinned is the third-party arithmetic itself (FFTW's FP32 rounding, GSL's
+ * floating-point order).
  */
 #include "accel_oracle.h"
 
