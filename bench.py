@@ -59,8 +59,9 @@ METRIC = "f-fdot cells/s"
 UNIT = "cells/s"
 
 
-def make_spectrum(name, seed_offset=0):
-    from presto_b200 import synth
+def make_spectrum(name, seed_offset=0, synth=None):
+    if synth is None:
+        from presto_b200 import synth
     w = WORKLOADS[name]
     if name in ("cfg2", "cfg2s"):
         return synth.cfg2_spectrum(N=w["N"], dt=w["dt"], seed=2000 + seed_offset)[0]
@@ -123,41 +124,88 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
-def cpu_sample(name, threads, budget_s=20.0, first_block=200):
-    """Times the oracle port (FP32) on a bounded block sample of the workload;
-    returns (searches/s, cells/s, description)."""
-    import presto_b200 as pb
+def load_synth():
+    """presto_b200/synth.py (numpy only) loaded by path, so that the CPU legs
+    generate the same seeded spectra without importing the engine package."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_bench_synth", os.path.join(ROOT, "presto_b200", "synth.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def config_dict(name, blocks, cells):
+    """The workload as both arms name it (identical dicts)."""
+    w = WORKLOADS[name]
+    return {"workload": name, "desc": w["desc"], "N": w["N"], "zmax": w["zmax"],
+            "wmax": w["wmax"], "numharm": w["numharm"], "blocks": blocks,
+            "cells_per_search": cells,
+            "l2": "GPU arm: 256 MiB buffer written between timed steps",
+            "parallelism": "replicas (independent spectra per GPU); CPU arm: rank 0 only"}
+
+
+CPU_SAMPLE_STRIDE = 20          # every 20th block: a 5 % sample spread over the spectrum
+
+
+def cpu_sample(name, threads, fft=None, stride=CPU_SAMPLE_STRIDE, extras=False, max_blocks=None):
+    """The oracle port (FP32 arithmetic like the reference's FFTW path, OpenMP
+    over templates like the reference) timed on one search's template banks
+    plus every stride-th block of the main loop, scaled to the whole search
+    (in-memory searches run whole: their plane needs every block).  Geometry,
+    block count and cells come from the oracle's own obs_init.  Returns a
+    dict: cells/s, searches/s, the step's wall ms, description and, with
+    extras, the FFT share of thread time, a one-thread block-loop point and
+    the -march=native build's point."""
     from oracle import pyoracle as po
     w = WORKLOADS[name]
-    fft = make_spectrum(name)
+    if fft is None:
+        fft = make_spectrum(name, synth=load_synth())
     p = po.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
                        numharm=w["numharm"], sigma=w["sigma"])
-    obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
-                                     numharm=w["numharm"], sigma=w["sigma"]))
-    counts = pb.algorithmic_counts(obs)
-    # the oracle times its template banks and its block loop itself; in memory
-    # every block up to the sample is computed (the plane needs all rows), so
-    # the sample starts at block 0 there
-    if obs.inmem:
-        first_block = 0
-    nb = 2
-    _, _, done = po.accelsearch(p, fft, nthreads=threads, first_block=first_block, max_blocks=nb,
-                                prec=32)
-    t_setup, t_blocks = po.last_timing(32)
-    per_block = max(t_blocks / max(done, 1), 1e-6)
-    more = int(max(0, (budget_s - 2 * t_setup - t_blocks) / per_block))
-    more = min(max(more, 8), 64)            # at least 8 blocks (~0.3 s)
-    if more > 0 and not obs.inmem:
-        _, _, done2 = po.accelsearch(p, fft, nthreads=threads, first_block=first_block,
-                                     max_blocks=more, prec=32)
-        t_setup, t_blocks = po.last_timing(32)
-        per_block = t_blocks / max(done2, 1)
-        nb = done2
-    t_search = t_setup + per_block * counts["blocks"]
-    desc = (f"oracle port FP32 (scalar mixed-radix FFT, not FFTW), {threads} threads: template "
-            f"banks {t_setup:.2f} s + {nb} blocks timed at {per_block * 1e3:.1f} ms/block, "
-            f"scaled to {counts['blocks']} blocks")
-    return 1.0 / t_search, counts["cells"] / t_search, desc
+    obs = po.obs_init(p, 32)
+    counts = po.search_counts(obs)
+    nb = counts["blocks"]
+    first, count = (0, nb) if obs.inmem else (stride // 2, max(1, (nb - stride // 2 + stride - 1)
+                                                                 // stride))
+    if max_blocks is not None:
+        count = min(count, max_blocks)
+    t0 = time.perf_counter()
+    done, t_setup, t_blocks, fft_s, loop_s = po.accelsearch_sample(
+        p, fft, threads, first, count, 1 if obs.inmem else stride)
+    step_ms = (time.perf_counter() - t0) * 1e3
+    per_block = t_blocks / max(done, 1)
+    t_search = t_setup + per_block * nb
+    out = {"cells_per_s": counts["cells"] / t_search, "searches_per_s": 1.0 / t_search,
+           "step_ms": step_ms, "blocks": nb, "cells": counts["cells"],
+           "desc": (f"oracle port FP32 (project scalar mixed-radix FFT, not FFTW), {threads} "
+                    f"threads: template banks {t_setup:.2f} s + {done} of {nb} blocks "
+                    f"(every {1 if obs.inmem else stride}th from block {first}) at "
+                    f"{per_block * 1e3:.1f} ms/block, scaled to {nb} blocks"),
+           "fft_share": fft_s / max(loop_s, 1e-9)}
+    if extras and not obs.inmem:
+        k = max(1, count // 16)             # one-thread loop: a sixteenth of the sample
+        d1, _, tb1, _, _ = po.accelsearch_sample(p, fft, threads, first, k, stride * (count // k),
+                                                 loop_threads=1)
+        pb1 = tb1 / max(d1, 1)
+        out["one_thread"] = {"ms_per_block": pb1 * 1e3,
+                             "block_loop_cells_per_s": counts["cells"] / nb / pb1,
+                             "blocks_timed": d1,
+                             "openmp_speedup": pb1 / per_block,
+                             "what": "the block loop on 1 thread (template banks built on "
+                                     f"{threads} threads, not counted)"}
+        nat = po.build_native()
+        if nat:
+            dn, tsn, tbn, _, _ = po.accelsearch_sample(p, fft, threads, first, count, stride,
+                                                       libpath=nat)
+            tn = tsn + tbn / max(dn, 1) * nb
+            out["march_native"] = {"cells_per_s": counts["cells"] / tn,
+                                   "template_banks_s": tsn,
+                                   "ms_per_block": tbn / max(dn, 1) * 1e3,
+                                   "speedup_vs_default_build": t_search / tn,
+                                   "what": "the same oracle compiled with -march=native "
+                                           "on this host, same sample"}
+    return out
 
 
 def cpu_polish_sample(fft, lobin, cands, threads, jerk=False, max_cands=16):
@@ -176,35 +224,39 @@ def cpu_polish_sample(fft, lobin, cands, threads, jerk=False, max_cands=16):
 
 
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle port; the reference program
+    built here runs over a test-stand-in FFT and is never timed) on this
+    host's cores.  Nothing of the engine package is imported or loaded."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     name = args.workload
-    vals = []
-    desc = ""
-    for _ in range(args.warmup + args.steps):
-        sps, cps, desc = cpu_sample(name, threads, budget_s=args.cpu_budget / max(args.steps, 1))
-        vals.append(cps)
-    v = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+    fft = make_spectrum(name, synth=load_synth())
+    for _ in range(args.warmup):
+        cpu_sample(name, threads, fft=fft, max_blocks=1)         # banks + one block
+    steps = [cpu_sample(name, threads, fft=fft, extras=(k == 0)) for k in range(args.steps)]
+    first = steps[0]
+    v = statistics.median(st["cells_per_s"] for st in steps)
+    base = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": first["desc"] + "; median of the steps",
+            "fft_share_of_thread_time": first["fft_share"]}
+    for key in ("one_thread", "march_native"):
+        if key in first:
+            base[key] = first[key]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": name, "desc": WORKLOADS[name]["desc"]},
-            "searches_per_s": v / max(1.0, 1.0) / _cells_per_search(name),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": desc},
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(st["step_ms"] for st in steps),
+            "ms_per_step_is": "wall time of one step's sample (template banks + the block "
+                              "sample), not of a whole search",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": config_dict(name, first["blocks"], first["cells"]),
+            "searches_per_s": v / first["cells"],
+            "cpu_baseline": base,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
-
-
-def _cells_per_search(name):
-    import presto_b200 as pb
-    w = WORKLOADS[name]
-    obs = pb.obs_init(pb.make_params(w["N"], w["dt"], w["N"] // 2, zmax=w["zmax"], wmax=w["wmax"],
-                                     numharm=w["numharm"], sigma=w["sigma"]))
-    return pb.algorithmic_counts(obs)["cells"]
 
 
 def run_ours(args):
@@ -269,19 +321,30 @@ def run_ours(args):
     value = total_cells / (ms_max / 1e3)
 
     # ---- end to end through the C ABI with pinned host buffers ----
+    # each step: L2 flushed as in the device loop (outside the timed span),
+    # then the call with the spectrum in pinned host memory; the call returns
+    # once the candidates are on the host
     host = torch.from_numpy(fft.view(np.float32).copy()).pin_memory()
     host_np = host.numpy().view(np.complex64)
     ctx.search(obs, host_np)
     barrier()
-    t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    wall_ms = ev_ms = 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
         ctx.search(obs, host_np)
-    e1.record(stream)
+        e1.record(stream)
+        t1 = time.perf_counter()
+        e1.synchronize()
+        wall_ms += (t1 - t0) * 1e3
+        ev_ms += e0.elapsed_time(e1)
     barrier()
-    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+    e2e_ms = max(ev_ms, wall_ms)
     e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device=f"cuda:{local}")
     nhits = len(ctx.last_hits()[0])
 
@@ -363,12 +426,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16 hi+lo products, f32 accumulate" if tc else "f32",
             "data": "synthetic",
-            "config": {"workload": name, "desc": w["desc"], "N": w["N"], "zmax": w["zmax"],
-                       "wmax": w["wmax"], "numharm": w["numharm"], "blocks": counts["blocks"],
-                       "cells_per_search": counts["cells"],
-                       "corr": "tc_split_bf16" if tc else "fft_f32",
-                       "l2": "256 MiB buffer written between timed steps",
-                       "parallelism": f"replicas x{world} (independent spectra per GPU)"},
+            "config": config_dict(name, counts["blocks"], counts["cells"]),
+            "corr": "tc_split_bf16" if tc else "fft_f32",
             "searches_per_s": value / counts["cells"],
             "candidates_per_search": ncands,
             "gpu_launches": int(launches),
@@ -396,9 +455,11 @@ def run_ours(args):
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu:
-            sps, cps, desc = cpu_sample(name, os.cpu_count() or 1, budget_s=args.cpu_budget)
-            line["cpu_baseline"] = {"value": cps, "unit": UNIT, "cores": os.cpu_count() or 1,
-                                    "kind": "port", "sample": desc, "searches_per_s": sps}
+            cs = cpu_sample(name, os.cpu_count() or 1, fft=fft)
+            line["cpu_baseline"] = {"value": cs["cells_per_s"], "unit": UNIT,
+                                    "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": cs["desc"], "searches_per_s": cs["searches_per_s"],
+                                    "fft_share_of_thread_time": cs["fft_share"]}
             if polish and polish["candidates"]:
                 pms, pdesc = cpu_polish_sample(fft, obs.lobin, cl, os.cpu_count() or 1,
                                                jerk=bool(obs.numw))
@@ -547,7 +608,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="cfg2")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scratch-mb", type=int, default=0,
                     help="cap the engine's block scratch (profiling runs)")

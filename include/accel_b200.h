@@ -258,25 +258,32 @@ int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int
  * Inputs and outputs are device pointers owned by the caller: d_fft holds
  * obs->numbins bins; d_templates the bank of harmonic harmnum/numharm as
  * [numkern_wdim][numkern_zdim][L] FFT'd templates (L and the dimensions from
- * ab_bank_geometry, each template as ab_bank_kernel returns it); d_powers
- * receives powers[numws][numzs][numrs] (capacity in floats).  The block
- * starts at fullrlo and ends at fullrlo + rstep - 0.5.  Work is queued on
- * `stream` (a cudaStream_t, NULL for the default stream) of the calling
- * thread's current device; the call does not wait for it.
+ * ab_bank_geometry, each template as ab_bank_kernel returns it) in a buffer
+ * of templates_capacity complex values (AB_ERR_ARG when the bank needs more,
+ * e.g. after ab_set_transform_costs or ab_autotune changed L); d_powers
+ * receives powers[numws][numzs][numrs] (capacity in floats, else
+ * AB_ERR_OVERFLOW).  The block starts at fullrlo and ends at
+ * fullrlo + rstep - 0.5.  Work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream) of the calling thread's current device; the call
+ * does not wait for it.  A CUDA error already pending on the calling thread
+ * returns AB_ERR_STATE with nothing launched and the error left in place.
  * The engine's intermediates live in one static device array of 192 KiB
  * that every GPU loading the library keeps until exit, so the bank must need
  * at most 8192 correlation work items and a data spectrum of at most 4096
- * points; larger banks return AB_ERR_BUDGET (and a line on stderr).  The
+ * points, else AB_ERR_BUDGET (and a line on stderr); every bank that
+ * ab_bank_geometry accepts fits (at most ~4600 items and 2048 points).  The
  * array is shared by all calls and keeps the last call's contents; every
  * word a call reads is written earlier in the same call, so nothing needs
  * clearing, but calls whose GPU work overlaps (different streams, threads)
- * race on it.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress): make that first call before any stream capture.
+ * race on it.  The first call in each CUDA context looks up the array's
+ * address (cudaGetSymbolAddress) and caches it under the context's ID, so a
+ * context created after a cudaDeviceReset gets a fresh lookup: make that
+ * first call before any stream capture.
  * meta_out (optional) receives the plane's rlo, zlo, wlo and sizes. */
 int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnum, double fullrlo,
                            const ab_fcomplex *d_fft, const ab_fcomplex *d_templates,
-                           float *d_powers, size_t powers_capacity, void *stream,
-                           ab_ffdotpows *meta_out);
+                           size_t templates_capacity, float *d_powers, size_t powers_capacity,
+                           void *stream, ab_ffdotpows *meta_out);
 
 /* Batched and served searches (no counterpart in the reference, whose
  * accelsearch searches one spectrum per process: src/accelsearch.c:44-316).

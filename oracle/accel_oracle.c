@@ -852,6 +852,25 @@ static void get_amplitudes(const orc_obs *obs, const orc_fcomplex *fft, long lon
     }
 }
 
+static double wall_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+/* thread-seconds spent in the correlation's FFTs since the last search's
+   template banks were built (the CPU baseline reports the FFT share) */
+static double g_t_fft;
+
+static void fft_time_add(double s)
+{
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+    g_t_fft += s;
+}
+
 int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int numharm,
                             int harmnum, double fullrlo, double fullrhi, orc_bank *bank,
                             orc_ffdot *ffd)
@@ -936,7 +955,9 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
     free(data);
     free(lnorm);
     rcplx *tmp = (rcplx *) malloc(sizeof(rcplx) * L);
+    double tf0 = wall_s();
     cfft(pdata, tmp, L, -1);
+    fft_time_add(wall_s() - tf0);
     free(tmp);
     get_plan(L, +1);
 
@@ -951,6 +972,7 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
         rcplx *buf = (rcplx *) malloc(sizeof(rcplx) * L);
         rcplx *out = (rcplx *) malloc(sizeof(rcplx) * L);
         const fftplan *pl = get_plan(L, +1);
+        double t_fft = 0.0;
 #ifdef _OPENMP
 #pragma omp for collapse(2) schedule(static)
 #endif
@@ -963,7 +985,9 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
                     buf[kk].r = dr * kr + di * ki;
                     buf[kk].i = di * kr - dr * ki;
                 }
+                const double tf = wall_s();
                 fft_work(out, buf, 1, pl->fac, pl);      /* inverse FFT (:1174-1175) */
+                t_fft += wall_s() - tf;
                 float *op = ffd->powers + ((size_t) ii * nzs + jj) * nrs;
                 for (int kk = 0; kk < nrs; kk++) {         /* powers (:1183-1188) */
                     const rcplx v = out[kk + offset];
@@ -972,6 +996,7 @@ int orc_subharm_fderivs_vol(const orc_obs *obs, const orc_fcomplex *fft, int num
             }
         }
         free(buf); free(out);
+        fft_time_add(t_fft);
     }
     free(pdata);
     return 0;
@@ -1144,20 +1169,24 @@ void orc_search_ffdotpows(const orc_ffdot *ffd, int numharm, const orc_obs *obs,
  * Full search: src/accelsearch.c:161-224
  * ==================================================================== */
 /* wall seconds of the last orc_accelsearch: template banks, then the block
-   loop (timing for the CPU baseline, which needs no subtraction) */
-static double g_t_setup, g_t_blocks;
+   loop (timing for the CPU baseline, which needs no subtraction), and the
+   thread-seconds its block loop spent inside the correlation FFTs */
+static double g_t_setup, g_t_blocks, g_t_fft_blocks;
+static int g_threads_used = 1;
+static int g_loop_threads = 0;          /* block-loop threads; 0: as the banks */
 
-static double wall_s(void)
-{
-    struct timespec ts;
-    clock_gettime(CLOCK_MONOTONIC, &ts);
-    return ts.tv_sec + 1e-9 * ts.tv_nsec;
-}
+void orc_set_loop_threads(int n) { g_loop_threads = n > 0 ? n : 0; }
 
 void orc_last_timing(double *setup_s, double *blocks_s)
 {
     *setup_s = g_t_setup;
     *blocks_s = g_t_blocks;
+}
+
+void orc_last_fft_share(double *fft_thread_s, double *loop_thread_s)
+{
+    *fft_thread_s = g_t_fft_blocks;
+    *loop_thread_s = g_t_blocks * g_threads_used;
 }
 
 long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthreads,
@@ -1166,13 +1195,27 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
                           orc_hit *hits, long long maxhits, long long *numhits,
                           long long *numblocks_done)
 {
+    return orc_accelsearch_sample(p, fft, nthreads, first_block, max_blocks, 1, cands,
+                                  maxcands, hits, maxhits, numhits, numblocks_done);
+}
+
+long long orc_accelsearch_sample(const orc_params *p, const orc_fcomplex *fft, int nthreads,
+                                 long long first_block, long long max_blocks,
+                                 long long block_stride, orc_cand *cands, long long maxcands,
+                                 orc_hit *hits, long long maxhits, long long *numhits,
+                                 long long *numblocks_done)
+{
     orc_obs obs;
     if (orc_obs_init(p, &obs)) return -1;
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
+    g_threads_used = omp_get_max_threads();
 #else
     (void) nthreads;
+    g_threads_used = 1;
 #endif
+    if (block_stride < 1) block_stride = 1;
+    if (obs.inmem) block_stride = 1;        /* the plane needs every row */
     if (numhits) *numhits = 0;
     const double t0 = wall_s();
     const int stages = obs.numharmstages;
@@ -1188,8 +1231,15 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
     const int rstep = obs.rstep;
     orc_list *l = orc_list_new();
     double startr, lastr, nextr;
+#ifdef _OPENMP
+    if (g_loop_threads > 0) {
+        omp_set_num_threads(g_loop_threads);
+        g_threads_used = g_loop_threads;
+    }
+#endif
     const double t1 = wall_s();
     g_t_setup = t1 - t0;
+    g_t_fft = 0.0;
     if (obs.inmem) {
         startr = 8;
         while (startr < obs.rlo) {
@@ -1205,14 +1255,17 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
     startr = obs.rlo;
     long long block = 0, done = 0;
     while (startr + rstep < obs.highestbin) {
-        if (max_blocks >= 0 && block >= first_block + max_blocks) break;
-        int active = (block >= first_block) || obs.inmem;   /* inmem: plane needs all rows */
+        if (max_blocks >= 0 && block >= first_block + max_blocks * block_stride) break;
+        /* inmem: the plane needs all rows; a strided sample visits every
+           block_stride-th block from first_block */
+        int active = (block >= first_block && (block - first_block) % block_stride == 0) ||
+                     obs.inmem;
         nextr = startr + rstep;
         lastr = nextr - A_DR;
         if (active) {
             orc_ffdot fund;
             orc_subharm_fderivs_vol(&obs, fft, 1, 1, startr, lastr, banks[0], &fund);
-            int rec = block >= first_block;
+            int rec = block >= first_block && (block - first_block) % block_stride == 0;
             orc_search_ffdotpows(&fund, 1, &obs, rec ? l : NULL, block, rec ? hits : NULL,
                                  maxhits, numhits);
             if (stages > 1) {
@@ -1241,6 +1294,7 @@ long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthr
         block++;
     }
     g_t_blocks = wall_s() - t1;
+    g_t_fft_blocks = g_t_fft;
     if (numblocks_done) *numblocks_done = done;
     long long nc = orc_list_get(l, cands, maxcands);
     orc_list_free(l);

@@ -135,6 +135,20 @@ void orc_inmem_add_ffdotpows(orc_ffdot *fund, const orc_obs *obs, const float *p
  * blocks [first_block, first_block + max_blocks) of the main loop are
  * searched (bounded CPU samples).  Returns number of candidates or < 0. */
 void orc_last_timing(double *setup_s, double *blocks_s);
+/* Thread-seconds the last search's block loop spent in its correlation FFTs
+ * (forward and inverse) and the loop's wall time x threads. */
+void orc_last_fft_share(double *fft_thread_s, double *loop_thread_s);
+/* Threads of later searches' block loops (0: the template banks' count), so
+ * that a one-thread block loop can be timed without one-thread banks. */
+void orc_set_loop_threads(int n);
+/* The same search over every block_stride-th block from first_block
+ * (max_blocks of them; a CPU sample spread over the spectrum).  In-memory
+ * searches ignore the stride. */
+long long orc_accelsearch_sample(const orc_params *p, const orc_fcomplex *fft, int nthreads,
+                                 long long first_block, long long max_blocks,
+                                 long long block_stride, orc_cand *cands, long long maxcands,
+                                 orc_hit *hits, long long maxhits, long long *numhits,
+                                 long long *numblocks_done);
 long long orc_accelsearch(const orc_params *p, const orc_fcomplex *fft, int nthreads,
                           long long first_block, long long max_blocks,
                           orc_cand *cands, long long maxcands,

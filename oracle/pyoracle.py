@@ -106,6 +106,12 @@ def lib(prec=64):
         L.orc_calc_required_r.argtypes = [C.c_double, C.c_double]
         L.orc_calc_required_z.argtypes = [C.c_double, C.c_double]
         L.orc_calc_required_w.argtypes = [C.c_double, C.c_double]
+        L.orc_accelsearch_sample.restype = C.c_longlong
+        L.orc_accelsearch_sample.argtypes = [C.POINTER(Params), vp, C.c_int, C.c_longlong,
+                                             C.c_longlong, C.c_longlong, vp, C.c_longlong, vp,
+                                             C.c_longlong, C.POINTER(C.c_longlong),
+                                             C.POINTER(C.c_longlong)]
+        L.orc_last_fft_share.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_accelsearch.restype = C.c_longlong
         L.orc_accelsearch.argtypes = [C.POINTER(Params), vp, C.c_int, C.c_longlong,
                                       C.c_longlong, C.POINTER(Cand), C.c_longlong,
@@ -226,6 +232,72 @@ def accelsearch(p, fft, nthreads=1, first_block=0, max_blocks=-1, maxcands=10000
     cl = [(c.power, c.sigma, c.numharm, c.r, c.z, c.w) for c in cands[:min(nc, maxcands)]]
     hl = [(h.block, h.stage, h.wi, h.zi, h.ri, h.power) for h in hits[:min(nh.value, maxhits)]]
     return cl, hl, nb.value
+
+
+def accelsearch_sample(p, fft, nthreads, first_block, max_blocks, block_stride, prec=32,
+                       libpath=None, loop_threads=0):
+    """Times a search over every block_stride-th block from first_block
+    (max_blocks of them, hits and candidates not kept): returns (blocks done,
+    template-bank s, block-loop s, FFT thread-s, loop thread-s).  libpath
+    selects another build of the same oracle (e.g. one compiled with
+    -march=native); loop_threads > 0 runs the block loop on that many threads
+    (the template banks on nthreads)."""
+    L = lib(prec) if libpath is None else _lib_at(libpath)
+    nb = C.c_longlong()
+    fft = np.ascontiguousarray(fft, dtype=np.complex64)
+    L.orc_set_loop_threads(int(loop_threads))
+    try:
+        rc = L.orc_accelsearch_sample(C.byref(p), fft.ctypes.data, nthreads, first_block,
+                                      max_blocks, block_stride, None, 0, None, 0, None,
+                                      C.byref(nb))
+    finally:
+        L.orc_set_loop_threads(0)
+    if rc < 0:
+        raise RuntimeError("orc_accelsearch_sample failed")
+    a, b = C.c_double(), C.c_double()
+    L.orc_last_timing(C.byref(a), C.byref(b))
+    f, t = C.c_double(), C.c_double()
+    L.orc_last_fft_share(C.byref(f), C.byref(t))
+    return nb.value, a.value, b.value, f.value, t.value
+
+
+def _lib_at(path):
+    if path not in _libs:
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.orc_accelsearch_sample.restype = C.c_longlong
+        L.orc_accelsearch_sample.argtypes = [C.POINTER(Params), vp, C.c_int, C.c_longlong,
+                                             C.c_longlong, C.c_longlong, vp, C.c_longlong, vp,
+                                             C.c_longlong, C.POINTER(C.c_longlong),
+                                             C.POINTER(C.c_longlong)]
+        L.orc_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_last_fft_share.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _libs[path] = L
+    return _libs[path]
+
+
+def build_native():
+    """liboracle32n.so: the FP32 oracle compiled with -march=native for the
+    host it runs on (the reference's documented 1.5-2x build knob); None when
+    the compiler refuses."""
+    # always rebuilt (-B): a copy built on another host may use instructions
+    # this CPU lacks
+    r = subprocess.run(["make", "-s", "-B", "-C", HERE, "native"], capture_output=True, text=True)
+    path = os.path.join(HERE, "liboracle32n.so")
+    return path if r.returncode == 0 and os.path.exists(path) else None
+
+
+def search_counts(obs):
+    """Blocks and f-fdot cells of one search from the oracle's own geometry:
+    the main loop's block count (startr from rlo in steps of rstep while
+    startr + rstep < highestbin, src/accelsearch.c:187-189) and cells =
+    numrs x numz x max(numw, 1) per block per harmonic stage."""
+    nb, startr = 0, float(obs.rlo)
+    while startr + obs.rstep < obs.highestbin:
+        nb += 1
+        startr += obs.rstep
+    cells = nb * obs.corr_uselen * obs.numz * max(obs.numw, 1) * obs.numharmstages
+    return dict(blocks=nb, cells=cells)
 
 
 def last_timing(prec=64):

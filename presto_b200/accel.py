@@ -211,8 +211,8 @@ def lib():
     L.ab_pool_wait.argtypes = [vp, ll, C.POINTER(Cand), ll, C.POINTER(ll), C.POINTER(d)]
     L.ab_pool_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
     L.ab_pool_reset_stats.argtypes = [vp]
-    L.ab_fderivs_vol_noalloc.argtypes = [C.POINTER(Obs), i, i, d, vp, vp, vp, C.c_size_t, vp,
-                                         C.POINTER(FFDotPows)]
+    L.ab_fderivs_vol_noalloc.argtypes = [C.POINTER(Obs), i, i, d, vp, vp, C.c_size_t, vp,
+                                         C.c_size_t, vp, C.POINTER(FFDotPows)]
     L.ab_ctx_launch_count.restype = ll
     L.ab_ctx_launch_count.argtypes = [vp]
     _lib = L

@@ -35,22 +35,68 @@ static_assert(sizeof(ab_bank) <= kStartOff - kDescOff, "descriptor slot");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
+// The array's device address, looked up (cudaGetSymbolAddress) on the first
+// call in each CUDA context and cached by the context's process-unique ID
+// (cuCtxGetId), so that a context created later on the same device -- after
+// a cudaDeviceReset, or a caller's own driver-API context -- gets its own
+// lookup instead of a stale address.  The two driver functions come through
+// the runtime's entry-point query; the library does not link libcuda.
+typedef int (*ctx_get_current_fn)(void **ctx);
+typedef int (*ctx_get_id_fn)(void *ctx, unsigned long long *id);
+constexpr int kCacheSlots = 64;
 std::mutex g_mu;
-void *g_scratch_addr[kMaxDevices];
+ctx_get_current_fn g_get_current = nullptr;
+ctx_get_id_fn g_get_id = nullptr;
+bool g_entry_points_tried = false;
+unsigned long long g_ctx_id[kCacheSlots];
+void *g_scratch_addr[kCacheSlots];
+int g_next_slot = 0;
 
-// Address of the static array on the current device; the first call on a
-// device looks it up (cudaGetSymbolAddress) with that device current.
-cudaError_t scratch_address(int dev, unsigned char **out)
+// the current context's ID (0 when the thread has no current context yet)
+bool current_ctx_id(unsigned long long *id)
+{
+    *id = 0;
+    void *c = nullptr;
+    if (g_get_current(&c) != 0) return false;
+    if (c && g_get_id(c, id) != 0) return false;
+    return true;
+}
+
+cudaError_t scratch_address(unsigned char **out)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
+    if (!g_entry_points_tried) {
+        g_entry_points_tried = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void **) &g_get_current, 12000,
+                                             cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            g_get_current = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void **) &g_get_id, 12000,
+                                             cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            g_get_id = nullptr;
     }
-    *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+    if (!g_get_current || !g_get_id) return cudaErrorNotSupported;
+    unsigned long long id = 0;
+    if (!current_ctx_id(&id)) return cudaErrorDeviceUninitialized;
+    if (id)
+        for (int i = 0; i < kCacheSlots; i++)
+            if (g_ctx_id[i] == id) {
+                *out = static_cast<unsigned char *>(g_scratch_addr[i]);
+                return cudaSuccess;
+            }
+    // first call in this context: the lookup also makes the runtime's
+    // context current when the thread had none
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if (!current_ctx_id(&id) || !id) return cudaErrorDeviceUninitialized;
+    const int slot = g_next_slot;
+    g_next_slot = (g_next_slot + 1) % kCacheSlots;
+    g_ctx_id[slot] = id;
+    g_scratch_addr[slot] = p;
+    *out = static_cast<unsigned char *>(p);
     return cudaSuccess;
 }
 
@@ -72,11 +118,14 @@ __global__ void k_noalloc_setup(ab_bank desc, double startr, int ntmpl, int tile
 
 extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnum,
                                       double fullrlo, const ab_fcomplex *d_fft,
-                                      const ab_fcomplex *d_templates, float *d_powers,
-                                      size_t powers_capacity, void *stream,
+                                      const ab_fcomplex *d_templates, size_t templates_capacity,
+                                      float *d_powers, size_t powers_capacity, void *stream,
                                       ab_ffdotpows *meta_out)
 {
     if (!obs || !d_fft || !d_templates || !d_powers) return AB_ERR_ARG;
+    // a CUDA error left pending by the caller's own work stays the caller's:
+    // nothing is launched, so no error check below can consume it
+    if (cudaPeekAtLastError() != cudaSuccess) return AB_ERR_STATE;
     ab_bankset bs;
     if (ab_bankset_init(obs, &bs) != AB_OK) return AB_ERR_ARG;
     int k = -1;
@@ -96,7 +145,6 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
         meta_out->numzs = b.nz;
         meta_out->numws = b.nw;
     }
-    if (powers_capacity < need) return AB_ERR_OVERFLOW;
     if (g.numrs > b.numrs_max) return AB_ERR_ARG;
     const int G = b.L >= 4096 ? 1 : 4096 / b.L, tile = 16 * G;
     const int nitems = (b.ntmpl + tile - 1) / tile;
@@ -106,10 +154,13 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
                 harmnum, numharm, nitems, b.L / 2, kMaxItems, kScratchBytes);
         return AB_ERR_BUDGET;
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AB_ERR_CUDA;
+    // the template length follows the process-wide transform-cost table: a
+    // table changed since the caller built its templates changes L, which
+    // the capacity check catches before anything reads past them
+    if (templates_capacity < (size_t) b.ntmpl * b.L) return AB_ERR_ARG;
+    if (powers_capacity < need) return AB_ERR_OVERFLOW;
     unsigned char *scr = nullptr;
-    if (scratch_address(dev, &scr) != cudaSuccess) return AB_ERR_CUDA;
+    if (scratch_address(&scr) != cudaSuccess) return AB_ERR_CUDA;
     ab_bank *d_desc = reinterpret_cast<ab_bank *>(scr + kDescOff);
     double *d_start = reinterpret_cast<double *>(scr + kStartOff);
     CorrItem *d_items = reinterpret_cast<CorrItem *>(scr + kItemsOff);

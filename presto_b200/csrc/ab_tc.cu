@@ -83,7 +83,14 @@ __global__ void __launch_bounds__(128) k_tc_gemm(const float *A, const float *B,
         }
         tc::commit(&bar);
     }
-    const bool ok = tc::mbar_wait(&bar, 0, err, 2u);
+    bool ok = tc::mbar_wait(&bar, 0, err, 2u);
+    ok = __all_sync(0xffffffffu, ok);           // warp-uniform for the collective loads
+    if (!ok) {
+        // the output is discarded (the error word is set), but MMAs already
+        // issued still read shared memory and write tensor memory: wait for
+        // them (bounded again) before both are released
+        tc::mbar_wait(&bar, 0, err, 16u);
+    }
     tc::fence_after_sync();
     if (ok) {
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -302,6 +309,13 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
     __syncwarp();
     bool ok = tc::mbar_wait(&done, 0, sc.err, 8u);
     ok = __all_sync(0xffffffffu, ok);           // warp-uniform for the collective loads
+    if (!ok) {
+        // the batch's planes are discarded (the error word is set and the
+        // search returns AB_ERR_CUDA), but MMAs already issued still read the
+        // ring and the data operand and write tensor memory: wait for them
+        // (bounded again) before shared and tensor memory are released
+        tc::mbar_wait(&done, 0, sc.err, 16u);
+    }
     tc::fence_after_sync();
     if (ok) {
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -51,6 +51,9 @@ CASES = {
     # the larger search's parameters (zmax 600, 16 harmonics, standard mode) on
     # N = 2^20: presto_b200.synth.cfg2_spectrum's three 8-harmonic pulsars
     "cfg2s": (1 << 20, 2000, "cfg2", ["-zmax", "600", "-numharm", "16"]),
+    # the jerk search's parameters (zmax 200, wmax 300, 8 harmonics) on N = 2^18:
+    # presto_b200.synth.cfg3_spectrum's two 4-harmonic sinusoids
+    "cfg3s": (1 << 18, 3000, "cfg3", ["-zmax", "200", "-wmax", "300", "-numharm", "8"]),
     # -photon: Poisson counts at 4 per bin, 10 % modulated at r = 3100.4, z = 15;
     # the spectrum is the raw transform, so nph = its DC term
     "photon": (1 << 16, 15, "photon", ["-zmax", "40", "-numharm", "2", "-photon"]),
@@ -72,12 +75,14 @@ def inf_text(name, N, dt):
 
 
 def spectrum(N, seed, pulsars):
-    """pulsars: injected signals, "cfg2" for synth.cfg2_spectrum's draw, or
+    """pulsars: injected signals, "cfg2" / "cfg3" for synth's cfg2/cfg3 draws, or
     "photon" for photon counts (raw transform, PRESTO's packing)"""
     sys.path.insert(0, ROOT)
     from presto_b200 import synth
     if pulsars == "cfg2":
         return synth.cfg2_spectrum(N=N, dt=DT, seed=seed)[0].astype(np.complex64)
+    if pulsars == "cfg3":
+        return synth.cfg3_spectrum(N=N, dt=DT, seed=seed)[0].astype(np.complex64)
     if pulsars == "photon":
         rng = np.random.default_rng(seed)
         u = np.arange(N) / N
