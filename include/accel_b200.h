@@ -218,6 +218,14 @@ int ab_candlist_insert(ab_candlist *l, float power, float sigma, int numharm,
                        double r, double z, double w);
 int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd,
                         int numharm, ab_candlist *list);
+/* The threshold crossings search_ffdotpows visits (src/accel_utils.c:1412-1452),
+ * for callers that keep their own candidate list: every cell of ffd above
+ * obs->powcut[stage of numharm], in the reference's visit order (w, z, r),
+ * as (power, candidate_sigma, numharm, r, z, w) of the candidate it would
+ * insert.  *numhits gets the count; AB_ERR_OVERFLOW when it exceeds maxout
+ * (out may be NULL with maxout 0 to count). */
+int ab_ffdot_hits(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
+                  ab_cand *out, long long maxout, long long *numhits);
 
 /* The .txtcand work file: search_ffdotpows writes one line per candidate an
  * insertion adds, "%-7.2f  %-7.4f  %-2d  %-14.4f  %-14.9f  %-10.4f %-10.4f"

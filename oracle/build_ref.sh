@@ -89,3 +89,39 @@ done
 $CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/accel.map" -Wl,-z,defs \
     -o "$OUT/libref_accel.so" "$OBJ/refdrv.o" $LOBJ $SOBJ "$OBJ/orc_stats.o" -lm
 echo "built $OUT/libref_accel.so (oracle/refdrv.c over the reference objects)"
+# The same program linked the way an installed PRESTO is (src/meson.build: a
+# shared libpresto): libpresto_ref.so holds the libpresto objects with the
+# stand-ins, accelsearch_dyn links against it, and accelsearch_b200 is the
+# same unmodified accelsearch.o linked against presto_b200/libaccel_dropin.so
+# ahead of libpresto_ref.so, so that the dynamic linker binds the main
+# loop's accel.h calls (create_subharminfos, subharm_fderivs_vol,
+# add_ffdotpows, search_ffdotpows, ...) to the B200 engine and everything
+# else to the reference's own code.  accelsearch_dyn with
+# LD_PRELOAD=presto_b200/libaccel_dropin.so does the same to the stock link.
+# exported: what accelsearch.o imports, plus the list functions and the
+# accelcand destructor that the drop-in library calls back into
+{
+    printf 'REF { global: g_slist_alloc; g_slist_remove_link; g_slist_free_1; free_accelcand;\n'
+    nm -u "$OBJ/accelsearch.o" | awk '{ printf "  %s;\n", $2 }'
+    printf 'local: *; };\n'
+} > "$OUT/presto.map"
+$CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/presto.map" -Wl,-z,defs \
+    -o "$OUT/libpresto_ref.so" $LOBJ $SOBJ "$OBJ/orc_stats.o" -lm
+$CC -fopenmp -o "$OUT/accelsearch_dyn" "$OBJ/accelsearch.o" -L"$OUT" -lpresto_ref \
+    -Wl,-rpath,"\$ORIGIN" -lm
+echo "built $OUT/accelsearch_dyn (src/accelsearch.c over libpresto_ref.so)"
+DROPIN="$HERE/../presto_b200/libaccel_dropin.so"
+if [ -f "$DROPIN" ]; then
+    $CC -fopenmp -o "$OUT/accelsearch_b200" "$OBJ/accelsearch.o" \
+        -L"$HERE/../presto_b200" -laccel_dropin -L"$OUT" -lpresto_ref \
+        -Wl,-rpath,"\$ORIGIN" -Wl,-rpath,"\$ORIGIN/../../presto_b200" -lm
+    echo "built $OUT/accelsearch_b200 (src/accelsearch.c over libaccel_dropin.so, then libpresto_ref.so)"
+else
+    echo "build_ref.sh: $DROPIN not built; skipping accelsearch_b200" >&2
+fi
+# member offsets of the structures crossing the accel.h boundary, from the
+# reference's own header (checked against include/accel_dropin.h by
+# tests/test_cpu_dropin.py)
+$CC -w -I "$HERE/refshim" -I "$REF/include" -o "$OBJ/layout_probe" "$HERE/layout_probe.c"
+"$OBJ/layout_probe" > "$OUT/accel_layout.txt"
+echo "wrote $OUT/accel_layout.txt (the reference's accel.h structure layout)"

@@ -37,7 +37,7 @@ EXPORTS = [
     "ab_get_fourier_amplitudes", "ab_optimize_cands", "ab_realfft", "ab_deredden",
     "ab_series_to_fft", "ab_calc_props", "ab_calc_rzwerrs", "ab_cand_props",
     "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
-    "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog",
+    "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog", "ab_ffdot_hits",
 ]
 
 COST_SLOTS = 16
@@ -182,6 +182,8 @@ def lib():
     L.ab_candlist_get.argtypes = [vp, C.POINTER(Cand), ll]
     L.ab_candlist_insert.argtypes = [vp, C.c_float, C.c_float, i, d, d, d]
     L.ab_search_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, vp]
+    L.ab_ffdot_hits.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, C.POINTER(Cand), ll,
+                                C.POINTER(ll)]
     L.ab_block_stage_sums.argtypes = [vp, C.POINTER(Obs), vp, ll, vp, C.c_size_t]
     L.ab_gen_response.argtypes = [vp, d, i, d, d, i, vp]
     L.ab_bank_kernel.argtypes = [vp, C.POINTER(Obs), i, i, i, i, vp, i, C.POINTER(i)]

@@ -13,6 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libaccel_b200.so")
+# the reference's accel.h hot-path functions over the engine (include/accel_dropin.h)
+DROPIN = os.path.join(HERE, "libaccel_dropin.so")
+DROPIN_SRC = "accel_dropin.c"
 BUILD = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu", "ab_pool.cu", "ab_tc.cu", "ab_polish.cu", "ab_polish_rzw.cu", "ab_series.cu"]
@@ -35,16 +38,29 @@ def _nvcc():
 
 
 def sources():
-    return ([os.path.join(CSRC, s) for s in CU_SOURCES + C_SOURCES] +
+    return ([os.path.join(CSRC, s) for s in CU_SOURCES + C_SOURCES + [DROPIN_SRC]] +
             [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))] +
-            [os.path.join(ROOT, "include", "accel_b200.h")])
+            [os.path.join(ROOT, "include", h) for h in os.listdir(os.path.join(ROOT, "include"))])
 
 
 def up_to_date():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(DROPIN):
         return False
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(DROPIN))
     return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build_dropin():
+    """libaccel_dropin.so: links libaccel_b200.so (found beside it at run
+    time); glib's list functions and libpresto's free_accelcand stay
+    undefined, resolved from the accelsearch process that loads it."""
+    tmp = DROPIN + ".tmp"
+    cmd = [_cc()] + CC_FLAGS + ["-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+                                os.path.join(CSRC, DROPIN_SRC), "-o", tmp, "-L", HERE,
+                                "-laccel_b200", "-Wl,-rpath,$ORIGIN", "-lm"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, DROPIN)
+    return DROPIN
 
 
 def build(force=False, verbose=False, ptxas_info=False):
@@ -74,6 +90,7 @@ def build(force=False, verbose=False, ptxas_info=False):
            "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lm", "-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_dropin()
     return LIB
 
 

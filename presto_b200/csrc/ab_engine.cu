@@ -1698,10 +1698,14 @@ int ab_candlist_insert(ab_candlist *l, float power, float sigma, int numharm, do
     return ab_list_insert(l, power, sigma, numharm, r, z, w);
 }
 
-int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
-                        ab_candlist *list)
+// Threshold crossings of one host plane in the reference's visit order
+// (w, z, r: src/accel_utils.c:1418-1433) with their candidate coordinates
+// and sigma; the plane is copied to the device, thresholded there and the
+// crossings come back.
+static int plane_hits(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
+                      std::vector<ab_cand> &out)
 {
-    if (!ctx || !obs || !ffd || !list) return AB_ERR_ARG;
+    out.clear();
     int rc = use_device(ctx);
     if (rc) return rc;
     int stage = 0;
@@ -1738,10 +1742,34 @@ int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd,
         double rr = (ffd->rlo + ri * (double) AB_DR) / (double) numharm;
         double zz = (ffd->zlo + zi * (double) AB_DZ) / (double) numharm;
         double ww = (ffd->wlo + wi * (double) AB_DW) / (double) numharm;
-        if (ab_list_insert(list, pw, sig, numharm, rr, zz, ww) < 0)
-            return fail(ctx, AB_ERR_NOMEM, "candidate list");
+        out.push_back(ab_cand{pw, sig, numharm, rr, zz, ww});
     }
     return AB_OK;
+}
+
+int ab_search_ffdotpows(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
+                        ab_candlist *list)
+{
+    if (!ctx || !obs || !ffd || !list) return AB_ERR_ARG;
+    std::vector<ab_cand> hits;
+    int rc = plane_hits(ctx, obs, ffd, numharm, hits);
+    if (rc) return rc;
+    for (const ab_cand &h : hits)
+        if (ab_list_insert(list, h.power, h.sigma, numharm, h.r, h.z, h.w) < 0)
+            return fail(ctx, AB_ERR_NOMEM, "candidate list");
+    return AB_OK;
+}
+
+int ab_ffdot_hits(ab_ctx *ctx, const ab_obs *obs, const ab_ffdotpows *ffd, int numharm,
+                  ab_cand *out, long long maxout, long long *numhits)
+{
+    if (!ctx || !obs || !ffd || !numhits || (maxout > 0 && !out)) return AB_ERR_ARG;
+    std::vector<ab_cand> hits;
+    int rc = plane_hits(ctx, obs, ffd, numharm, hits);
+    *numhits = (long long) hits.size();
+    if (rc) return rc;
+    for (long long i = 0; i < (long long) hits.size() && i < maxout; i++) out[i] = hits[i];
+    return (long long) hits.size() > maxout ? AB_ERR_OVERFLOW : AB_OK;
 }
 
 int ab_set_worklog(ab_ctx *ctx, int on)
