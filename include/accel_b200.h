@@ -412,6 +412,39 @@ int ab_deredden(ab_ctx *ctx, ab_fcomplex *fft, long long numbins, int startwidth
 int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, int series_on_device,
                      ab_fcomplex *out, int out_on_device);
 
+/* Birdie zapping of -zaplist (src/accelsearch.c:87-110; accelsearch zaps
+ * only a spectrum it holds in memory, i.e. one made from a .dat time
+ * series):
+ *   ab_read_zaplist   get_birdies (src/birdzap.c:6-88): "<freq> <width>"
+ *                     lines in Hz (Doppler shifted by 1 + baryv), "B<freq>
+ *                     <width>" barycentric, '#' comments; each birdie at
+ *                     least one bin wide; sorted by low bin.  *numbirds gets
+ *                     the count (AB_ERR_OVERFLOW above maxbirds).  Blank or
+ *                     unparseable lines are skipped.
+ *   ab_zapbirds       the reference's loop over the sorted list: birdies
+ *                     from N/2 on are dropped, high edges clipped to N/2 - 1,
+ *                     each zapped as zapbirds (src/zapping.c:58-150) does --
+ *                     the bins replaced by exponential-power, uniform-phase
+ *                     noise at the local mean power (the median of 200
+ *                     bins each side, 100 bins out, over ln 2), drawn from
+ *                     GSL's MT19937 seeded with 1 (a fresh stream per call,
+ *                     as per accelsearch run).  fft_on_device: fft is a
+ *                     device pointer; only the bins read and written cross
+ *                     the bus.  *numzapped (optional) counts the birdies
+ *                     zapped (those with no room for either window are
+ *                     skipped, as the reference does with a warning).
+ *   ab_zapbirds_host  the same on a host spectrum, no context needed.
+ *   ab_mt19937_output the k-th (from 1) 32-bit output of that generator
+ *                     for a seed (GSL seeding; seed 0 means 4357), to check
+ *                     it against the generator's published outputs. */
+int ab_read_zaplist(const char *path, double T, double baryv, double *lobins, double *hibins,
+                    int maxbirds, int *numbirds);
+int ab_zapbirds(ab_ctx *ctx, ab_fcomplex *fft, int fft_on_device, long long numbins, long long N,
+                const double *lobins, const double *hibins, int numbirds, int *numzapped);
+int ab_zapbirds_host(ab_fcomplex *fft, long long numbins, long long N, const double *lobins,
+                     const double *hibins, int numbirds, int *numzapped);
+unsigned int ab_mt19937_output(unsigned long seed, long long k);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

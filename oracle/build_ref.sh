@@ -34,9 +34,9 @@ echo "built $OUT/libref_output.so from $REF/src/output.c"
 # our own for the third-party libraries that are not in this image
 # (refshim/refshim_fftw.c: FFTW's plans over an FP64 mixed-radix transform;
 # refshim_glib.c: GSList; refshim_gsl.c: CDFs from oracle/accel_oracle.c,
-# median, vectors, nmsimplex2, no random numbers; refshim_erfa.c: angle
-# conversions).  oracle/_ref/accelsearch runs like the installed program
-# (telescope "None (Artificial Data Set)" .inf files; no -zaplist).
+# median, vectors, nmsimplex2, MT19937; refshim_erfa.c: angle conversions).
+# oracle/_ref/accelsearch runs like the installed program (telescope "None
+# (Artificial Data Set)" .inf files).
 # libref_polish.so exports the polishing primitives, responses and candidate
 # properties from the same objects.
 OBJ="$OUT/obj"
@@ -89,6 +89,12 @@ done
 $CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/accel.map" -Wl,-z,defs \
     -o "$OUT/libref_accel.so" "$OBJ/refdrv.o" $LOBJ $SOBJ "$OBJ/orc_stats.o" -lm
 echo "built $OUT/libref_accel.so (oracle/refdrv.c over the reference objects)"
+# birdie zapping (src/zapping.c zapbirds, src/birdzap.c get_birdies) over
+# the same objects, with the stand-in's MT19937
+echo 'REF { global: zapbirds; get_birdies; local: *; };' > "$OUT/zap.map"
+$CC -shared -fopenmp -Wl,--gc-sections -Wl,--version-script="$OUT/zap.map" -Wl,-z,defs \
+    -o "$OUT/libref_zap.so" $LOBJ $SOBJ "$OBJ/orc_stats.o" -lm
+echo "built $OUT/libref_zap.so (zapbirds, get_birdies)"
 # The same program linked the way an installed PRESTO is (src/meson.build: a
 # shared libpresto): libpresto_ref.so holds the libpresto objects with the
 # stand-ins, accelsearch_dyn links against it, and accelsearch_b200 is the

@@ -1,7 +1,6 @@
 /* Declaration-only stand-in for GSL's gsl_rng.h: src/zapping.c (birdie
- * zapping, reached only with accelsearch -zaplist) includes it.  The
- * functions in oracle/refshim/refshim_gsl.c report that the stand-in has no
- * generator and exit.  Test infrastructure only. */
+ * zapping, reached only with accelsearch -zaplist) includes it; MT19937 is
+ * in oracle/refshim/refshim_gsl.c.  Test infrastructure only. */
 #ifndef REFSHIM_GSL_RNG_H
 #define REFSHIM_GSL_RNG_H
 typedef struct gsl_rng_type gsl_rng_type;

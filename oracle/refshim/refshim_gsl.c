@@ -19,7 +19,8 @@
  *       recomputed after a shrink (the manual's distinction from nmsimplex);
  *       vector norms as the reference BLAS dnrm2 (scaled sum of squares).
  *       Iterates agree with GSL's only to rounding;
- *   gsl_rng / gsl_ran       not provided: birdie zapping (-zaplist) exits. */
+ *   gsl_rng / gsl_ran       MT19937 with GSL's seeding, uniform and exponential
+ *       variates (birdie zapping, -zaplist); no Gaussian variates. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -319,26 +320,68 @@ int gsl_multimin_test_size(const double size, double epsabs)
     return size < epsabs ? GSL_SUCCESS : GSL_CONTINUE;
 }
 
-/* ---- random numbers: not provided ----------------------------------------- */
+/* ---- random numbers: MT19937 and the variates zapbirds draws ------------- */
+/* MT19937 (Matsumoto & Nishimura, ACM TOMACS 8 (1998) 3-30) with the 2002
+ * init_genrand seeding that GSL's gsl_rng_mt19937 documents (seed 0 means
+ * 4357); gsl_rng_uniform is the 32-bit output / 2^32 and gsl_ran_exponential
+ * -mu log1p(-u) (GSL 2.x).  Gaussian variates are not provided. */
 static void no_rng(void)
 {
-    fprintf(stderr, "GSL stand-in: random number generators are not provided "
-                    "(birdie zapping, -zaplist)\n");
+    fprintf(stderr, "GSL stand-in: Gaussian variates are not provided\n");
     exit(1);
 }
 
 struct gsl_rng_type {
     const char *name;
 };
+struct gsl_rng {
+    unsigned int s[624];
+    int next;
+};
 static const struct gsl_rng_type mt_type = {"mt19937"};
 const gsl_rng_type *gsl_rng_mt19937 = &mt_type;
 const gsl_rng_type *gsl_rng_default = &mt_type;
-gsl_rng *gsl_rng_alloc(const gsl_rng_type *T) { (void) T; no_rng(); return NULL; }
-void gsl_rng_free(gsl_rng *r) { (void) r; }
-void gsl_rng_set(const gsl_rng *r, unsigned long int seed) { (void) r; (void) seed; no_rng(); }
-unsigned long int gsl_rng_get(const gsl_rng *r) { (void) r; no_rng(); return 0; }
-double gsl_rng_uniform(const gsl_rng *r) { (void) r; no_rng(); return 0.0; }
+
+void gsl_rng_set(const gsl_rng *r, unsigned long int seed)
+{
+    gsl_rng *m = (gsl_rng *) r;
+    if (seed == 0) seed = 4357;
+    m->s[0] = (unsigned int) (seed & 0xffffffffUL);
+    for (int i = 1; i < 624; i++)
+        m->s[i] = (unsigned int) (1812433253UL * (m->s[i - 1] ^ (m->s[i - 1] >> 30)) + i);
+    m->next = 624;
+}
+
+gsl_rng *gsl_rng_alloc(const gsl_rng_type *T)
+{
+    (void) T;
+    gsl_rng *r = (gsl_rng *) calloc(1, sizeof(gsl_rng));
+    gsl_rng_set(r, 0);
+    return r;
+}
+
+void gsl_rng_free(gsl_rng *r) { free(r); }
+
+unsigned long int gsl_rng_get(const gsl_rng *r)
+{
+    gsl_rng *m = (gsl_rng *) r;
+    if (m->next >= 624) {
+        for (int k = 0; k < 624; k++) {
+            unsigned int y = (m->s[k] & 0x80000000u) | (m->s[(k + 1) % 624] & 0x7fffffffu);
+            m->s[k] = m->s[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        m->next = 0;
+    }
+    unsigned int y = m->s[m->next++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+double gsl_rng_uniform(const gsl_rng *r) { return gsl_rng_get(r) / 4294967296.0; }
 const gsl_rng_type *gsl_rng_env_setup(void) { return gsl_rng_default; }
 double gsl_ran_gaussian(const gsl_rng *r, double sigma) { (void) r; (void) sigma; no_rng(); return 0.0; }
 double gsl_ran_ugaussian(const gsl_rng *r) { (void) r; no_rng(); return 0.0; }
-double gsl_ran_exponential(const gsl_rng *r, double mu) { (void) r; (void) mu; no_rng(); return 0.0; }
+double gsl_ran_exponential(const gsl_rng *r, double mu) { return -mu * log1p(-gsl_rng_uniform(r)); }

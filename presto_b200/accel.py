@@ -38,6 +38,7 @@ EXPORTS = [
     "ab_series_to_fft", "ab_calc_props", "ab_calc_rzwerrs", "ab_cand_props",
     "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
     "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog", "ab_ffdot_hits",
+    "ab_read_zaplist", "ab_zapbirds", "ab_zapbirds_host", "ab_mt19937_output",
 ]
 
 COST_SLOTS = 16
@@ -182,6 +183,11 @@ def lib():
     L.ab_candlist_get.argtypes = [vp, C.POINTER(Cand), ll]
     L.ab_candlist_insert.argtypes = [vp, C.c_float, C.c_float, i, d, d, d]
     L.ab_search_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, vp]
+    L.ab_read_zaplist.argtypes = [C.c_char_p, d, d, vp, vp, i, C.POINTER(i)]
+    L.ab_zapbirds.argtypes = [vp, vp, i, ll, ll, vp, vp, i, C.POINTER(i)]
+    L.ab_zapbirds_host.argtypes = [vp, ll, ll, vp, vp, i, C.POINTER(i)]
+    L.ab_mt19937_output.restype = C.c_uint
+    L.ab_mt19937_output.argtypes = [C.c_ulong, ll]
     L.ab_ffdot_hits.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, C.POINTER(Cand), ll,
                                 C.POINTER(ll)]
     L.ab_block_stage_sums.argtypes = [vp, C.POINTER(Obs), vp, ll, vp, C.c_size_t]
@@ -656,6 +662,27 @@ class Context:
                                             out.ctypes.data, 0), "ab_series_to_fft")
         return out
 
+    def zapbirds(self, fft, N, lobins, hibins, device_ptr=None, numbins=None):
+        """-zaplist zapping (ab_zapbirds) of a host spectrum (returns the
+        zapped copy) or, with device_ptr, of numbins bins in device memory
+        (zapped in place; returns None).  The birdie count zapped is kept in
+        self.last_numzapped."""
+        lo = np.ascontiguousarray(lobins, dtype=np.float64)
+        hi = np.ascontiguousarray(hibins, dtype=np.float64)
+        nz = C.c_int()
+        if device_ptr is not None:
+            self._check(self.L.ab_zapbirds(self.ptr, C.c_void_p(device_ptr), 1, int(numbins),
+                                           int(N), lo.ctypes.data, hi.ctypes.data, lo.size,
+                                           C.byref(nz)), "ab_zapbirds")
+            self.last_numzapped = nz.value
+            return None
+        y = np.ascontiguousarray(fft, dtype=np.complex64).copy()
+        self._check(self.L.ab_zapbirds(self.ptr, y.ctypes.data, 0, y.size, int(N),
+                                       lo.ctypes.data, hi.ctypes.data, lo.size, C.byref(nz)),
+                    "ab_zapbirds")
+        self.last_numzapped = nz.value
+        return y
+
     def autotune(self):
         """Measure the correlation cost per transform length on this context's
         device and install it process-wide; returns the table."""
@@ -723,6 +750,39 @@ class CandList:
             pass
 
 
+def read_zaplist(path, T, baryv=0.0):
+    """get_birdies: (lobins, hibins) arrays of a zap list, sorted by low bin."""
+    L = lib()
+    n = C.c_int()
+    rc = L.ab_read_zaplist(str(path).encode(), float(T), float(baryv), None, None, 0, C.byref(n))
+    if rc not in (0, -4):
+        raise AccelError(f"ab_read_zaplist: {ERRORS.get(rc, rc)}")
+    lo = np.zeros(max(n.value, 1), np.float64)
+    hi = np.zeros(max(n.value, 1), np.float64)
+    rc = L.ab_read_zaplist(str(path).encode(), float(T), float(baryv), lo.ctypes.data,
+                           hi.ctypes.data, n.value, C.byref(n))
+    if rc:
+        raise AccelError(f"ab_read_zaplist: {ERRORS.get(rc, rc)}")
+    return lo[:n.value], hi[:n.value]
+
+
+def zapbirds_host(fft, N, lobins, hibins):
+    """ab_zapbirds_host: the zapped copy of a host spectrum (no GPU)."""
+    lo = np.ascontiguousarray(lobins, dtype=np.float64)
+    hi = np.ascontiguousarray(hibins, dtype=np.float64)
+    y = np.ascontiguousarray(fft, dtype=np.complex64).copy()
+    nz = C.c_int()
+    rc = lib().ab_zapbirds_host(y.ctypes.data, y.size, int(N), lo.ctypes.data, hi.ctypes.data,
+                                lo.size, C.byref(nz))
+    if rc:
+        raise AccelError(f"ab_zapbirds_host: {ERRORS.get(rc, rc)}")
+    return y
+
+
+def mt19937_output(seed, k):
+    return int(lib().ab_mt19937_output(int(seed), int(k)))
+
+
 def candidate_sigma(power, numsum, numtrials):
     return lib().ab_candidate_sigma(float(power), int(numsum), float(numtrials))
 
@@ -764,7 +824,23 @@ class AccelSearch:
         obs = self.obs(N, dt, fft.size)
         return self.ctx.search(obs, fft)
 
-    def run(self, fft, N, dt, harmremove=True, candfile=None, rootname=None):
+    def run_series(self, series, dt, zaplist=None, baryv=0.0, harmremove=True, candfile=None,
+                   rootname=None):
+        """accelsearch on a .dat time series (src/accel_utils.c:1507-1563 and
+        src/accelsearch.c:87-110): realfft and deredden on the device, the
+        -zaplist birdies zapped (zaplist: a zap-list file) in the device
+        spectrum, then run() with the reference's .dat conventions (no
+        .txtcand).  Returns run()'s dict."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        N = x.size
+        fft = self.ctx.series_to_fft(x, dt)
+        if zaplist is not None:
+            lo, hi = read_zaplist(zaplist, N * dt, baryv)
+            fft = self.ctx.zapbirds(fft, N, lo, hi)
+        return self.run(fft, N, dt, harmremove=harmremove, candfile=candfile, rootname=rootname,
+                        dat_input=True)
+
+    def run(self, fft, N, dt, harmremove=True, candfile=None, rootname=None, dat_input=False):
         """The whole of src/accelsearch.c:155-284 for one spectrum: the search,
         sort_accelcands, eliminate_harmonics (numharm > 1 unless harmremove
         is False, as -noharmremove), optimize_accelcand of every candidate on
@@ -777,13 +853,14 @@ class AccelSearch:
         reference.  Returns dict(cands, polished, props, obs)."""
         fft = np.ascontiguousarray(fft, dtype=np.complex64)
         obs = self.obs(N, dt, fft.size)
-        if rootname:
+        log = bool(rootname) and not dat_input      # .dat input: no .txtcand
+        if log:
             self.ctx.set_worklog(True)
         try:
             cands = self.ctx.search(obs, fft)
-            worklog = self.ctx.last_worklog() if rootname else ""
+            worklog = self.ctx.last_worklog() if log else ""
         finally:
-            if rootname:
+            if log:
                 self.ctx.set_worklog(False)
         polished, props = [], []
         if cands:
@@ -796,8 +873,9 @@ class AccelSearch:
                 write_candfile(candfile, props)
         if rootname:
             names = accel_filenames(rootname, obs)
-            with open(names["txtcand"], "w") as f:
-                f.write(worklog)
+            if not dat_input:
+                with open(names["txtcand"], "w") as f:
+                    f.write(worklog)
             if cands:
                 inf = rootname + ".inf"
                 write_accelfile(names["accel"], obs, cands, polished,

@@ -1357,6 +1357,41 @@ int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, i
     return AB_OK;
 }
 
+int ab_zapbirds(ab_ctx *ctx, ab_fcomplex *fft, int fft_on_device, long long numbins, long long N,
+                const double *lobins, const double *hibins, int numbirds, int *numzapped)
+{
+    if (!ctx || !fft || numbins < 0 || numbirds < 0 || (numbirds > 0 && (!lobins || !hibins)))
+        return AB_ERR_ARG;
+    if (!fft_on_device)
+        return ab_zapbirds_host(fft, numbins, N, lobins, hibins, numbirds, numzapped);
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    long long lo = 0, hi = 0;
+    if (ab_zap_bounds(numbins, N, lobins, hibins, numbirds, &lo, &hi))
+        return fail(ctx, AB_ERR_ARG, "a birdie lies outside the spectrum");
+    if (numzapped) *numzapped = 0;
+    if (hi <= lo) return AB_OK;
+    // the bins the zapping reads (measurement windows) and writes, to the host
+    std::vector<ab_fcomplex> span((size_t) (hi - lo));
+    CK(cudaMemcpyAsync(span.data(), fft + lo, sizeof(ab_fcomplex) * span.size(),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    rc = ab_zapbirds_span(span.data(), lo, numbins, N, lobins, hibins, numbirds, numzapped);
+    if (rc) return fail(ctx, rc, "zapping");
+    // and the zapped bins back
+    const double top = (double) (N / 2);
+    for (int i = 0; i < numbirds; i++) {
+        if (lobins[i] >= top) break;
+        const double hb = hibins[i] >= top ? top - 1 : hibins[i];
+        const long long a = (long long) floor(lobins[i]), b = (long long) ceil(hb);
+        if (b - a < 1) continue;
+        CK(cudaMemcpyAsync(fft + a, span.data() + (a - lo), sizeof(ab_fcomplex) * (size_t) (b - a),
+                           cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
 int ab_ctx_set_corr_path(ab_ctx *ctx, int path)
 {
     if (!ctx || (path != AB_CORR_FFT && path != AB_CORR_TC_SPLIT_BF16)) return AB_ERR_ARG;

@@ -90,6 +90,16 @@ int       ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pow
                          long long ntab, ab_list *l);
 /* Start frequencies of the main-loop blocks, accumulated exactly as the
  * reference's driver does (startr += rstep). */
+/* Birdie zapping (ab_zap.c): the span of bins [*span_lo, *span_hi) that the
+ * -zaplist loop reads and writes (AB_ERR_ARG when a birdie's bins lie outside
+ * the spectrum), and the loop over a host copy of that span (span[k] = bin
+ * base + k). */
+int       ab_zap_bounds(long long numbins, long long N, const double *lobins,
+                        const double *hibins, int numbirds, long long *span_lo,
+                        long long *span_hi);
+int       ab_zapbirds_span(ab_fcomplex *span, long long base, long long numbins, long long N,
+                           const double *lobins, const double *hibins, int numbirds,
+                           int *numzapped);
 void      ab_block_starts(const ab_obs *obs, double *out, long long n);
 void      ab_preblock_starts(const ab_obs *obs, double *out, long long n);
 

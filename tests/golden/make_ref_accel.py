@@ -10,8 +10,10 @@ the fixtures travel with the repository.
 Usage: python tests/golden/make_ref_accel.py [case ...] (all cases when none
 is named; the manifest keeps the other cases' entries).
 
-Per case: the .fft input is presto_b200.synth's seeded spectrum (its SHA-256
-is recorded so that a test can confirm it regenerated the same input), the
+Per case: the .fft input is presto_b200.synth's seeded spectrum, or for the
+.dat cases its seeded time series (the SHA-256 of the input is recorded so
+that a test can confirm it regenerated it; a zap list's text is kept in the
+manifest), the
 .inf is a telescope "None (Artificial Data Set)" observation, and the
 program's three outputs are kept: <root>_ACCEL_<zmax>[_JERK_<wmax>] (text),
 .cand (fourierprops records) and .txtcand (one line per candidate insertion
@@ -60,6 +62,20 @@ CASES = {
     "noharmpolish": (1 << 17, 11,
                      [dict(r=1500.3, z=12.0, harms=[(0.08, 0.3), (0.05, 1.0), (0.03, 2.0)])],
                      ["-zmax", "60", "-wmax", "0", "-numharm", "4", "-noharmpolish"]),
+    # a .dat time series (realfft + deredden inside accelsearch) with a zap
+    # list: a mains line, the injected pulsar's second harmonic (37.3 Hz
+    # fundamental, r ~ 625.8), a barycentric birdie, a narrow one widened to
+    # a bin, a wide one, one with no room below and one running past Nyquist
+    "datzap": (1 << 18, 16, [dict(r=37.3 * (1 << 18) * DT, z=8.0,
+                                  harms=[(0.08, 0.2), (0.08, 1.3), (0.06, 2.1), (0.05, 0.7)])],
+               ["-zmax", "60", "-numharm", "4", "-zaplist", "datzap.zaplist"]),
+}
+# inputs other than a seeded .fft: name -> {"dat": True} (the time series is
+# written as <name>.dat) and "zaplist": the text of <name>.zaplist
+INPUTS = {
+    "datzap": dict(dat=True, zaplist="# birdies for the .dat zapping case (Hz, width Hz)\n"
+                                      "50.0 0.1\n74.6 0.2\nB1234.5 0.05\n2000.0 0.01\n"
+                                      "3100.0 4.0\n1.0 0.2\n7811.5 3.0\n"),
 }
 
 
@@ -72,6 +88,13 @@ def inf_text(name, N, dt):
             f" Data analyzed by                       =  synthetic\n"
             f" Any additional notes:\n"
             f"    seeded synthetic spectrum\n")
+
+
+def series(N, seed, pulsars):
+    """the float32 time series of a .dat case"""
+    sys.path.insert(0, ROOT)
+    from presto_b200 import synth
+    return synth.time_series(N, seed, pulsars).astype(np.float32)
 
 
 def spectrum(N, seed, pulsars):
@@ -104,13 +127,18 @@ def main():
     for name, (N, seed, pulsars, opts) in CASES.items():
         if only and name not in only:
             continue
-        fft = spectrum(N, seed, pulsars)
+        extra = INPUTS.get(name, {})
+        data = series(N, seed, pulsars) if extra.get("dat") else spectrum(N, seed, pulsars)
+        suffix = ".dat" if extra.get("dat") else ".fft"
         with tempfile.TemporaryDirectory() as tmp:
             root = os.path.join(tmp, name)
-            fft.tofile(root + ".fft")
+            data.tofile(root + suffix)
             with open(root + ".inf", "w") as f:
                 f.write(inf_text(name, N, DT))
-            r = subprocess.run([PROG] + opts + [name + ".fft"], cwd=tmp, capture_output=True,
+            if "zaplist" in extra:
+                with open(root + ".zaplist", "w") as f:
+                    f.write(extra["zaplist"])
+            r = subprocess.run([PROG] + opts + [name + suffix], cwd=tmp, capture_output=True,
                                text=True, timeout=3600)
             if r.returncode:
                 raise RuntimeError(f"{name}: accelsearch exited {r.returncode}\n{r.stdout[-2000:]}")
@@ -121,7 +149,8 @@ def main():
             for f in outs:
                 shutil.copy(os.path.join(tmp, f), dst)
         manifest[name] = dict(N=N, seed=seed, dt=DT, pulsars=pulsars, options=opts,
-                              fft_sha256=hashlib.sha256(fft.tobytes()).hexdigest(), files=outs)
+                              fft_sha256=hashlib.sha256(data.tobytes()).hexdigest(), files=outs,
+                              **extra)
         print(name, outs)
     with open(mpath, "w") as f:
         json.dump(dict(sorted(manifest.items())), f, indent=1)

@@ -16,6 +16,7 @@ harmonics sit off their own maxima and move to first order), the coherent
 sum of a candidate's harmonics to 5e-3 + 0.03.  Printed columns may also
 round to neighbouring last digits.
 """
+import hashlib
 import importlib.util
 import json
 import os
@@ -48,9 +49,32 @@ def opts(options):
             kw["noharmpolish"] = True
         elif o == "-photon":
             kw["photon"] = True          # the spectrum's DC term, set by the caller
+        elif o == "-zaplist":
+            next(it)                     # the case's zap list, written by the caller
         else:
             raise ValueError(o)
     return kw
+
+
+def write_inputs(name, tmp):
+    """the case's input files in tmp (<name>.fft or <name>.dat, .inf and any
+    zap list); returns (input file name, the spectrum or series array)"""
+    case = MANIFEST[name]
+    mk = maker()
+    if case.get("dat"):
+        data = mk.series(case["N"], case["seed"], case["pulsars"])
+        fname = name + ".dat"
+    else:
+        data = mk.spectrum(case["N"], case["seed"], case["pulsars"])
+        fname = name + ".fft"
+    assert hashlib.sha256(data.tobytes()).hexdigest() == case["fft_sha256"]
+    data.tofile(os.path.join(tmp, fname))
+    with open(os.path.join(tmp, name + ".inf"), "w") as f:
+        f.write(mk.inf_text(name, case["N"], case["dt"]))
+    if "zaplist" in case:
+        with open(os.path.join(tmp, name + ".zaplist"), "w") as f:
+            f.write(case["zaplist"])
+    return fname, data
 
 
 def gold_files(name):

@@ -16,7 +16,6 @@ tolerances of tests/ref_compare.py.  The stock dynamically linked program
 same.  Both programs are built by oracle/build_ref.sh where the reference
 tree is present.
 """
-import hashlib
 import os
 import subprocess
 
@@ -33,13 +32,8 @@ DROPIN = os.path.join(ROOT, "presto_b200", "libaccel_dropin.so")
 
 def _run_program(name, tmp, argv0, env=None):
     case = rc.MANIFEST[name]
-    mk = rc.maker()
-    fft = mk.spectrum(case["N"], case["seed"], case["pulsars"])
-    assert hashlib.sha256(fft.tobytes()).hexdigest() == case["fft_sha256"]
-    fft.tofile(os.path.join(tmp, name + ".fft"))
-    with open(os.path.join(tmp, name + ".inf"), "w") as f:
-        f.write(mk.inf_text(name, case["N"], case["dt"]))
-    r = subprocess.run([argv0] + case["options"] + [name + ".fft"], cwd=tmp, capture_output=True,
+    fname, _ = rc.write_inputs(name, tmp)
+    r = subprocess.run([argv0] + case["options"] + [fname], cwd=tmp, capture_output=True,
                        text=True, timeout=1800, env=env)
     assert r.returncode == 0, (name, r.stdout[-3000:], r.stderr[-3000:])
     assert "on the GPU" in r.stdout, "the drop-in's create_subharminfos did not run"
@@ -54,7 +48,8 @@ def _check(name, mine, ablib):
     gold = rc.gold_files(name)
     numw = 1 if "-wmax" in rc.MANIFEST[name]["options"] and \
         int(rc.MANIFEST[name]["options"][rc.MANIFEST[name]["options"].index("-wmax") + 1]) else 0
-    rc.check_txtcand(name, mine["txtcand"], gold["txtcand"])
+    if "txtcand" in gold:
+        rc.check_txtcand(name, mine["txtcand"], gold["txtcand"])
     rc.check_candfile(name, mine["cand"], gold["cand"], ablib.FourierProps)
     rc.check_accelfile(name, numw, mine["accel"], gold["accel"])
 
