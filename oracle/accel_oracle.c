@@ -587,9 +587,12 @@ static void dfft_rec(dcplx *out, const dcplx *in, int n, int stride, int sign)
 {
     if (n == 1) { out[0] = in[0]; return; }
     int p = (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : (n % 5 == 0) ? 5 : n;
+    for (int f = 7; p == n && f * f <= n; f += 2)      /* else the smallest odd factor */
+        if (n % f == 0) p = f;
     int m = n / p;
     for (int q = 0; q < p; q++) dfft_rec(out + q * m, in + q * stride, m, stride * p, sign);
-    dcplx sc[64];
+    dcplx sc_small[64];
+    dcplx *sc = p <= 64 ? sc_small : (dcplx *) malloc(sizeof(dcplx) * (size_t) p);
     for (int k = 0; k < m; k++) {
         for (int q = 0; q < p; q++) {
             double a = sign * 2.0 * O_PI * (double) q * k / n;
@@ -608,6 +611,7 @@ static void dfft_rec(dcplx *out, const dcplx *in, int n, int stride, int sign)
             out[k + s * m] = acc;
         }
     }
+    if (sc != sc_small) free(sc);
 }
 
 void orc_cfft_double(double *data, int n, int sign)

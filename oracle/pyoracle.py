@@ -569,7 +569,7 @@ def realfft(series):
     """realfft(data, n, -1): n/2 complex bins, bin 0 = (DC, Nyquist)."""
     x = np.ascontiguousarray(series, dtype=np.float32).copy()
     if _series_lib().orc_realfft_forward(x.ctypes.data, x.size):
-        raise ValueError("realfft needs a length divisible by 4")
+        raise ValueError("realfft needs an even length")
     return x.view(np.complex64)
 
 

@@ -17,11 +17,11 @@
 
 #define S_TWOPI 6.28318530717958647692528676655900576
 
-/* realfft(data, n, -1): n real samples in, n/2 complex bins out in place,
- * bin 0 = (DC, Nyquist). */
+/* realfft(data, n, -1) (src/fastffts.c:163-229): n real samples in (any
+ * even n), n/2 complex bins out in place, bin 0 = (DC, Nyquist). */
 int orc_realfft_forward(float *data, long n)
 {
-    if (n < 4 || n % 4) return -1;
+    if (n < 4 || n % 2) return -1;
     const long nby2 = n >> 1, nby4 = n >> 2;
     double *d = (double *) malloc(sizeof(double) * (size_t) n);
     if (!d) return -1;

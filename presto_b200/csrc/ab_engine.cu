@@ -90,6 +90,8 @@ struct ab_ctx {
     int corr_path = AB_CORR_FFT;            // correlation path of searches and drop-ins
     DevBuf<float2> dtime;                   // normalised block data (tensor-core path)
     DevBuf<float2> ser_in, ser_scr;         // time-series input path
+    DevBuf<float2> blu_a, blu_b;            // Bluestein work and chirp-kernel transform
+    long long blu_M = 0;                    // the length blu_b was built for
     DevBuf<int2> dered_blocks;
     DevBuf<float> dered_means;
     DevBuf<TcItem> titems;
@@ -1035,6 +1037,9 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->dtime.release();
     ctx->ser_in.release();
     ctx->ser_scr.release();
+    ctx->blu_a.release();
+    ctx->blu_b.release();
+    ctx->blu_M = 0;
     ctx->dered_blocks.release();
     ctx->dered_means.release();
     ctx->titems.release();
@@ -1257,18 +1262,31 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
 static int realfft_dev(ab_ctx *ctx, const float *series, long long n, int series_on_device, float2 *dout)
 {
     if (!realfft_supported(n))
-        return fail(ctx, AB_ERR_ARG, "realfft length %lld: need n/2 a power of two in 512..8192 or "
-                                     "65536..2^26", n);
+        return fail(ctx, AB_ERR_ARG, "realfft length %lld: need an even length from 1024 to 2^26 "
+                                     "(n/2 a power of two up to 2^26, else up to 2^25)", n);
     const float *din = series;
     if (!series_on_device) {
-        CK(ctx->ser_in.ensure((size_t) (n / 2)));
+        CK(ctx->ser_in.ensure((size_t) ((n + 1) / 2)));
         CK(cudaMemcpyAsync(ctx->ser_in.p, series, sizeof(float) * n, cudaMemcpyHostToDevice,
                            ctx->stream));
         din = reinterpret_cast<const float *>(ctx->ser_in.p);
     }
-    CK(ctx->ser_scr.ensure((size_t) (n / 2)));
-    CK(launch_realfft(din, dout, ctx->ser_scr.p, n, ctx->stream));
-    ctx->launches += 6;
+    const long long M = n / 2;
+    if (pow2_fft_supported(M)) {
+        CK(ctx->ser_scr.ensure((size_t) M));
+        CK(launch_realfft(din, dout, ctx->ser_scr.p, n, ctx->stream));
+        ctx->launches += 6;
+        return AB_OK;
+    }
+    const long long L = bluestein_len(M);
+    CK(ctx->ser_scr.ensure((size_t) L));
+    CK(ctx->blu_a.ensure((size_t) L));
+    const bool fresh = ctx->blu_M != M || ctx->blu_b.n < (size_t) L;
+    CK(ctx->blu_b.ensure((size_t) L));
+    CK(launch_realfft_bluestein(din, dout, ctx->blu_a.p, ctx->ser_scr.p, ctx->blu_b.p, fresh, n,
+                                ctx->stream));
+    ctx->blu_M = M;
+    ctx->launches += fresh ? 24 : 17;
     return AB_OK;
 }
 

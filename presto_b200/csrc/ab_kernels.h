@@ -190,7 +190,13 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
 // time-series input path: realfft and deredden
 constexpr int AB_DERED_MAXW = 1024;     // longest de-reddening block
 bool realfft_supported(long long n);
+bool pow2_fft_supported(long long M);
+long long bluestein_len(long long M);
 cudaError_t launch_realfft(const float *series, float2 *out, float2 *scratch, long long n, cudaStream_t st);
+// any even n (1024 <= n <= 2^26): a: bluestein_len(n/2) points of work, scratch
+// as many, B the cached transform of the chirp kernel (rebuilt when build_B)
+cudaError_t launch_realfft_bluestein(const float *series, float2 *out, float2 *a, float2 *scratch,
+                                     float2 *B, bool build_B, long long n, cudaStream_t st);
 cudaError_t launch_deredden(float2 *fft, const int2 *blocks, int nb, float *means, cudaStream_t st);
 
 }  // namespace ab

@@ -4,11 +4,14 @@
 // 0.5/dt, n dt) (src/misc_utils.c:912-1067).
 //
 // realfft: the n/2-point complex FFT of the samples taken in pairs, then the
-// untangling pass into n/2 bins with bin 0 = (DC, Nyquist).  The complex FFT
-// is one radix-16 Stockham transform in shared memory up to 8192 points, and
-// above that a four-step transform M = M1 M2: transpose, M2 transforms of
-// length M1 multiplied by exp(-2 pi i n2 k1 / M), transpose, M1 transforms of
-// length M2, transpose (each step one pass over HBM).
+// untangling pass into n/2 bins with bin 0 = (DC, Nyquist).  For a
+// power-of-two M = n/2 the complex FFT is one radix-16 Stockham transform in
+// shared memory up to 8192 points, and above that a four-step transform
+// M = M1 M2: transpose, M2 transforms of length M1 multiplied by
+// exp(-2 pi i n2 k1 / M), transpose, M1 transforms of length M2, transpose
+// (each step one pass over HBM).  Any other even n (dedispersed series are
+// usually 2^a 3^b 5^c 7^d samples long) goes through Bluestein's chirp-z
+// transform on three power-of-two transforms of length >= 2M - 1.
 //
 // deredden: the block partition depends only on bin indices (lengths
 // startwidth ln(bin) up to endwidth), so the host plans it; one CTA per block
@@ -192,39 +195,139 @@ cudaError_t transpose(const float2 *in, float2 *out, int R, int C, cudaStream_t 
     return cudaGetLastError();
 }
 
+// Forward complex FFT of M points, M a power of two in 512..8192 or 2^16..2^26;
+// out may be in, scratch (M points) may not.
+cudaError_t cfft_pow2(const float2 *in, float2 *out, float2 *scratch, long long M, cudaStream_t st)
+{
+    if (M <= 8192) return fft_rows((int) M, in, out, 1, 0, st);
+    int m = 0;
+    while ((1LL << m) < M) m++;
+    const int M1 = 1 << (m / 2), M2 = (int) (M / M1);
+    // x[n1][n2] (M1 x M2) -> scratch[n2][n1]; rows of length M1 with the
+    // twiddle; -> out[k1][n2]; rows of length M2; -> scratch[k2][k1]; copy
+    cudaError_t e = transpose(in, scratch, M1, M2, st);
+    if (e == cudaSuccess) e = fft_rows(M1, scratch, scratch, M2, M, st);
+    if (e == cudaSuccess) e = transpose(scratch, out, M2, M1, st);
+    if (e == cudaSuccess) e = fft_rows(M2, out, out, M1, 0, st);
+    if (e == cudaSuccess) e = transpose(out, scratch, M1, M2, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, scratch, sizeof(float2) * M, cudaMemcpyDeviceToDevice, st);
+    return e;
+}
+
+// Bluestein's chirp-z transform for any length M: with c_j = exp(i pi j^2 / M),
+// X_k = conj(c_k) sum_j (x_j conj(c_j)) c_{k-j}, a linear convolution done as
+// a circular one of power-of-two length L >= 2M - 1.  Chirps are evaluated in
+// FP64 from j^2 mod 2M (exact in 64-bit integers), the products with them in
+// FP64; the three length-L transforms are the FP32 power-of-two FFT above.
+__device__ __forceinline__ void chirp(long long j, long long M, double &c, double &s)
+{
+    const long long r = (j * j) % (2 * M);
+    sincospi((double) r / (double) M, &s, &c);
+}
+
+__global__ void k_blu_pre(const float2 *z, float2 *a, long long M, long long L)
+{
+    const long long j = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    if (j >= M) {
+        a[j] = make_float2(0.f, 0.f);
+        return;
+    }
+    double c, s;
+    chirp(j, M, c, s);
+    const double xr = z[j].x, xi = z[j].y;           // x conj(c)
+    a[j] = make_float2((float) (xr * c + xi * s), (float) (xi * c - xr * s));
+}
+
+__global__ void k_blu_kernel(float2 *b, long long M, long long L)
+{
+    const long long j = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    const long long m = j < M ? j : (j > L - M ? L - j : -1);
+    if (m < 0) {
+        b[j] = make_float2(0.f, 0.f);
+        return;
+    }
+    double c, s;
+    chirp(m, M, c, s);
+    b[j] = make_float2((float) c, (float) s);
+}
+
+// a = conj(a B): the inverse transform as a forward one of the conjugate
+__global__ void k_blu_mul(float2 *a, const float2 *B, long long L)
+{
+    const long long j = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    const float2 x = a[j], y = B[j];
+    a[j] = make_float2(x.x * y.x - x.y * y.y, -(x.x * y.y + x.y * y.x));
+}
+
+__global__ void k_blu_post(const float2 *v, float2 *out, long long M, long long L)
+{
+    const long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    double c, s;
+    chirp(k, M, c, s);
+    const double inv = 1.0 / (double) L;
+    const double yr = (double) v[k].x * inv, yi = -(double) v[k].y * inv;   // conj(v) / L
+    out[k] = make_float2((float) (yr * c + yi * s), (float) (yi * c - yr * s));
+}
+
 }  // namespace
+
+bool pow2_fft_supported(long long M)
+{
+    if (M & (M - 1)) return false;
+    return (M >= 512 && M <= 8192) || (M >= (1 << 16) && M <= (1LL << 26));
+}
+
+long long bluestein_len(long long M)
+{
+    long long L = 1;
+    while (L < 2 * M - 1) L <<= 1;
+    if (L < 512) L = 512;
+    if (L > 8192 && L < (1 << 16)) L = 1 << 16;       // the four-step's shortest
+    return L;
+}
 
 bool realfft_supported(long long n)
 {
-    if (n < 1024 || n % 4) return false;
+    if (n < 1024 || n % 2) return false;
     const long long M = n / 2;
-    if (M & (M - 1)) return false;
-    return M <= 8192 || (M >= (1 << 16) && M <= (1LL << 26));
+    return pow2_fft_supported(M) || M <= (1LL << 25);
 }
 
 cudaError_t launch_realfft(const float *series, float2 *out, float2 *scratch, long long n, cudaStream_t st)
 {
-    if (!realfft_supported(n)) return cudaErrorInvalidValue;
     const long long M = n / 2;
-    const float2 *in = reinterpret_cast<const float2 *>(series);
-    cudaError_t e;
-    if (M <= 8192) {
-        e = fft_rows((int) M, in, out, 1, 0, st);
-    } else {
-        int m = 0;
-        while ((1LL << m) < M) m++;
-        const int M1 = 1 << (m / 2), M2 = (int) (M / M1);
-        // x[n1][n2] (M1 x M2) -> scratch[n2][n1]; rows of length M1 with the
-        // twiddle; -> out[k1][n2]; rows of length M2; -> scratch[k2][k1]; copy
-        e = transpose(in, scratch, M1, M2, st);
-        if (e == cudaSuccess) e = fft_rows(M1, scratch, scratch, M2, M, st);
-        if (e == cudaSuccess) e = transpose(scratch, out, M2, M1, st);
-        if (e == cudaSuccess) e = fft_rows(M2, out, out, M1, 0, st);
-        if (e == cudaSuccess) e = transpose(out, scratch, M1, M2, st);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(out, scratch, sizeof(float2) * M, cudaMemcpyDeviceToDevice, st);
-    }
+    if (n % 2 || !pow2_fft_supported(M)) return cudaErrorInvalidValue;
+    cudaError_t e = cfft_pow2(reinterpret_cast<const float2 *>(series), out, scratch, M, st);
     if (e != cudaSuccess) return e;
+    const long long nthr = M / 2 + 1;
+    k_untangle<<<(unsigned) ((nthr + 255) / 256), 256, 0, st>>>(out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_realfft_bluestein(const float *series, float2 *out, float2 *a, float2 *scratch,
+                                     float2 *B, bool build_B, long long n, cudaStream_t st)
+{
+    const long long M = n / 2, L = bluestein_len(M);
+    if (n % 2 || n < 1024 || M > (1LL << 25)) return cudaErrorInvalidValue;
+    const unsigned gL = (unsigned) ((L + 255) / 256), gM = (unsigned) ((M + 255) / 256);
+    cudaError_t e = cudaSuccess;
+    if (build_B) {                                   // FFT of the chirp kernel, kept per M
+        k_blu_kernel<<<gL, 256, 0, st>>>(B, M, L);
+        e = cfft_pow2(B, B, scratch, L, st);
+        if (e != cudaSuccess) return e;
+    }
+    k_blu_pre<<<gL, 256, 0, st>>>(reinterpret_cast<const float2 *>(series), a, M, L);
+    e = cfft_pow2(a, a, scratch, L, st);
+    if (e != cudaSuccess) return e;
+    k_blu_mul<<<gL, 256, 0, st>>>(a, B, L);
+    e = cfft_pow2(a, a, scratch, L, st);
+    if (e != cudaSuccess) return e;
+    k_blu_post<<<gM, 256, 0, st>>>(a, out, M, L);
     const long long nthr = M / 2 + 1;
     k_untangle<<<(unsigned) ((nthr + 255) / 256), 256, 0, st>>>(out, n);
     return cudaGetLastError();

@@ -69,6 +69,11 @@ CASES = {
     "datzap": (1 << 18, 16, [dict(r=37.3 * (1 << 18) * DT, z=8.0,
                                   harms=[(0.08, 0.2), (0.08, 1.3), (0.06, 2.1), (0.05, 0.7)])],
                ["-zmax", "60", "-numharm", "4", "-zaplist", "datzap.zaplist"]),
+    # a 2^7 3^3 5^2 7-sample time series (a typical dedispersed length), its
+    # realfft not of a power-of-two length, with two birdies
+    "dat7": (604800, 17, [dict(r=88.8 * 604800 * DT, z=-5.0,
+                               harms=[(0.07, 0.0), (0.05, 1.1), (0.04, 2.0)])],
+             ["-zmax", "40", "-numharm", "2", "-zaplist", "dat7.zaplist"]),
 }
 # inputs other than a seeded .fft: name -> {"dat": True} (the time series is
 # written as <name>.dat) and "zaplist": the text of <name>.zaplist
@@ -76,6 +81,7 @@ INPUTS = {
     "datzap": dict(dat=True, zaplist="# birdies for the .dat zapping case (Hz, width Hz)\n"
                                       "50.0 0.1\n74.6 0.2\nB1234.5 0.05\n2000.0 0.01\n"
                                       "3100.0 4.0\n1.0 0.2\n7811.5 3.0\n"),
+    "dat7": dict(dat=True, zaplist="60.0 0.1\n266.4 0.3\n"),
 }
 
 

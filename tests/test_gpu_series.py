@@ -22,6 +22,49 @@ def test_device_realfft(ctx, oracle, n):
     assert np.max(np.abs(dev - orc)) <= 2e-6 * scale
 
 
+@pytest.mark.parametrize("n", [1026, 67228, 604800, 3888000])
+def test_device_realfft_any_even_length(ctx, oracle, n):
+    """Lengths that are not powers of two (n/2 = 3^3 19, 2 7^5, 2^6 3^3 5^2 7,
+    2^6 3^5 5^3): Bluestein's transform over power-of-two FFTs, against the
+    oracle's FP64 mixed-radix FFT."""
+    x = np.random.default_rng(n + 3).standard_normal(n).astype(np.float32)
+    dev = ctx.realfft(x)
+    orc = oracle.realfft(x)
+    scale = np.max(np.abs(orc))
+    assert np.max(np.abs(dev - orc)) <= 3e-6 * scale, np.max(np.abs(dev - orc)) / scale
+
+
+def test_device_realfft_prime_half_length(ctx):
+    """n/2 = 65537 (prime), against numpy's FP64 transform in the reference's
+    packing (bin 0 = DC, Nyquist)."""
+    n = 2 * 65537
+    x = np.random.default_rng(5).standard_normal(n).astype(np.float32)
+    X = np.fft.rfft(x.astype(np.float64))
+    want = X[:n // 2].copy()
+    want[0] = complex(X[0].real, X[n // 2].real)
+    dev = ctx.realfft(x)
+    assert np.max(np.abs(dev - want)) <= 3e-6 * np.max(np.abs(want))
+
+
+def test_series_search_at_a_dedispersed_length(ctx, ablib, oracle):
+    """A 2^7 3^3 5^2 7-sample series (604800 samples, a typical dedispersed
+    length): the device's series-to-spectrum path and search give the
+    candidates of the oracle's path."""
+    n = 604800
+    series = np.asarray(synth.time_series(n, 77, [dict(r=2100.3, z=6.0, harms=[(0.06, 0.1)] * 2)]),
+                        np.float32)
+    dev = ctx.series_to_fft(series, DT)
+    orc = oracle.deredden(oracle.realfft(series), 6, 200, 0.5 / DT, n * DT)
+    assert np.max(np.abs(dev - orc)) <= 1e-4 * np.max(np.abs(orc))
+    kw = dict(zmax=20, numharm=2)
+    obs = ablib.obs_init(ablib.make_params(n, DT, dev.size, **kw))
+    a = ctx.search(obs, dev)
+    b = ctx.search(obs, orc)
+    assert len(a) == len(b) and len(a) > 0
+    for x, y in zip(a, b):
+        assert x[2] == y[2] and abs(x[3] - y[3]) < 1e-3 and abs(x[4] - y[4]) < 1e-3
+
+
 @pytest.mark.parametrize("numbins", [1 << 11, 1 << 16, 1 << 22])
 def test_device_deredden_bitexact(ctx, oracle, numbins):
     rng = np.random.default_rng(numbins)
