@@ -116,7 +116,15 @@ def test_jerk_hits_near_injection(ctx, oracle, jerk):
 
 
 def test_jerk_hits_mid_spectrum(ctx, oracle, jerk):
-    _window(ctx, oracle, jerk, jerk.nblocks // 2, 8, True)
+    """Noise only: no crossings on either side."""
+    _window(ctx, oracle, jerk, jerk.nblocks // 2, 8, False)
+
+
+def test_jerk_hits_highest_crossings(ctx, oracle, jerk):
+    """The 8 blocks ending at the highest block with a crossing in the whole
+    device search."""
+    top = int(jerk.hits[0].max())
+    _window(ctx, oracle, jerk, max(0, top - 7), 8, True)
 
 
 def test_jerk_key_fields(jerk):
@@ -147,8 +155,17 @@ def test_jerk_planes(ctx, oracle, jerk, nh, hn):
 
 def test_accel_last_blocks(ctx, oracle, accel):
     """The last 16 blocks of the N = 2^23 search (the top of the spectrum, the
-    last superblock groups and batch)."""
-    _window(ctx, oracle, accel, accel.nblocks - 16, 16, True)
+    last superblock groups and batch): noise only, no crossings on either
+    side."""
+    _window(ctx, oracle, accel, accel.nblocks - 16, 16, False)
+
+
+def test_accel_highest_crossings(ctx, oracle, accel):
+    """The 16 blocks ending at the highest block with a crossing in the whole
+    device search (a pulsar harmonic far up the spectrum)."""
+    top = int(accel.hits[0].max())
+    assert top > accel.nblocks // 4
+    _window(ctx, oracle, accel, max(0, top - 15), 16, True)
 
 
 def test_accel_high_block_planes(ctx, oracle, accel):
