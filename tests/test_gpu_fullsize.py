@@ -164,7 +164,6 @@ def test_accel_highest_crossings(ctx, oracle, accel):
     """The 16 blocks ending at the highest block with a crossing in the whole
     device search (a pulsar harmonic far up the spectrum)."""
     top = int(accel.hits[0].max())
-    assert top > accel.nblocks // 4
     _window(ctx, oracle, accel, max(0, top - 15), 16, True)
 
 
