@@ -308,6 +308,9 @@ typedef struct ab_pool ab_pool;
 int  ab_pool_create(int device, int nworkers, size_t hbm_budget, ab_pool **out);
 void ab_pool_destroy(ab_pool *pool);
 const char *ab_pool_last_error(const ab_pool *pool);
+/* The correlation path (AB_CORR_*) of every worker, set while no request is
+ * queued (AB_ERR_STATE otherwise). */
+int  ab_pool_set_corr_path(ab_pool *pool, int path);
 int  ab_pool_submit(ab_pool *pool, const ab_params *p, const ab_fcomplex *fft, long long *ticket);
 int  ab_pool_wait(ab_pool *pool, long long ticket, ab_cand *out, long long maxout,
                   long long *numcands, double *latency_ms);

@@ -39,6 +39,7 @@ EXPORTS = [
     "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
     "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog", "ab_ffdot_hits",
     "ab_read_zaplist", "ab_zapbirds", "ab_zapbirds_host", "ab_mt19937_output",
+    "ab_pool_set_corr_path",
 ]
 
 COST_SLOTS = 16
@@ -219,6 +220,7 @@ def lib():
     L.ab_pool_wait.argtypes = [vp, ll, C.POINTER(Cand), ll, C.POINTER(ll), C.POINTER(d)]
     L.ab_pool_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
     L.ab_pool_reset_stats.argtypes = [vp]
+    L.ab_pool_set_corr_path.argtypes = [vp, i]
     L.ab_fderivs_vol_noalloc.argtypes = [C.POINTER(Obs), i, i, d, vp, vp, C.c_size_t, vp,
                                          C.c_size_t, vp, C.POINTER(FFDotPows)]
     L.ab_ctx_launch_count.restype = ll

@@ -181,6 +181,21 @@ void ab_pool_destroy(ab_pool *p)
 
 const char *ab_pool_last_error(const ab_pool *p) { return p ? p->err.c_str() : "no pool"; }
 
+int ab_pool_set_corr_path(ab_pool *p, int path)
+{
+    if (!p) return AB_ERR_ARG;
+    std::lock_guard<std::mutex> lk(p->mu);
+    if (!p->queue.empty()) {
+        p->err = "the correlation path is set before requests are submitted";
+        return AB_ERR_STATE;
+    }
+    for (auto *c : p->ctxs) {
+        int rc = ab_ctx_set_corr_path(c, path);
+        if (rc) return rc;
+    }
+    return AB_OK;
+}
+
 int ab_pool_submit(ab_pool *p, const ab_params *params, const ab_fcomplex *fft, long long *ticket)
 {
     if (!p || !params || !fft || !ticket) return AB_ERR_ARG;

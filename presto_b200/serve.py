@@ -22,6 +22,11 @@ class SearchPool:
             raise AccelError(f"ab_pool_create: {ERRORS.get(rc, rc)}")
         self.nworkers = nworkers
 
+    def set_corr_path(self, path):
+        """accel.CORR_FFT or accel.CORR_TC_SPLIT_BF16 for every worker (before
+        any submit)."""
+        self._check(self.L.ab_pool_set_corr_path(self.ptr, int(path)), "ab_pool_set_corr_path")
+
     def _check(self, rc, what):
         if rc:
             msg = self.L.ab_pool_last_error(self.ptr)
