@@ -266,9 +266,8 @@ int ab_bank_kernel(ab_ctx *ctx, const ab_obs *obs, int numharm, int harmnum, int
  * Inputs and outputs are device pointers owned by the caller: d_fft holds
  * obs->numbins bins; d_templates the bank of harmonic harmnum/numharm as
  * [numkern_wdim][numkern_zdim][L] FFT'd templates (L and the dimensions from
- * ab_bank_geometry, each template as ab_bank_kernel returns it) in a 16-byte
- * aligned buffer of templates_capacity complex values (AB_ERR_ARG when the
- * bank needs more,
+ * ab_bank_geometry, each template as ab_bank_kernel returns it) in a buffer
+ * of templates_capacity complex values (AB_ERR_ARG when the bank needs more,
  * e.g. after ab_set_transform_costs or ab_autotune changed L); d_powers
  * receives powers[numws][numzs][numrs] (capacity in floats, else
  * AB_ERR_OVERFLOW).  The block starts at fullrlo and ends at

@@ -23,7 +23,6 @@
 #include "ab_norm.cuh"
 #include "ab_resp.cuh"
 #include "ab_select.cuh"
-#include "ab_tc.cuh"
 
 namespace ab {
 
@@ -509,20 +508,8 @@ cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host
 // (b) correlation
 // ======================================================================
 // Correlation of one (block, bank) data spectrum with a tile of templates:
-// the data spectrum is staged in shared memory once; the templates of each
-// iteration (G transforms, G * L points, contiguous) come from L2 by one
-// bulk copy into shared memory, issued while the previous iteration's
-// transforms run, so the FFTs do not wait on L2 latency.
-template <int L> struct CorrSmem {
-    using SH = FftShape<L>;
-    static constexpr size_t XS = L / 2;                  // data spectrum
-    static constexpr size_t EX = SH::G * SH::SMEM;       // one exchange buffer set
-    static constexpr size_t CMAP = L / 8;                // L bytes, in float2 units
-    static constexpr size_t TB = SH::G * L;              // template buffer
-    static constexpr size_t BYTES = (XS + EX + CMAP + TB) * sizeof(float2);
-    static_assert((XS + EX + CMAP) % 2 == 0, "template buffer 16-byte aligned");
-};
-
+// the data spectrum is staged in shared memory once, templates stream from
+// L2 (each template row is read by every block of the batch).
 template <int L>
 __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
                                               const CorrItem *items, const float2 *xhat,
@@ -531,37 +518,22 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
                                               float *fullplane)
 {
     using SH = FftShape<L>;
-    using SM = CorrSmem<L>;
-    extern __shared__ __align__(16) float2 fsm[];
+    extern __shared__ float2 fsm[];
     __shared__ long long s_off[AB_MAX_SBM];
     __shared__ float s_scale[AB_MAX_SBM];
     __shared__ int s_c0[AB_MAX_SBM], s_lim[AB_MAX_SBM];
-    __shared__ __align__(8) uint64_t s_tbar;
     float2 *xs = fsm;                                   // [L/2]
     const CorrItem it = items[blockIdx.x];              // it.bi: transform unit
     const ab_bank b = banks[it.bank];
     const int grp = threadIdx.x / SH::NT, t = threadIdx.x - grp * SH::NT;
-    // one exchange buffer per transform group
-    float2 *sm = fsm + SM::XS + grp * SH::SMEM;
+    // exchange buffers: one per transform group, a second set where the
+    // transform has exactly two exchanges (fewer barriers)
+    constexpr int NBUF = SH::DBUF ? 2 : 1;
+    float2 *sm = fsm + L / 2 + grp * SH::SMEM;
+    float2 *sm2 = SH::DBUF ? fsm + L / 2 + (SH::G + grp) * SH::SMEM : nullptr;
     // column -> block map of a superblock: low / high nibble = first / second
     // block whose sub-plane holds the column (15 = none)
-    unsigned char *cmap = reinterpret_cast<unsigned char *>(fsm + SM::XS + SM::EX);
-    float2 *tbuf = fsm + SM::XS + SM::EX + SM::CMAP;    // this iteration's templates
-    const float2 *tsrc = tmpl + b.tmpl_off;
-    const int iters = (it.nt + SH::G - 1) / SH::G;
-    // templates of iteration k into tbuf (one thread; completes on s_tbar)
-    auto fetch = [&](int k) {
-        const int t0 = it.t0 + k * SH::G;
-        const int cnt = min(SH::G, it.t0 + it.nt - t0);
-        const uint32_t bytes = (uint32_t) (cnt * L * sizeof(float2));
-        tc::fence_smem_async();               // earlier reads of tbuf before the async write
-        tc::mbar_expect_tx(&s_tbar, bytes);
-        tc::bulk_g2s(tbuf, tsrc + (long long) t0 * L, bytes, &s_tbar);
-    };
-    if (threadIdx.x == 0) {
-        tc::mbar_init(&s_tbar, 1);
-        if (iters > 0) fetch(0);
-    }
+    unsigned char *cmap = reinterpret_cast<unsigned char *>(fsm + L / 2 + NBUF * SH::G * SH::SMEM);
     const float2 *xsrc = xhat + (long long) it.bi * xhat_per_block + b.xhat_off;
     for (int i = threadIdx.x; i < L / 2; i += blockDim.x) xs[i] = xsrc[i];
     const bool sb = !sc.inmem && sc.superblocks && b.sbm > 1;
@@ -599,33 +571,23 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
     FftTw<L, 1> tw;                                     // twiddle bases in registers
     tw.init(t);
     __syncthreads();
-    int kfail = -1;                                     // iteration whose copy timed out
+    const int iters = (it.nt + SH::G - 1) / SH::G;
     for (int k = 0; k < iters; k++) {
         const int tl = it.t0 + k * SH::G + grp;
         const bool valid = tl < it.t0 + it.nt;
-        // bounded wait; on a timeout the error word is set (the search
-        // reports AB_ERR_CUDA and its planes are discarded)
-        const bool landed = tc::mbar_wait(&s_tbar, (uint32_t) (k & 1), sc.err, 64u);
         float2 v[16];
         if (valid) {
-            const float2 *kp = tbuf + grp * L;
+            const float2 *kp = tmpl + b.tmpl_off + (long long) tl * L;
 #pragma unroll
             for (int m = 0; m < 16; m++) {
                 int i = t + SH::NT * m;
-                v[m] = cmulc(xs[i & (L / 2 - 1)], kp[i]);
+                v[m] = cmulc(xs[i & (L / 2 - 1)], __ldg(kp + i));
             }
         } else {
 #pragma unroll
             for (int m = 0; m < 16; m++) v[m] = make_float2(0.f, 0.f);
         }
-        // every read of tbuf is done; the CTA stops, uniformly, at a copy
-        // that did not land (no further copy is issued over it)
-        if (!__syncthreads_and(landed)) {
-            kfail = k;
-            break;
-        }
-        if (threadIdx.x == 0 && k + 1 < iters) fetch(k + 1);
-        fft_run<L, 1>(v, sm, t, tw);
+        fft_run<L, 1>(v, sm, t, tw, sm2);
         if (valid && sb) {
             const long long row = (long long) tl * b.numrs_max;
 #pragma unroll
@@ -663,9 +625,6 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
             }
         }
     }
-    // a copy whose wait ran out may still be landing in shared memory: wait
-    // for it (bounded again) before the CTA's shared memory is released
-    if (kfail >= 0) tc::mbar_wait(&s_tbar, (uint32_t) (kfail & 1), sc.err, 64u);
 }
 
 cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
@@ -678,11 +637,11 @@ cudaError_t launch_corr(int L, const ab_bank *banks_dev, const SearchConsts &sc,
     switch (L) {
 #define AB_CORR_CASE(N)                                                                       \
     case N: {                                                                                 \
-        const size_t smem = CorrSmem<N>::BYTES;                                               \
-        if (smem > 200 * 1024) return cudaErrorInvalidValue;                                  \
+        using SH = FftShape<N>;                                                               \
+        const size_t smem = (size_t) (N / 2 + (SH::DBUF ? 2 : 1) * SH::G * SH::SMEM) *      \
+                            sizeof(float2) + (size_t) N;                                     \
         cudaFuncSetAttribute(k_corr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
-        k_corr<N><<<nitems, FftShape<N>::CTA, smem, st>>>(banks_dev, sc, bb, items, xhat,     \
-                                                          xhat_per_block, \
+        k_corr<N><<<nitems, SH::CTA, smem, st>>>(banks_dev, sc, bb, items, xhat, xhat_per_block, \
                                                  tmpl, planes, plane_per_block, fullplane);   \
         break;                                                                                \
     }

@@ -11,7 +11,6 @@
 // in a file-scope static device array instead of context memory.
 #include <cuda_runtime.h>
 
-#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -124,8 +123,6 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
                                       ab_ffdotpows *meta_out)
 {
     if (!obs || !d_fft || !d_templates || !d_powers) return AB_ERR_ARG;
-    // the correlation streams templates by bulk copies from 16-byte boundaries
-    if (reinterpret_cast<uintptr_t>(d_templates) % 16) return AB_ERR_ARG;
     // a CUDA error left pending by the caller's own work stays the caller's:
     // nothing is launched, so no error check below can consume it
     if (cudaPeekAtLastError() != cudaSuccess) return AB_ERR_STATE;
