@@ -276,9 +276,9 @@ def run_ours(args):
     w = WORKLOADS[name]
     fft = make_spectrum(name, seed_offset=rank)
     ctx = pb.Context(local)
-    tc = args.corr == "tc"
+    tc = args.corr in ("tc", "tc16")
     if tc:
-        ctx.set_corr_path(pb.CORR_TC_SPLIT_BF16)
+        ctx.set_corr_path(pb.CORR_TC_SPLIT_BF16 if args.corr == "tc" else pb.CORR_TC_SPLIT_FP16)
     if args.scratch_mb:
         ctx.L.ab_ctx_set_hbm_budget(ctx.ptr, int(args.scratch_mb) * 4 << 20)
     obs = pb.obs_init(pb.make_params(w["N"], w["dt"], fft.size, zmax=w["zmax"], wmax=w["wmax"],
@@ -401,7 +401,8 @@ def run_ours(args):
         src = "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
         if bf16 is None:
             bf16, src = 1400.0, "fallback sustained BF16 1.4 PFLOP/s (of fallback)"
-        roof = {"bound": "tensor", "kernel": "k_corr_tc (split-BF16 banded contraction)",
+        roof = {"bound": "tensor", "kernel": "k_corr_tc (split-%s banded contraction)"
+                % ("BF16" if args.corr == "tc" else "FP16"),
                 "achieved": tflops, "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16,
                 "traffic": None, "flops_per_search": counts["tc_flops"],
                 "kernel_ms_per_search": corr_ms_per_search, "peak_source": src}
@@ -424,10 +425,11 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16 hi+lo products, f32 accumulate" if tc else "f32",
+            "dtype": ("bf16" if args.corr == "tc" else "fp16") + " hi+lo products, f32 accumulate"
+                     if tc else "f32",
             "data": "synthetic",
             "config": config_dict(name, counts["blocks"], counts["cells"]),
-            "corr": "tc_split_bf16" if tc else "fft_f32",
+            "corr": {"fft": "fft_f32", "tc": "tc_split_bf16", "tc16": "tc_split_fp16"}[args.corr],
             "searches_per_s": value / counts["cells"],
             "candidates_per_search": ncands,
             "gpu_launches": int(launches),
@@ -476,8 +478,10 @@ def run_ours(args):
         line["batched"] = [pool_compare("batched", args.requests, workers=args.workers),
                            pool_compare("batched", args.requests, workers=args.workers,
                                         corr="tc")]
-        line["served"] = pool_compare("served", 2 * args.requests, rate=args.rate,
-                                      workers=args.workers)
+        line["served"] = [pool_compare("served", 2 * args.requests, rate=args.rate,
+                                       workers=args.workers),
+                          pool_compare("served", 2 * args.requests, rate=args.rate,
+                                       workers=args.workers, corr="tc16")]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -563,9 +567,10 @@ def pool_compare(mode, nreq, rate=2000.0, workers=4, corr="fft"):
     ffts = [cache.get(r["N"], r["inject"], rng) for r in reqs]
     obss = [pb.obs_init(pb.make_params(r["N"], dt, f.size, **r["opts"])) for r, f in zip(reqs, ffts)]
     cells = sum(pb.algorithmic_counts(o)["cells"] for o in obss)
+    paths = {"tc": pb.CORR_TC_SPLIT_BF16, "tc16": pb.CORR_TC_SPLIT_FP16}
     ctx = pb.Context(0)
-    if corr == "tc":
-        ctx.set_corr_path(pb.CORR_TC_SPLIT_BF16)
+    if corr in paths:
+        ctx.set_corr_path(paths[corr])
     seen = set()
     t0 = time.perf_counter()
     for r, o in zip(reqs, obss):
@@ -586,8 +591,8 @@ def pool_compare(mode, nreq, rate=2000.0, workers=4, corr="fft"):
     ctx.close()
     busy = sum(kms[:4]) / 1e3 / t_plain
     pool = serve.SearchPool(0, nworkers=workers)
-    if corr == "tc":
-        pool.set_corr_path(pb.CORR_TC_SPLIT_BF16)
+    if corr in paths:
+        pool.set_corr_path(paths[corr])
     for r, f in zip(reqs[:workers], ffts[:workers]):          # warm-up
         pool.wait(pool.submit(f, r["N"], dt, **r["opts"]))
     pool.reset_stats()
@@ -608,7 +613,7 @@ def pool_compare(mode, nreq, rate=2000.0, workers=4, corr="fft"):
               f"cfg5 (served stream: Poisson arrivals at {rate:g}/s, N log-uniform 2^19..2^23, "
               "zmax 0/100/300/600, wmax 0/0/0/200, numharm 4/8/16)")
     return {"mode": mode, "recipe": recipe, "requests": len(reqs), "workers": workers,
-            "corr": "tc_split_bf16" if corr == "tc" else "fft_f32",
+            "corr": {"fft": "fft_f32", "tc": "tc_split_bf16", "tc16": "tc_split_fp16"}[corr],
             "searches_per_s": len(reqs) / t_pool,
             "plain_searches_per_s": len(reqs) / t_plain,
             "speedup_vs_plain": t_plain / t_pool,
@@ -641,8 +646,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scratch-mb", type=int, default=0,
                     help="cap the engine's block scratch (profiling runs)")
-    ap.add_argument("--corr", choices=["fft", "tc"], default="fft",
-                    help="correlation path: FP32 FFTs, or the split-BF16 tensor-core contraction")
+    ap.add_argument("--corr", choices=["fft", "tc", "tc16"], default="fft",
+                    help="correlation path: FP32 FFTs, or the tensor-core contraction with "
+                         "split-BF16 (tc) or split-FP16 (tc16) operands")
     ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
                     help="batched/served: the request pool vs the plain path (one GPU)")
     ap.add_argument("--requests", type=int, default=64)

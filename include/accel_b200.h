@@ -116,10 +116,15 @@ int  ab_ctx_set_hbm_budget(ab_ctx *ctx, size_t bytes);
  *                          multiply and power (default);
  *   AB_CORR_TC_SPLIT_BF16  the banded template product as a complex
  *                          contraction on the tensor cores, operands split
- *                          into BF16 hi + lo parts, FP32 accumulation.
+ *                          into BF16 hi + lo parts, FP32 accumulation;
+ *   AB_CORR_TC_SPLIT_FP16  the same with FP16 hi + lo parts (11 significant
+ *                          bits each instead of 8: ~2^-22 relative products;
+ *                          normalised amplitudes must stay below 65504, i.e.
+ *                          powers below ~4e9 times the block's noise level).
  * The reference has no counterpart (it has one path). */
 #define AB_CORR_FFT            0
 #define AB_CORR_TC_SPLIT_BF16  1
+#define AB_CORR_TC_SPLIT_FP16  2
 int  ab_ctx_set_corr_path(ab_ctx *ctx, int path);
 
 /* Transform schedule (no counterpart in the reference, whose FFT length per

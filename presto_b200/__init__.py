@@ -4,7 +4,7 @@ a drop-in for the hot path of PRESTO's accelsearch.
 The compute lives in libaccel_b200.so (CUDA for sm_100a + host C) behind the
 C ABI in include/accel_b200.h; this package is its Python host mirror.
 """
-from .accel import (CORR_FFT, CORR_TC_SPLIT_BF16, AccelError, AccelSearch, CandList,  # noqa: F401
+from .accel import (CORR_FFT, CORR_TC_SPLIT_BF16, CORR_TC_SPLIT_FP16, AccelError, AccelSearch, CandList,  # noqa: F401
                     Context, algorithmic_counts,
                     bank_geometry, candidate_sigma, eliminate_harmonics, lib, make_params,
                     get_fourier_amplitudes, get_transform_costs, num_blocks, obs_init,

@@ -47,6 +47,7 @@ COST_SLOTS = 16
 # correlation paths (ab_ctx_set_corr_path)
 CORR_FFT = 0
 CORR_TC_SPLIT_BF16 = 1
+CORR_TC_SPLIT_FP16 = 2
 
 
 POLISH_MAX_HARM = 32
@@ -693,8 +694,9 @@ class Context:
         return list(c)
 
     def set_corr_path(self, path):
-        """CORR_FFT (FP32 FFT correlation, default) or CORR_TC_SPLIT_BF16
-        (tensor-core banded contraction, split BF16 operands)."""
+        """CORR_FFT (FP32 FFT correlation, default), CORR_TC_SPLIT_BF16 or
+        CORR_TC_SPLIT_FP16 (tensor-core banded contraction, split BF16 or FP16
+        operands)."""
         self._check(self.L.ab_ctx_set_corr_path(self.ptr, int(path)), "ab_ctx_set_corr_path")
 
     # ---- timing -------------------------------------------------------------

@@ -70,12 +70,14 @@ struct ab_ctx {
     // operands of the tensor-core correlation for one bank set: templates
     // sorted by half-width into tiles, packed split-BF16 taps per tile
     struct TcBank {
-        bool ready = false;
+        bool ready = false;                 // tiles and permutation
         std::vector<TcTile> tiles;          // bank-major
         std::vector<int> tile_lo;           // first tile of each bank, nbanks + 1 entries
         DevBuf<TcTile> dtiles;
         DevBuf<int> dperm;
-        DevBuf<unsigned char> pack;
+        DevBuf<unsigned char> pack[2];      // packed operands: split BF16, split FP16
+        bool pack_ready[2] = {false, false};
+        long long pack_bytes = 0;
         int nks_max = 0;
     };
     struct BankEntry {
@@ -220,7 +222,8 @@ static void free_entry(ab_ctx::BankEntry *e)
     e->tmpl.release();
     e->tc.dtiles.release();
     e->tc.dperm.release();
-    e->tc.pack.release();
+    e->tc.pack[0].release();
+    e->tc.pack[1].release();
     if (e->ready) cudaEventDestroy(e->ready);
     delete e;
 }
@@ -279,7 +282,8 @@ static int ensure_banks(ab_ctx *ctx, const ab_obs *obs)
             sb.entries.push_back(hit);
         }
         hit->bs.nbanks = 0;
-        hit->tc.ready = false;
+        hit->tc.ready = false;                  // a reused entry's operands are stale
+        hit->tc.pack_ready[0] = hit->tc.pack_ready[1] = false;
         if (!hit->ready) CK(cudaEventCreateWithFlags(&hit->ready, cudaEventDisableTiming));
         CK(hit->tmpl.ensure((size_t) nb.tmpl_total));
         for (int i = 0; i < nb.nbanks; i++) {
@@ -401,20 +405,21 @@ static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
 // Tiles of the current bank set: per bank, templates sorted by half-width
 // (widest first, then by index) in groups of TC_TILE_T, each covering the taps
 // [hw0 - hwmax, hw0 + hwmax) of its widest member rounded out to 8; then the
-// raw responses and the packed split-BF16 operand, built once per bank set.
-static int ensure_tc(ab_ctx *ctx)
+// raw responses and the packed split operand (BF16 or FP16), built once per
+// bank set and format.
+static int tc_fmt(const ab_ctx *ctx) { return ctx->corr_path == AB_CORR_TC_SPLIT_FP16 ? 1 : 0; }
+
+// Tiles and template permutation of the current bank set (shared by both
+// 16-bit formats); the caller holds the bank lock.
+static int ensure_tc_tiles(ab_ctx *ctx, ab_ctx::TcBank &tb)
 {
-    // the operands live in the shared bank entry: built once, under its lock
-    std::lock_guard<std::mutex> lock(g_banks[ctx->device].mu);
-    ab_ctx::TcBank &tb = ctx->cur_bank->tc;
     if (tb.ready) return AB_OK;
-    if (int rc0 = ensure_tw64(ctx)) return rc0;
     const ab_bankset &bs = ctx->bs;
     tb.tiles.clear();
     tb.tile_lo.assign(1, 0);
     std::vector<int> perm;
     long long off = 0;
-    int nks_max = 0, stride_max = 0;
+    int nks_max = 0;
     for (int k = 0; k < bs.nbanks; k++) {
         const ab_bank &b = bs.b[k];
         std::vector<int> hw(b.ntmpl), order(b.ntmpl);
@@ -442,20 +447,41 @@ static int ensure_tc(ab_ctx *ctx)
             tb.tiles.push_back(t);
         }
         tb.tile_lo.push_back((int) tb.tiles.size());
-        stride_max = std::max(stride_max, 4 * b.hw0);
     }
     if (tc_corr_smem(nks_max) > 227 * 1024)
         return fail(ctx, AB_ERR_ARG, "template responses too wide for the tensor-core path");
     CK(tb.dtiles.ensure(tb.tiles.size()));
     CK(tb.dperm.ensure(perm.size()));
-    CK(tb.pack.ensure((size_t) off));
     CK(cudaMemcpyAsync(tb.dtiles.p, tb.tiles.data(), sizeof(TcTile) * tb.tiles.size(),
                        cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(tb.dperm.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));           // perm is a host vector
+    tb.pack_bytes = off;
+    tb.nks_max = nks_max;
+    tb.ready = true;
+    return AB_OK;
+}
+
+// The raw responses and the packed operand of the context's 16-bit format,
+// built once per bank set and format.
+static int ensure_tc(ab_ctx *ctx)
+{
+    // the operands live in the shared bank entry: built under its lock
+    std::lock_guard<std::mutex> lock(g_banks[ctx->device].mu);
+    ab_ctx::TcBank &tb = ctx->cur_bank->tc;
+    const int fmt = tc_fmt(ctx);
+    if (tb.ready && tb.pack_ready[fmt]) return AB_OK;
+    if (int rc0 = ensure_tw64(ctx)) return rc0;
+    if (int rc0 = ensure_tc_tiles(ctx, tb)) return rc0;
+    const ab_bankset &bs = ctx->bs;
+    CK(tb.pack[fmt].ensure((size_t) tb.pack_bytes));
     DevBuf<float2> raw;
-    int ntmax = 0;
-    for (int k = 0; k < bs.nbanks; k++) ntmax = std::max(ntmax, bs.b[k].ntmpl);
+    int ntmax = 0, stride_max = 0;
+    for (int k = 0; k < bs.nbanks; k++) {
+        ntmax = std::max(ntmax, bs.b[k].ntmpl);
+        stride_max = std::max(stride_max, 4 * bs.b[k].hw0);
+    }
     CK(raw.ensure((size_t) ntmax * stride_max));
     int rc = AB_OK;
     for (int k = 0; k < bs.nbanks && rc == AB_OK; k++) {
@@ -467,7 +493,7 @@ static int ensure_tc(ab_ctx *ctx)
         cudaError_t e = launch_tc_raw(&b, 4 * b.hw0, raw.p, ctx->tw64.p, kTwLog2, ctx->stream);
         if (e == cudaSuccess)
             e = launch_tc_pack(&b, tb.dtiles.p + lo, nt, nks_k, tb.dperm.p, raw.p, 4 * b.hw0,
-                               tb.pack.p, ctx->stream);
+                               tb.pack[fmt].p, fmt, ctx->stream);
         tick(ctx, 0, false);
         ctx->launches += 2;
         if (e != cudaSuccess)
@@ -478,8 +504,7 @@ static int ensure_tc(ab_ctx *ctx)
     if (rc) return rc;
     if (e != cudaSuccess)
         return fail(ctx, AB_ERR_CUDA, "tensor-core operand packing failed: %s", cudaGetErrorString(e));
-    tb.nks_max = nks_max;
-    tb.ready = true;
+    tb.pack_ready[fmt] = true;
     return AB_OK;
 }
 
@@ -517,9 +542,10 @@ static int run_tc(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, con
     ctx->launches++;
     if (e != cudaSuccess) return fail(ctx, AB_ERR_CUDA, "data preparation failed: %s", cudaGetErrorString(e));
     tick(ctx, 2, true);
+    const int fmt = tc_fmt(ctx);
     e = launch_corr_tc(ctx->dbanks.p, sc, bb, ditems, nitems, tb.dtiles.p, tb.dperm.p, ctx->dtime.p,
-                       ctx->bs.dtime_per_block, tb.pack.p, tb.nks_max, planes, ppb, fullplane,
-                       ctx->stream);
+                       ctx->bs.dtime_per_block, tb.pack[fmt].p, tb.nks_max, planes, ppb, fullplane,
+                       fmt, ctx->stream);
     tick(ctx, 2, false);
     ctx->launches++;
     if (e != cudaSuccess)
@@ -744,7 +770,7 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
         if (first_col > 0)
             CK(cudaMemset2DAsync(ctx->fullplane.p, sizeof(float) * sc.rlen, 0,
                                  sizeof(float) * first_col, sc.numz, ctx->stream));
-        const bool tcp = ctx->corr_path == AB_CORR_TC_SPLIT_BF16;
+        const bool tcp = ctx->corr_path != AB_CORR_FFT;
         if (tcp) {
             rc = ensure_tc(ctx);
             if (rc) return rc;
@@ -839,7 +865,7 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
     // standard mode: batches of blocks, each correlated for every bank, then
     // summed; hit sets rotate so the host replays batch k - (kHitSets - 1)
     // meanwhile
-    const bool tcp = ctx->corr_path == AB_CORR_TC_SPLIT_BF16;
+    const bool tcp = ctx->corr_path != AB_CORR_FFT;
     if (tcp) {
         rc = ensure_tc(ctx);
         if (rc) return rc;
@@ -1412,7 +1438,9 @@ int ab_zapbirds(ab_ctx *ctx, ab_fcomplex *fft, int fft_on_device, long long numb
 
 int ab_ctx_set_corr_path(ab_ctx *ctx, int path)
 {
-    if (!ctx || (path != AB_CORR_FFT && path != AB_CORR_TC_SPLIT_BF16)) return AB_ERR_ARG;
+    if (!ctx || (path != AB_CORR_FFT && path != AB_CORR_TC_SPLIT_BF16 &&
+                 path != AB_CORR_TC_SPLIT_FP16))
+        return AB_ERR_ARG;
     ctx->corr_path = path;
     return AB_OK;
 }
@@ -1628,7 +1656,7 @@ int ab_subharm_fderivs_vol(ab_ctx *ctx, const ab_obs *obs, int numharm, int harm
     CK(cudaMemcpyAsync(ctx->startr.p, &fullrlo, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(ctx->planes.ensure((size_t) ctx->bs.plane_per_block));
     BlockBatch bb{ctx->startr.p, 0, 1, 0};
-    if (ctx->corr_path == AB_CORR_TC_SPLIT_BF16) {
+    if (ctx->corr_path != AB_CORR_FFT) {
         rc = ensure_tc(ctx);
         if (rc) return rc;
         CK(ctx->dtime.ensure((size_t) ctx->bs.dtime_per_block));

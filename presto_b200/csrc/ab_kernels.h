@@ -101,7 +101,7 @@ cudaError_t launch_tc_gemm(const float *A, const float *B, float *C, int N, int 
                            unsigned *err, cudaStream_t st);
 
 // kernel set (b'), tensor-core correlation: the banded template product as a
-// complex contraction in split BF16 (hi + lo) with FP32 accumulation.
+// complex contraction in split BF16 or FP16 (hi + lo) with FP32 accumulation.
 constexpr int TC_TILE_T = 128;          // templates per tile (MMA N = 2 per template)
 constexpr int TC_ATILE = 128;           // output positions per accumulator (MMA M)
 constexpr int TC_ACC = 1;               // accumulators (128 x 256 FP32, 256 TMEM columns) per CTA
@@ -122,7 +122,7 @@ cudaError_t launch_tc_raw(const ab_bank *b, int stride, float2 *out, const doubl
                           int max_log2, cudaStream_t st);
 cudaError_t launch_tc_pack(const ab_bank *b, const TcTile *tiles_dev, int ntiles, int nks_max,
                            const int *perm_dev, const float2 *raw, int stride,
-                           unsigned char *pack, cudaStream_t st);
+                           unsigned char *pack, int fp16, cudaStream_t st);
 cudaError_t launch_prep_time(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
                              const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
                              float2 *dtime, long long dt_per_block, cudaStream_t st);
@@ -130,7 +130,7 @@ cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, con
                            const TcItem *items, int nitems, const TcTile *tiles, const int *perm,
                            const float2 *dtime, long long dt_per_block, const unsigned char *pack,
                            int nks_max, float *planes, long long plane_per_block, float *fullplane,
-                           cudaStream_t st);
+                           int fp16, cudaStream_t st);
 size_t tc_corr_smem(int nks_max);
 
 // candidate polishing (optimize_accelcand for acceleration searches)

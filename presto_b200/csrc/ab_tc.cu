@@ -15,9 +15,13 @@
 // c in [0, 2 hw0), d the normalised block data and resp_t the template's
 // 4 hw_t response points (zero outside).  Per parity this is a real GEMM:
 // M = output positions a, N = (re, im) rows of each template, K = taps with
-// re/im interleaved.  Operands are split into BF16 hi + lo parts and the
-// products hi.hi + hi.lo + lo.hi are accumulated in FP32 in tensor memory.
+// re/im interleaved.  Operands are split into 16-bit hi + lo parts -- BF16
+// (8 significant bits each, FP32's exponent range) or FP16 (11 bits each, so
+// about 2^-22 instead of 2^-16 relative, for operands below 65504 in
+// magnitude) -- and the products hi.hi + hi.lo + lo.hi are accumulated in
+// FP32 in tensor memory.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "ab_index.h"
@@ -30,6 +34,22 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bflo
 {
     hi = __float2bfloat16_rn(x);
     lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// hi + lo 16-bit parts of x as raw bits: BF16 (F16 = false) or FP16
+template <bool F16> __device__ __forceinline__ void split16(float x, uint16_t &hi, uint16_t &lo)
+{
+    if constexpr (F16) {
+        const __half h = __float2half_rn(x);
+        const __half l = __float2half_rn(x - __half2float(h));
+        hi = __half_as_ushort(h);
+        lo = __half_as_ushort(l);
+    } else {
+        __nv_bfloat16 h, l;
+        split_bf16(x, h, l);
+        hi = __bfloat16_as_ushort(h);
+        lo = __bfloat16_as_ushort(l);
+    }
 }
 
 // 128 threads.  A: [128][K], B: [N][K] row-major FP32 in global memory,
@@ -125,6 +145,7 @@ __device__ __forceinline__ uint32_t kstep_off(int row, int k)
 // row) x 16 bf16 (taps c_lo + 8 s + k / 2, re and im interleaved), hi part
 // then lo part.  Rows re: (Re r, Im r); im: (-Im r, Re r) for the response
 // point r, so that A . B^T gives Re and Im of d * conj(r).
+template <bool F16>
 __global__ void __launch_bounds__(256) k_tc_pack(const ab_bank b, const TcTile *tiles, int nks_max,
                                                  const int *perm, const float2 *raw, int stride,
                                                  unsigned char *pack)
@@ -149,22 +170,25 @@ __global__ void __launch_bounds__(256) k_tc_pack(const ab_bank b, const TcTile *
                 else v = (k & 1) ? r.x : -r.y;
             }
         }
-        __nv_bfloat16 h, l;
-        split_bf16(v, h, l);
+        uint16_t h, l;
+        split16<F16>(v, h, l);
         const uint32_t o = kstep_off(row, k);
-        *reinterpret_cast<__nv_bfloat16 *>(dst + o) = h;
-        *reinterpret_cast<__nv_bfloat16 *>(dst + 32 * tl.n + o) = l;
+        *reinterpret_cast<uint16_t *>(dst + o) = h;
+        *reinterpret_cast<uint16_t *>(dst + 32 * tl.n + o) = l;
     }
 }
 
 cudaError_t launch_tc_pack(const ab_bank *b, const TcTile *tiles_dev, int ntiles, int nks_max,
                            const int *perm_dev, const float2 *raw, int stride,
-                           unsigned char *pack, cudaStream_t st)
+                           unsigned char *pack, int fp16, cudaStream_t st)
 {
     if (ntiles <= 0) return cudaSuccess;
     if (ntiles > 65535 || nks_max <= 0) return cudaErrorInvalidValue;
     dim3 grid(2 * nks_max, ntiles);
-    k_tc_pack<<<grid, 256, 0, st>>>(*b, tiles_dev, nks_max, perm_dev, raw, stride, pack);
+    if (fp16)
+        k_tc_pack<true><<<grid, 256, 0, st>>>(*b, tiles_dev, nks_max, perm_dev, raw, stride, pack);
+    else
+        k_tc_pack<false><<<grid, 256, 0, st>>>(*b, tiles_dev, nks_max, perm_dev, raw, stride, pack);
     return cudaGetLastError();
 }
 
@@ -202,6 +226,7 @@ struct TcArgs {
 // Hankel matrix: row r holds d[a0 + p + c_lo + r + j], j < 8, so K step s of
 // accumulator u is rows 8 s + 128 u .. + 127, one 8-row group (256 B) further
 // per step.  Every wait is bounded and reports through sc.err.
+template <bool F16>
 __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
 {
     extern __shared__ __align__(1024) unsigned char tsm[];
@@ -248,12 +273,12 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
     for (int e = threadIdx.x; e < nrows * 8; e += blockDim.x) {
         const int r = e >> 3, j = e & 7;
         const float2 v = __ldg(d + (base + r + j) % numdata);
-        __nv_bfloat16 hr, lr, hi_, li;
-        split_bf16(v.x, hr, lr);
-        split_bf16(v.y, hi_, li);
+        uint16_t hr, lr, hi_, li;
+        split16<F16>(v.x, hr, lr);
+        split16<F16>(v.y, hi_, li);
         const uint32_t o = kstep_off(r, 2 * j);
-        *reinterpret_cast<__nv_bfloat162 *>(h_hi + o) = __halves2bfloat162(hr, hi_);
-        *reinterpret_cast<__nv_bfloat162 *>(h_lo + o) = __halves2bfloat162(lr, li);
+        *reinterpret_cast<uint32_t *>(h_hi + o) = (uint32_t) hr | ((uint32_t) hi_ << 16);
+        *reinterpret_cast<uint32_t *>(h_lo + o) = (uint32_t) lr | ((uint32_t) li << 16);
     }
     if (threadIdx.x < 32) tc::tmem_alloc(&s_taddr, 256 * TC_ACC);
     if (threadIdx.x == 0) {
@@ -286,7 +311,7 @@ __global__ void __launch_bounds__(128, 1) k_corr_tc(TcArgs a)
             tc::mbar_wait(&full[q % TC_STAGES], (q / TC_STAGES) & 1, sc.err, 4u);
     } else if (threadIdx.x == 32) {
         // MMA issuer
-        const uint32_t idesc = tc::idesc_bf16_f32(TC_ATILE, tl.n);
+        const uint32_t idesc = F16 ? tc::idesc_f16_f32(TC_ATILE, tl.n) : tc::idesc_bf16_f32(TC_ATILE, tl.n);
         for (int s = 0; s < tl.nks; s++) {
             const int st = s % TC_STAGES;
             if (!tc::mbar_wait(&full[st], (s / TC_STAGES) & 1, sc.err, 4u)) break;
@@ -347,15 +372,20 @@ cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, con
                            const TcItem *items, int nitems, const TcTile *tiles, const int *perm,
                            const float2 *dtime, long long dt_per_block, const unsigned char *pack,
                            int nks_max, float *planes, long long plane_per_block, float *fullplane,
-                           cudaStream_t st)
+                           int fp16, cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
     size_t smem = tc_corr_smem(nks_max);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaFuncSetAttribute(k_corr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     TcArgs a{banks_dev, sc, bb, items, tiles, perm, dtime, dt_per_block, pack, planes,
              plane_per_block, fullplane};
-    k_corr_tc<<<nitems, 128, smem, st>>>(a);
+    if (fp16) {
+        cudaFuncSetAttribute(k_corr_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        k_corr_tc<true><<<nitems, 128, smem, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_corr_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        k_corr_tc<false><<<nitems, 128, smem, st>>>(a);
+    }
     return cudaGetLastError();
 }
 

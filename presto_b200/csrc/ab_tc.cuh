@@ -54,7 +54,16 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N)
          | ((uint32_t) (M >> 4) << 24);
 }
 
-// D[tmem] (+)= A . B^T, issued by one thread.
+// Instruction descriptor: kind::f16 with FP16 A and B (K-major), FP32 D.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N)
+{
+    return (1u << 4)                  // D format F32; A, B format F16 (0)
+         | ((uint32_t) (N >> 3) << 17)
+         | ((uint32_t) (M >> 4) << 24);
+}
+
+// D[tmem] (+)= A . B^T, issued by one thread (kind::f16: A and B both BF16 or
+// both FP16, as the instruction descriptor says).
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate)
 {
