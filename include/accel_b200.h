@@ -453,6 +453,30 @@ int ab_zapbirds_host(ab_fcomplex *fft, long long numbins, long long N, const dou
                      const double *hibins, int numbirds, int *numzapped);
 unsigned int ab_mt19937_output(unsigned long seed, long long k);
 
+/* Subband dedispersion, the producer of accelsearch's DM trials (prepsubband,
+ * src/prepsubband.c:365-450, src/dispersion.c:54-232; no reference
+ * counterpart for the whole-array form: prepsubband streams blocks of the
+ * raw data through the same sums).  data: nspec spectra of nchan channels,
+ * time-major (all channels of a sample together, channel 0 the lowest
+ * frequency lofreq MHz, chanwidth > 0 MHz apart), as floats; dt the sample
+ * time (s).  Channels are summed into nsub subbands with the delays of the
+ * DMs' mean (subband_search_delays, rounded to samples), the subbands are
+ * downsampled by downsamp (averages, prepsubband -downsamp), then each DM
+ * d sums the subbands shifted by its offsets (subband_delays relative to the
+ * top subband, rounded to downsampled samples): out[d][u] for
+ * u < nspec / downsamp, DM-major.  Samples past the end read zero (the
+ * reference's zero-padded last block).  Every output element is summed in
+ * the reference's order, so it is the reference's float result.
+ *   ab_dedisp_delays  the channel delays (nchan ints) and subband offsets
+ *                     (ndm x nsub ints) it uses, host only;
+ *   ab_dedisperse     the dedispersion; *_on_device flags say whether data
+ *                     and out are device pointers. */
+int ab_dedisp_delays(int nchan, double lofreq, double chanwidth, double dt, int nsub,
+                     const double *dms, int ndm, int downsamp, int *chan_delay, int *sub_offset);
+int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long nspec, int nchan,
+                  double lofreq, double chanwidth, double dt, int nsub, const double *dms, int ndm,
+                  int downsamp, float *out, int out_on_device);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);
@@ -467,7 +491,8 @@ int  ab_w_resp_halfwidth(double z, double w);
 /* Kernel timing (CUDA events around each launch on the context stream).
  * kinds: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search (device
  * ms); 4 host work until the last launch is queued, 5 host sort + replay,
- * 6 wait for the device and hit read-back (host wall ms, ab_search only). */
+ * 6 wait for the device and hit read-back (host wall ms, ab_search only),
+ * 7 dedispersion (device ms, ab_dedisperse). */
 int ab_ctx_set_profiling(ab_ctx *ctx, int on);
 int ab_ctx_kernel_times(ab_ctx *ctx, double *ms, long long *launches, int nkinds);
 int ab_ctx_reset_kernel_times(ab_ctx *ctx);

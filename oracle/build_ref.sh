@@ -131,3 +131,16 @@ fi
 $CC -w -I "$HERE/refshim" -I "$REF/include" -o "$OBJ/layout_probe" "$HERE/layout_probe.c"
 "$OBJ/layout_probe" > "$OUT/accel_layout.txt"
 echo "wrote $OUT/accel_layout.txt (the reference's accel.h structure layout)"
+# subband dedispersion (src/dispersion.c: delay_from_dm, dedisp_delays,
+# subband_delays, subband_search_delays, dedisp_subbands, float_dedisp; doppler
+# from src/barycenter.c) for the dedispersion checks
+$CC -O2 -g -fPIC -ffunction-sections -fdata-sections -w -I "$HERE/refshim" -I "$REF/include" \
+    -c "$REF/src/dispersion.c" -o "$OBJ/dispersion.o"
+$CC -O2 -g -fPIC -ffunction-sections -fdata-sections -w -I "$HERE/refshim" -I "$REF/include" \
+    -c "$REF/src/barycenter.c" -o "$OBJ/barycenter.o"
+echo 'REF { global: delay_from_dm; dedisp_delays; subband_delays; subband_search_delays;
+      dedisp_subbands; float_dedisp; vect_free; local: *; };' > "$OUT/dedisp.map"
+$CC -shared -Wl,--gc-sections -Wl,--version-script="$OUT/dedisp.map" -Wl,-z,defs \
+    -o "$OUT/libref_dedisp.so" "$OBJ/dispersion.o" "$OBJ/barycenter.o" $LOBJ $SOBJ \
+    "$OBJ/orc_stats.o" -fopenmp -lm
+echo "built $OUT/libref_dedisp.so (src/dispersion.c)"

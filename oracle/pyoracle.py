@@ -830,3 +830,91 @@ def accelfile_text(T, nph, numw, cands, polished, inf_bytes=b""):
             out.append("  ".join(cells) + "    " + " " * 20 + "\n")
     out.append("\n\n")
     return "".join(out).encode() + inf_bytes
+
+
+def ref_dedisp_lib():
+    """oracle/_ref/libref_dedisp.so (src/dispersion.c compiled unmodified), or
+    None where the reference tree was not at hand."""
+    path = os.path.join(HERE, "_ref", "libref_dedisp.so")
+    if not os.path.exists(path):
+        return None
+    if path not in _libs:
+        L = C.CDLL(path)
+        dp = C.POINTER(C.c_double)
+        for name in ("dedisp_delays", "subband_delays"):
+            getattr(L, name).restype = dp
+        L.dedisp_delays.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.subband_delays.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                     C.c_double]
+        L.subband_search_delays.restype = dp
+        L.subband_search_delays.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                            C.c_double]
+        L.dedisp_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_int, C.c_void_p]
+        L.float_dedisp.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_float, C.c_void_p]
+        L.vect_free.argtypes = [C.c_void_p]
+        _libs[path] = L
+    return _libs[path]
+
+
+def _nearest_long(x):
+    return int(np.ceil(x - 0.5)) if x < 0 else int(np.floor(x + 0.5))
+
+
+def ref_dedisp_delays(L, nchan, lofreq, chanwidth, dt, nsub, dms, ds):
+    """prepsubband's integer delays (src/prepsubband.c:365-390) from the
+    reference's own subband_search_delays / subband_delays."""
+    avgdm = 0.0
+    for d in dms:
+        avgdm += d
+    avgdm /= len(dms)
+    p = L.subband_search_delays(nchan, nsub, avgdm, lofreq, chanwidth, 0.0)
+    cd = np.array([_nearest_long(p[i] / dt) for i in range(nchan)], np.int32)
+    L.vect_free(p)
+    off = np.zeros((len(dms), nsub), np.int32)
+    for i, dm in enumerate(dms):
+        q = L.subband_delays(nchan, nsub, float(dm), lofreq, chanwidth, 0.0)
+        top = q[nsub - 1]
+        off[i] = [_nearest_long((q[j] - top) / (dt * ds)) for j in range(nsub)]
+        L.vect_free(q)
+    return cd, off
+
+
+def ref_dedisperse(L, X, lofreq, chanwidth, dt, nsub, dms, ds, W):
+    """prepsubband's dedispersion over the reference's own dedisp_subbands
+    and float_dedisp, streamed in blocks of W spectra as the program streams
+    them (src/backend_common.c:660-758 prep_subbands; src/prepsubband.c:
+    919-1025 get_data): each stage pairs a block with the next (lastdata,
+    data), the raw blocks transposed to channel-major, the subband blocks
+    back to time-major, downsampled by averaging (float sums, then / ds), the
+    data followed by zero blocks.  X: time-major float32 [nspec][nchan],
+    nspec a multiple of W, W of ds.  Returns out[ndm][nspec // ds]."""
+    nspec, nchan = X.shape
+    nb = nspec // W
+    cd, off = ref_dedisp_delays(L, nchan, lofreq, chanwidth, dt, nsub, dms, ds)
+    zeros = np.zeros((W, nchan), np.float32)
+    raw = [np.ascontiguousarray(X[b * W:(b + 1) * W].T) for b in range(nb)] + \
+        [np.ascontiguousarray(zeros.T)] * 2
+    sub = []                                    # time-major [W][nsub] per block
+    for b in range(nb + 1):
+        res = np.zeros(nsub * W, np.float32)
+        L.dedisp_subbands(raw[b + 1].ctypes.data, raw[b].ctypes.data, W, nchan, cd.ctypes.data,
+                          nsub, res.ctypes.data)
+        s = res.reshape(nsub, W).T.copy()
+        if ds > 1:
+            ftmp = np.zeros((W // ds, nsub), np.float32)
+            for k in range(ds):
+                ftmp = (ftmp + s[k::ds]).astype(np.float32)
+            s = (np.float32(0.0) + ftmp / np.float32(ds)).astype(np.float32)
+        sub.append(np.ascontiguousarray(s))
+    n = W // ds
+    out = np.zeros((len(dms), nb * n), np.float32)
+    res = np.zeros(n, np.float32)
+    for b in range(nb):
+        for i in range(len(dms)):
+            o = np.ascontiguousarray(off[i])
+            L.float_dedisp(sub[b + 1].ctypes.data, sub[b].ctypes.data, n, nsub, o.ctypes.data,
+                           0.0, res.ctypes.data)
+            out[i, b * n:(b + 1) * n] = res
+    return out

@@ -10,4 +10,5 @@ from .accel import (CORR_FFT, CORR_TC_SPLIT_BF16, CORR_TC_SPLIT_FP16, AccelError
                     get_fourier_amplitudes, get_transform_costs, num_blocks, obs_init,
                     power_for_sigma, FourierProps, RzwErrs, calc_props, calc_rzwerrs, cand_props,
                     read_candfile, write_candfile, write_accelfile, accel_filenames, nice_output,
-                    set_transform_costs, sort_cands, read_zaplist, zapbirds_host, mt19937_output)
+                    set_transform_costs, sort_cands, read_zaplist, zapbirds_host, mt19937_output,
+                    dedisp_delays)

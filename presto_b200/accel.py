@@ -39,7 +39,7 @@ EXPORTS = [
     "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
     "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog", "ab_ffdot_hits",
     "ab_read_zaplist", "ab_zapbirds", "ab_zapbirds_host", "ab_mt19937_output",
-    "ab_pool_set_corr_path",
+    "ab_pool_set_corr_path", "ab_dedisp_delays", "ab_dedisperse",
 ]
 
 COST_SLOTS = 16
@@ -185,6 +185,8 @@ def lib():
     L.ab_candlist_get.argtypes = [vp, C.POINTER(Cand), ll]
     L.ab_candlist_insert.argtypes = [vp, C.c_float, C.c_float, i, d, d, d]
     L.ab_search_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, vp]
+    L.ab_dedisp_delays.argtypes = [i, d, d, d, i, vp, i, i, vp, vp]
+    L.ab_dedisperse.argtypes = [vp, vp, i, ll, i, d, d, d, i, vp, i, i, vp, i]
     L.ab_read_zaplist.argtypes = [C.c_char_p, d, d, vp, vp, i, C.POINTER(i)]
     L.ab_zapbirds.argtypes = [vp, vp, i, ll, ll, vp, vp, i, C.POINTER(i)]
     L.ab_zapbirds_host.argtypes = [vp, ll, ll, vp, vp, i, C.POINTER(i)]
@@ -686,6 +688,27 @@ class Context:
         self.last_numzapped = nz.value
         return y
 
+    def dedisperse(self, data, lofreq, chanwidth, dt, nsub, dms, downsamp=1, device_ptr=None,
+                   nspec=None, nchan=None, out_ptr=None):
+        """Subband dedispersion (ab_dedisperse) of time-major float spectra
+        data[nspec][nchan] (channel 0 the lowest frequency); returns
+        out[ndm][nspec // downsamp] (or fills out_ptr with device_ptr input)."""
+        dmv = np.ascontiguousarray(dms, dtype=np.float64)
+        if device_ptr is not None:
+            nout = int(nspec) // downsamp
+            self._check(self.L.ab_dedisperse(self.ptr, C.c_void_p(device_ptr), 1, int(nspec),
+                                             int(nchan), lofreq, chanwidth, dt, nsub,
+                                             dmv.ctypes.data, dmv.size, downsamp,
+                                             C.c_void_p(out_ptr), 1), "ab_dedisperse")
+            return None
+        x = np.ascontiguousarray(data, dtype=np.float32)
+        nspec, nchan = x.shape
+        out = np.zeros((dmv.size, nspec // downsamp), np.float32)
+        self._check(self.L.ab_dedisperse(self.ptr, x.ctypes.data, 0, nspec, nchan, lofreq,
+                                         chanwidth, dt, nsub, dmv.ctypes.data, dmv.size,
+                                         downsamp, out.ctypes.data, 0), "ab_dedisperse")
+        return out
+
     def autotune(self):
         """Measure the correlation cost per transform length on this context's
         device and install it process-wide; returns the table."""
@@ -706,10 +729,11 @@ class Context:
     def kernel_times(self):
         """Per kind: 0 templates, 1 prep, 2 correlation, 3 harmonic sum + search
         (device ms); 4 host setup until the last launch is queued, 5 host sort +
-        replay, 6 wait for the device and hit read-back (host wall ms)."""
-        ms = (C.c_double * 7)()
-        n = (C.c_longlong * 7)()
-        self.L.ab_ctx_kernel_times(self.ptr, ms, n, 7)
+        replay, 6 wait for the device and hit read-back (host wall ms); 7
+        dedispersion (device ms)."""
+        ms = (C.c_double * 8)()
+        n = (C.c_longlong * 8)()
+        self.L.ab_ctx_kernel_times(self.ptr, ms, n, 8)
         return list(ms), list(n)
 
     def reset_kernel_times(self):
@@ -785,6 +809,18 @@ def zapbirds_host(fft, N, lobins, hibins):
 
 def mt19937_output(seed, k):
     return int(lib().ab_mt19937_output(int(seed), int(k)))
+
+
+def dedisp_delays(nchan, lofreq, chanwidth, dt, nsub, dms, downsamp=1):
+    """ab_dedisp_delays: (channel delays [nchan], subband offsets [ndm][nsub])."""
+    dmv = np.ascontiguousarray(dms, dtype=np.float64)
+    cd = np.zeros(nchan, np.int32)
+    off = np.zeros((dmv.size, nsub), np.int32)
+    rc = lib().ab_dedisp_delays(nchan, lofreq, chanwidth, dt, nsub, dmv.ctypes.data, dmv.size,
+                                downsamp, cd.ctypes.data, off.ctypes.data)
+    if rc:
+        raise AccelError(f"ab_dedisp_delays: {ERRORS.get(rc, rc)}")
+    return cd, off
 
 
 def candidate_sigma(power, numsum, numtrials):

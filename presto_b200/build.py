@@ -18,8 +18,8 @@ DROPIN = os.path.join(HERE, "libaccel_dropin.so")
 DROPIN_SRC = "accel_dropin.c"
 BUILD = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu", "ab_pool.cu", "ab_tc.cu", "ab_polish.cu", "ab_polish_rzw.cu", "ab_series.cu"]
-C_SOURCES = ["ab_host.c", "ab_output.c", "ab_zap.c"]
+CU_SOURCES = ["ab_kernels.cu", "ab_engine.cu", "ab_noalloc.cu", "ab_pool.cu", "ab_tc.cu", "ab_polish.cu", "ab_polish_rzw.cu", "ab_series.cu", "ab_dedisp.cu"]
+C_SOURCES = ["ab_host.c", "ab_output.c", "ab_zap.c", "ab_dedisp.c"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 CC_FLAGS = ["-O2", "-g", "-fPIC", "-std=gnu11", "-pthread", "-ffp-contract=off", "-Wall",

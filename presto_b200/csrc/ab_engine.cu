@@ -26,7 +26,8 @@ using namespace ab;
 namespace {
 
 constexpr int kTwLog2 = 14;                 // FP64 twiddle table for FFTs up to 16384
-constexpr int kNumKinds = 7;   // templates, prep, corr, harmsum (device); host setup, host replay, hit fetch
+constexpr int kNumKinds = 8;   // templates, prep, corr, harmsum (device); host setup, host replay,
+                               // hit fetch; dedispersion (device)
 double now_ms()
 {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -93,6 +94,8 @@ struct ab_ctx {
     DevBuf<float2> dtime;                   // normalised block data (tensor-core path)
     DevBuf<float2> ser_in, ser_scr;         // time-series input path
     DevBuf<float2> blu_a, blu_b;            // Bluestein work and chirp-kernel transform
+    DevBuf<float> dd_x, dd_xcm, dd_sub, dd_out; // dedispersion: spectra, channel-major, subbands, DMs
+    DevBuf<int> dd_cd, dd_off;              // dedispersion delays
     long long blu_M = 0;                    // the length blu_b was built for
     DevBuf<int2> dered_blocks;
     DevBuf<float> dered_means;
@@ -142,8 +145,8 @@ struct ab_ctx {
 
     // timing
     bool prof = false;
-    double kms[kNumKinds] = {0, 0, 0, 0, 0, 0, 0};
-    long long kn[kNumKinds] = {0, 0, 0, 0, 0, 0, 0};
+    double kms[kNumKinds] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long kn[kNumKinds] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long launches = 0;
     std::vector<cudaEvent_t> evpool;
     std::vector<std::pair<int, int>> evpending;   // (kind, event index)
@@ -1066,6 +1069,12 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->blu_a.release();
     ctx->blu_b.release();
     ctx->blu_M = 0;
+    ctx->dd_x.release();
+    ctx->dd_xcm.release();
+    ctx->dd_sub.release();
+    ctx->dd_out.release();
+    ctx->dd_cd.release();
+    ctx->dd_off.release();
     ctx->dered_blocks.release();
     ctx->dered_means.release();
     ctx->titems.release();
@@ -1398,6 +1407,56 @@ int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, i
     if (!out_on_device)
         CK(cudaMemcpyAsync(out, dout, sizeof(float2) * (n / 2), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return AB_OK;
+}
+
+int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long nspec, int nchan,
+                  double lofreq, double chanwidth, double dt, int nsub, const double *dms, int ndm,
+                  int downsamp, float *out, int out_on_device)
+{
+    if (!ctx || !data || !out || !dms || nspec < 1 || nchan < 1 || nsub < 1 || ndm < 1 ||
+        downsamp < 1 || nchan % nsub || nsub > 1024)
+        return fail(ctx, AB_ERR_ARG, "dedispersion arguments");
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    const long long nout = nspec / downsamp;
+    if (nout < 1) return fail(ctx, AB_ERR_ARG, "fewer samples than the downsampling factor");
+    std::vector<int> cd((size_t) nchan), off((size_t) ndm * nsub);
+    rc = ab_dedisp_delays(nchan, lofreq, chanwidth, dt, nsub, dms, ndm, downsamp, cd.data(),
+                          off.data());
+    if (rc) return fail(ctx, rc, "dedispersion delays (channels ascending in frequency, "
+                                 "delays below 2^30 samples)");
+    const size_t nx = (size_t) nspec * nchan;
+    CK(ctx->dd_cd.ensure(cd.size()));
+    CK(ctx->dd_off.ensure(off.size()));
+    CK(cudaMemcpyAsync(ctx->dd_cd.p, cd.data(), sizeof(int) * cd.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->dd_off.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    const float *dx = data;
+    if (!data_on_device) {
+        CK(ctx->dd_x.ensure(nx));
+        CK(cudaMemcpyAsync(ctx->dd_x.p, data, sizeof(float) * nx, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        dx = ctx->dd_x.p;
+    }
+    CK(ctx->dd_xcm.ensure(nx));
+    CK(ctx->dd_sub.ensure((size_t) nsub * nout));
+    float *dout = out;
+    if (!out_on_device) {
+        CK(ctx->dd_out.ensure((size_t) ndm * nout));
+        dout = ctx->dd_out.p;
+    }
+    tick(ctx, 7, true);
+    CK(launch_dedisp(dx, ctx->dd_xcm.p, nspec, nchan, ctx->dd_cd.p, nsub, downsamp, ctx->dd_off.p,
+                     ndm, ctx->dd_sub.p, dout, ctx->stream));
+    tick(ctx, 7, false);
+    ctx->launches += 3;
+    if (!out_on_device)
+        CK(cudaMemcpyAsync(out, dout, sizeof(float) * (size_t) ndm * nout, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));           // cd and off are host vectors
+    harvest(ctx);
     return AB_OK;
 }
 

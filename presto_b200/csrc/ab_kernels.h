@@ -187,6 +187,12 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
                       long long n, ab_polished *out, const double2 *tw, size_t budget,
                       cudaStream_t st, char *err, size_t errlen, long long *launches);
 
+// subband dedispersion (prepsubband): x time-major [nspec][nchan] -> xcm
+// channel-major scratch -> D [nsub][nspec / ds] -> out [ndm][nspec / ds]
+cudaError_t launch_dedisp(const float *x, float *xcm, long long nspec, int nchan, const int *cd,
+                          int nsub, int ds, const int *off, int ndm, float *D, float *out,
+                          cudaStream_t st);
+
 // time-series input path: realfft and deredden
 constexpr int AB_DERED_MAXW = 1024;     // longest de-reddening block
 bool realfft_supported(long long n);
