@@ -367,6 +367,9 @@ def run_ours(args):
                            "time per call including the host block plan"}
     del series, sfft
 
+    # ---- subband dedispersion, the DM trials' producer (device in and out) ----
+    dd_line = dedisp_measure(ctx, torch, local)
+
     # ---- candidate polishing (optimize_accelcand) of the search's candidates ----
     cl = ctx.search(obs, None, device_ptr=dev_fft.data_ptr())
     torch.cuda.synchronize()
@@ -470,6 +473,7 @@ def run_ours(args):
         if polish:
             line["polish"] = polish
         line["series_to_fft"] = series_line
+        line["dedisperse"] = dd_line
     ctx.close()
     if rank == 0 and world == 1 and not args.no_pool:
         # the pool patterns against the plain path on the same GPU (after the
@@ -487,6 +491,35 @@ def run_ours(args):
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def dedisp_measure(ctx, torch, local, nspec=1 << 20, nchan=1024, nsub=64, ndm=128, reps=3):
+    """ab_dedisperse of nspec x nchan float spectra into ndm DM trials (device
+    buffers), timed by CUDA events on the context's stream."""
+    dev = f"cuda:{local}"
+    x = torch.randn((nspec, nchan), dtype=torch.float32, device=dev)
+    out = torch.empty((ndm, nspec), dtype=torch.float32, device=dev)
+    dms = np.linspace(0.0, 300.0, ndm)
+    args = (None, 1400.0, 0.25, 64e-6, nsub, dms)
+    kw = dict(device_ptr=x.data_ptr(), nspec=nspec, nchan=nchan, out_ptr=out.data_ptr())
+    ctx.dedisperse(*args, **kw)                               # warm-up
+    torch.cuda.synchronize()
+    ctx.reset_kernel_times()
+    ctx.set_profiling(True)
+    for _ in range(reps):
+        ctx.dedisperse(*args, **kw)
+    kms, _ = ctx.kernel_times()
+    ctx.set_profiling(False)
+    ms = kms[7] / reps
+    algo = 4.0 * nspec * nchan + 4.0 * ndm * nspec            # spectra read once, trials written
+    del x, out
+    torch.cuda.empty_cache()
+    return {"nspec": nspec, "nchan": nchan, "nsub": nsub, "ndm": ndm, "ms": ms,
+            "trials_per_s": ndm / (ms / 1e3),
+            "gb_per_s_algorithmic": algo / (ms / 1e3) / 1e9,
+            "what": "transpose to channel-major, subband sums at the DMs' mean, DM sums "
+                    "(prepsubband's two stages, 1400 MHz + 256 MHz band, DM 0-300), device in "
+                    "and out; algorithmic bytes = spectra read once + trials written"}
 
 
 def measured_fp32_peak(ctx):
