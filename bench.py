@@ -624,23 +624,25 @@ def pool_compare(mode, nreq, rate=2000.0, workers=4, corr="fft"):
     ctx.close()
     busy = sum(kms[:4]) / 1e3 / t_plain
     pool = serve.SearchPool(0, nworkers=workers)
-    if corr in paths:
-        pool.set_corr_path(paths[corr])
-    for r, f in zip(reqs[:workers], ffts[:workers]):          # warm-up
-        pool.wait(pool.submit(f, r["N"], dt, **r["opts"]))
-    pool.reset_stats()
-    t0 = time.perf_counter()
-    tickets = []
-    for r, f in zip(reqs, ffts):
-        if mode == "served":
-            delay = r["t"] - (time.perf_counter() - t0)
-            if delay > 0:
-                time.sleep(delay)
-        tickets.append(pool.submit(f, r["N"], dt, **r["opts"]))
-    got = [pool.wait(t)[0] for t in tickets]
-    t_pool = time.perf_counter() - t0
-    st = pool.stats()
-    pool.close()
+    try:
+        if corr in paths:
+            pool.set_corr_path(paths[corr])
+        for r, f in zip(reqs[:workers], ffts[:workers]):      # warm-up
+            pool.wait(pool.submit(f, r["N"], dt, **r["opts"]))
+        pool.reset_stats()
+        t0 = time.perf_counter()
+        tickets = []
+        for r, f in zip(reqs, ffts):
+            if mode == "served":
+                delay = r["t"] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            tickets.append(pool.submit(f, r["N"], dt, **r["opts"]))
+        got = [pool.wait(t)[0] for t in tickets]
+        t_pool = time.perf_counter() - t0
+        st = pool.stats()
+    finally:
+        pool.close()
     recipe = ("cfg4 (batched DM trials: N uniform in 2^20..2^23, zmax 50/200/600, numharm 8)"
               if mode == "batched" else
               f"cfg5 (served stream: Poisson arrivals at {rate:g}/s, N log-uniform 2^19..2^23, "

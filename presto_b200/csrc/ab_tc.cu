@@ -379,11 +379,14 @@ cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, con
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     TcArgs a{banks_dev, sc, bb, items, tiles, perm, dtime, dt_per_block, pack, planes,
              plane_per_block, fullplane};
+    // the attribute is the kernel's, shared by every host thread launching it
+    // (a request pool's workers launch it with different sizes at once): set
+    // it to the one ceiling every launch fits under, never to this launch's size
     if (fp16) {
-        cudaFuncSetAttribute(k_corr_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(k_corr_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         k_corr_tc<true><<<nitems, 128, smem, st>>>(a);
     } else {
-        cudaFuncSetAttribute(k_corr_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(k_corr_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         k_corr_tc<false><<<nitems, 128, smem, st>>>(a);
     }
     return cudaGetLastError();

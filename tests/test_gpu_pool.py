@@ -51,6 +51,32 @@ def test_pool_results_equal_alone(ctx, ablib):
     assert sum(len(a) for a in alone) > 0
 
 
+@pytest.mark.parametrize("path", ["bf16", "fp16"])
+def test_pool_tensor_core_mix_equal_alone(ablib, path):
+    """The same mix on the tensor-core correlation: workers launch the
+    contraction concurrently with different operand widths (different
+    dynamic shared-memory sizes), and every result equals the request alone
+    on a plain context of the same path."""
+    code = ablib.CORR_TC_SPLIT_BF16 if path == "bf16" else ablib.CORR_TC_SPLIT_FP16
+    cases = [_case(i, c) for i, c in enumerate(MIX)]
+    plain = ablib.Context(0)
+    try:
+        plain.set_corr_path(code)
+        alone = [plain.search(ablib.obs_init(ablib.make_params(c["N"], DT, fft.size, **opts)), fft)
+                 for (fft, opts), c in zip(cases, MIX)]
+    finally:
+        plain.close()
+    pool = serve.SearchPool(0, nworkers=3)
+    try:
+        pool.set_corr_path(code)
+        tickets = [pool.submit(fft, c["N"], DT, **opts) for (fft, opts), c in zip(cases * 3, MIX * 3)]
+        got = [pool.wait(t)[0] for t in tickets]
+    finally:
+        pool.close()
+    for k, cands in enumerate(got):
+        assert cands == alone[k % len(MIX)], k
+
+
 def test_pool_rejects_oversized_request(ablib):
     pool = serve.SearchPool(0, nworkers=1, hbm_budget=12 << 30)
     try:
