@@ -375,21 +375,25 @@ cudaError_t launch_corr_tc(const ab_bank *banks_dev, const SearchConsts &sc, con
                            int fp16, cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    size_t smem = tc_corr_smem(nks_max);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    const size_t smem = tc_corr_smem(nks_max);
     TcArgs a{banks_dev, sc, bb, items, tiles, perm, dtime, dt_per_block, pack, planes,
              plane_per_block, fullplane};
-    // the attribute is the kernel's, shared by every host thread launching it
-    // (a request pool's workers launch it with different sizes at once): set
-    // it to the one ceiling every launch fits under, never to this launch's size
-    if (fp16) {
-        cudaFuncSetAttribute(k_corr_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        k_corr_tc<true><<<nitems, 128, smem, st>>>(a);
-    } else {
-        cudaFuncSetAttribute(k_corr_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        k_corr_tc<false><<<nitems, 128, smem, st>>>(a);
-    }
-    return cudaGetLastError();
+    // The attribute is the kernel's, shared by every host thread launching it
+    // (a request pool's workers launch it with different sizes at once), so it
+    // is set to one ceiling every launch fits under, never to this launch's
+    // size: the 227 KB per block less the kernel's static shared memory.
+    auto launch = [&](auto kern) -> cudaError_t {
+        cudaFuncAttributes fa;
+        cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+        if (e != cudaSuccess) return e;
+        const size_t cap = 227 * 1024 - fa.sharedSizeBytes;
+        if (smem > cap) return cudaErrorInvalidValue;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) cap);
+        if (e != cudaSuccess) return e;
+        kern<<<nitems, 128, smem, st>>>(a);
+        return cudaGetLastError();
+    };
+    return fp16 ? launch(k_corr_tc<true>) : launch(k_corr_tc<false>);
 }
 
 cudaError_t launch_tc_gemm(const float *A, const float *B, float *C, int N, int K, int split,
