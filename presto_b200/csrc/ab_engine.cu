@@ -94,7 +94,7 @@ struct ab_ctx {
     DevBuf<float2> dtime;                   // normalised block data (tensor-core path)
     DevBuf<float2> ser_in, ser_scr;         // time-series input path
     DevBuf<float2> blu_a, blu_b;            // Bluestein work and chirp-kernel transform
-    DevBuf<float> dd_x, dd_xcm, dd_sub, dd_out; // dedispersion: spectra, channel-major, subbands, DMs
+    DevBuf<float> dd_x, dd_sub, dd_out;     // dedispersion: spectra, subbands, DM trials
     DevBuf<int> dd_cd, dd_off;              // dedispersion delays
     long long blu_M = 0;                    // the length blu_b was built for
     DevBuf<int2> dered_blocks;
@@ -1070,7 +1070,6 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->blu_b.release();
     ctx->blu_M = 0;
     ctx->dd_x.release();
-    ctx->dd_xcm.release();
     ctx->dd_sub.release();
     ctx->dd_out.release();
     ctx->dd_cd.release();
@@ -1440,7 +1439,6 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
                            ctx->stream));
         dx = ctx->dd_x.p;
     }
-    CK(ctx->dd_xcm.ensure(nx));
     CK(ctx->dd_sub.ensure((size_t) nsub * nout));
     float *dout = out;
     if (!out_on_device) {
@@ -1448,8 +1446,9 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
         dout = ctx->dd_out.p;
     }
     tick(ctx, 7, true);
-    CK(launch_dedisp(dx, ctx->dd_xcm.p, nspec, nchan, ctx->dd_cd.p, nsub, downsamp, ctx->dd_off.p,
-                     ndm, ctx->dd_sub.p, dout, ctx->stream));
+    const int maxcd = *std::max_element(cd.begin(), cd.end());
+    CK(launch_dedisp(dx, nspec, nchan, ctx->dd_cd.p, maxcd, nsub, downsamp, ctx->dd_off.p, ndm,
+                     ctx->dd_sub.p, dout, ctx->stream));
     tick(ctx, 7, false);
     ctx->launches += 3;
     if (!out_on_device)

@@ -187,9 +187,9 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
                       long long n, ab_polished *out, const double2 *tw, size_t budget,
                       cudaStream_t st, char *err, size_t errlen, long long *launches);
 
-// subband dedispersion (prepsubband): x time-major [nspec][nchan] -> xcm
-// channel-major scratch -> D [nsub][nspec / ds] -> out [ndm][nspec / ds]
-cudaError_t launch_dedisp(const float *x, float *xcm, long long nspec, int nchan, const int *cd,
+// subband dedispersion (prepsubband): x time-major [nspec][nchan] ->
+// D [nsub][nspec / ds] -> out [ndm][nspec / ds]; maxcd the largest channel delay
+cudaError_t launch_dedisp(const float *x, long long nspec, int nchan, const int *cd, int maxcd,
                           int nsub, int ds, const int *off, int ndm, float *D, float *out,
                           cudaStream_t st);
 
