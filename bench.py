@@ -517,7 +517,7 @@ def dedisp_measure(ctx, torch, local, nspec=1 << 20, nchan=1024, nsub=64, ndm=12
     return {"nspec": nspec, "nchan": nchan, "nsub": nsub, "ndm": ndm, "ms": ms,
             "trials_per_s": ndm / (ms / 1e3),
             "gb_per_s_algorithmic": algo / (ms / 1e3) / 1e9,
-            "what": "transpose to channel-major, subband sums at the DMs' mean, DM sums "
+            "what": "subband sums at the DMs' mean from the time-major spectra, then DM sums "
                     "(prepsubband's two stages, 1400 MHz + 256 MHz band, DM 0-300), device in "
                     "and out; algorithmic bytes = spectra read once + trials written"}
 
@@ -661,6 +661,22 @@ def pool_compare(mode, nreq, rate=2000.0, workers=4, corr="fft"):
                        "across requests; wall-clock timing (host arrays in, candidates out)"}
 
 
+def run_dedisp_mode(args):
+    """--mode dedisperse: the dedispersion measurement alone, one line."""
+    import torch
+    import presto_b200 as pb
+    ctx = pb.Context(0)
+    try:
+        dd = dedisp_measure(ctx, torch, 0, reps=max(1, args.steps))
+    finally:
+        ctx.close()
+    line = {"metric": "DM trials/s", "value": dd["trials_per_s"], "unit": "trials/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "steps": max(1, args.steps), "ms_per_step": dd["ms"], "dedisperse": dd}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_pool_mode(args):
     """--mode batched | served: one pool_compare line."""
     line = pool_compare(args.mode, args.requests, args.rate, args.workers, args.corr)
@@ -684,8 +700,10 @@ def main():
     ap.add_argument("--corr", choices=["fft", "tc", "tc16"], default="fft",
                     help="correlation path: FP32 FFTs, or the tensor-core contraction with "
                          "split-BF16 (tc) or split-FP16 (tc16) operands")
-    ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
-                    help="batched/served: the request pool vs the plain path (one GPU)")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "dedisperse"],
+                    default="plain",
+                    help="batched/served: the request pool vs the plain path (one GPU); "
+                         "dedisperse: subband dedispersion alone")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
@@ -694,6 +712,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.mode == "dedisperse" and args.impl == "ours":
+        return run_dedisp_mode(args)
     if args.mode != "plain" and args.impl == "ours":
         return run_pool_mode(args)
     if args.impl == "reference":

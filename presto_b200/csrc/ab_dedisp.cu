@@ -13,18 +13,19 @@
 // final block).  The input spectra X are time-major (all channels of a
 // sample together, channels ascending in frequency) and are read once, in
 // row segments of a subband's channels.  The DM stage gives each thread one
-// output sample of DM_GROUP consecutive DMs: nearby DMs read nearby samples
-// of the same subband (the L1), and all DM groups of a sample tile run
-// together (the L2 keeps the tile's subband windows).
+// output sample of 8, 16 or 32 consecutive DMs, which read nearby samples of
+// the same subband: one shared-memory window per subband serves them all.
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "ab_kernels.h"
 
 namespace ab {
 namespace {
 
-constexpr int DM_GROUP = 8;
 constexpr int SB_TILE = 256;            // downsampled samples per subband CTA
+constexpr int DM_TILE = 256;            // output samples per DM CTA
+constexpr int STAGES = 4;               // subband windows in flight per DM CTA
 
 // D[s][u] for u in [u0, u0 + SB_TILE) of subband s, from the time-major
 // spectra x[t][c]: the rows the tile reads (its samples plus the subband's
@@ -32,24 +33,56 @@ constexpr int SB_TILE = 256;            // downsampled samples per subband CTA
 // memory (each row's channels contiguous in memory, the shared rows padded to
 // an odd stride so that consecutive samples hit different banks), then each
 // thread sums its sample's channels and its ds samples in the reference's
-// order.
+// order.  blockIdx.x = sample tile * nsub + subband: the subbands of one tile
+// run together, so each spectra row is fetched from memory once.  VEC: the
+// rows are read 16 bytes at a time (cps and nchan multiples of 4, x 16-byte
+// aligned), four loads in flight per thread.
+template <bool VEC>
 __global__ void __launch_bounds__(SB_TILE) k_dd_subbands(const float *x, long long nspec, int nchan,
                                                          const int *cd, int cps, int ds,
                                                          long long nout, int maxcd, float *D)
 {
     extern __shared__ float rows[];                    // [nrows][pitch]
     __shared__ int s_cd[1024];
-    const int s = blockIdx.y;
+    const int nsub = nchan / cps;
+    const int s = (int) (blockIdx.x % (unsigned) nsub);
     const int pitch = cps | 1;
-    const long long u0 = (long long) blockIdx.x * SB_TILE;
+    const long long u0 = (long long) (blockIdx.x / (unsigned) nsub) * SB_TILE;
     const long long t_lo = u0 * ds;
     const int nrows = SB_TILE * ds + maxcd;
     for (int j = threadIdx.x; j < cps; j += blockDim.x) s_cd[j] = cd[s * cps + j];
     const float *src = x + (long long) s * cps;
-    for (int e = threadIdx.x; e < nrows * cps; e += blockDim.x) {
-        const int r = e / cps, j = e - r * cps;
-        const long long t = t_lo + r;
-        rows[r * pitch + j] = t < nspec ? __ldg(src + t * nchan + j) : 0.0f;
+    if (VEC) {
+        const int q = cps >> 2, n4 = nrows * q;
+        const float4 *src4 = reinterpret_cast<const float4 *>(src);
+        const long long rs4 = nchan >> 2;
+        for (int b = threadIdx.x; b < n4; b += 4 * SB_TILE) {
+            float4 v[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int e = b + k * SB_TILE, r = e / q;
+                const long long t = t_lo + r;
+                v[k] = e < n4 && t < nspec ? __ldg(src4 + t * rs4 + (e - r * q))
+                                           : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int e = b + k * SB_TILE, r = e / q;
+                if (e < n4) {
+                    float *d = rows + r * pitch + 4 * (e - r * q);
+                    d[0] = v[k].x;
+                    d[1] = v[k].y;
+                    d[2] = v[k].z;
+                    d[3] = v[k].w;
+                }
+            }
+        }
+    } else {
+        for (int e = threadIdx.x; e < nrows * cps; e += blockDim.x) {
+            const int r = e / cps, j = e - r * cps;
+            const long long t = t_lo + r;
+            rows[r * pitch + j] = t < nspec ? __ldg(src + t * nchan + j) : 0.0f;
+        }
     }
     __syncthreads();
     const long long u = u0 + threadIdx.x;
@@ -64,60 +97,184 @@ __global__ void __launch_bounds__(SB_TILE) k_dd_subbands(const float *x, long lo
     D[(long long) s * nout + u] = ds == 1 ? ftmp : __fadd_rn(0.0f, __fdiv_rn(ftmp, (float) ds));
 }
 
-// blockIdx.x = sample tile * ngroups + DM group: the DM groups of one sample
-// tile run together and share its subband windows in L2
-__global__ void __launch_bounds__(256) k_dd_dms(const float *D, long long nout, int nsub,
-                                                const int *off, int ndm, int ngroups, float *out)
+// 4-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, int src_bytes)
 {
-    extern __shared__ int s_off[];                     // [DM_GROUP][nsub]
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// out[d][u] for G consecutive DMs and the DM_TILE samples of one tile, one
+// sample per thread.  blockIdx.x = sample tile * ngroups + DM group: the DM
+// groups of one tile run together and share its subband rows in L2.  Per
+// subband, the window of D the group reads (DM_TILE samples plus the spread
+// of the group's offsets, zero past the end of the data) is copied into a
+// ring of STAGES shared-memory windows by asynchronous copies issued
+// STAGES - 1 subbands ahead, so that the copies of later subbands are in
+// flight while the threads add the current one.
+template <int G>
+__global__ void __launch_bounds__(DM_TILE) k_dd_dms(const float *D, long long nout, int nsub,
+                                                    const int *off, int ndm, int ngroups, int wcap,
+                                                    float *out)
+{
+    extern __shared__ __align__(16) int dsm[];
+    int *s_rel = dsm;                                  // [nsub][G] offset - window start
+    int *s_lo = s_rel + nsub * G;                      // [nsub] window start
+    int *s_len = s_lo + nsub;                          // [nsub] window length (<= wcap)
+    float *win = reinterpret_cast<float *>(s_len + nsub);   // [STAGES][wcap]
     const int grp = (int) (blockIdx.x % (unsigned) ngroups);
-    const long long tile = blockIdx.x / (unsigned) ngroups;
-    const int d0 = grp * DM_GROUP;
-    const int nd = min(DM_GROUP, ndm - d0);
-    for (int i = threadIdx.x; i < nd * nsub; i += blockDim.x) s_off[i] = off[(long long) d0 * nsub + i];
+    const long long u0 = (long long) (blockIdx.x / (unsigned) ngroups) * DM_TILE;
+    const int d0 = grp * G;
+    const int nd = min(G, ndm - d0);
+    for (int s = threadIdx.x; s < nsub; s += blockDim.x) {
+        int lo = off[(long long) d0 * nsub + s], hi = lo;
+        for (int d = 1; d < nd; d++) {
+            const int o = off[(long long) (d0 + d) * nsub + s];
+            lo = min(lo, o);
+            hi = max(hi, o);
+        }
+        s_lo[s] = lo;
+        s_len[s] = DM_TILE + hi - lo;
+        for (int d = 0; d < G; d++)
+            s_rel[s * G + d] = d < nd ? off[(long long) (d0 + d) * nsub + s] - lo : 0;
+    }
     __syncthreads();
-    const long long u = tile * blockDim.x + threadIdx.x;
-    if (u >= nout) return;
-    float acc[DM_GROUP];
-#pragma unroll
-    for (int d = 0; d < DM_GROUP; d++) acc[d] = -0.0f;
-    for (int s = 0; s < nsub; s++) {
-        const float *row = D + (long long) s * nout;
-#pragma unroll
-        for (int d = 0; d < DM_GROUP; d++) {
-            if (d < nd) {
-                const long long uu = u + s_off[d * nsub + s];
-                acc[d] = __fadd_rn(acc[d], uu < nout ? __ldg(row + uu) : 0.0f);
+    auto issue = [&](int s) {
+        if (s < nsub) {
+            float *w = win + (s % STAGES) * wcap;
+            const long long base = u0 + s_lo[s];
+            const float *row = D + (long long) s * nout + base;
+            const long long room = nout - base;
+            const int len = s_len[s];
+            for (int i = threadIdx.x; i < len; i += DM_TILE) {
+                const bool in = i < room;
+                cp_async4(w + i, in ? row + i : D, in ? 4 : 0);
             }
         }
-    }
+        cp_async_commit();                             // empty groups keep the count uniform
+    };
 #pragma unroll
-    for (int d = 0; d < DM_GROUP; d++)
+    for (int p = 0; p < STAGES - 1; p++) issue(p);
+    float acc[G];
+#pragma unroll
+    for (int d = 0; d < G; d++) acc[d] = -0.0f;
+    for (int s = 0; s < nsub; s++) {
+        cp_async_wait<STAGES - 2>();                   // subband s's window has landed
+        __syncthreads();                               // ... for every thread; stage s-1 is free
+        issue(s + STAGES - 1);
+        const float *w = win + (s % STAGES) * wcap + threadIdx.x;
+        const int4 *rel = reinterpret_cast<const int4 *>(s_rel + s * G);
+#pragma unroll
+        for (int q = 0; q < G / 4; q++) {
+            const int4 r = rel[q];
+            acc[4 * q + 0] = __fadd_rn(acc[4 * q + 0], w[r.x]);
+            acc[4 * q + 1] = __fadd_rn(acc[4 * q + 1], w[r.y]);
+            acc[4 * q + 2] = __fadd_rn(acc[4 * q + 2], w[r.z]);
+            acc[4 * q + 3] = __fadd_rn(acc[4 * q + 3], w[r.w]);
+        }
+    }
+    cp_async_wait<0>();
+    const long long u = u0 + threadIdx.x;
+    if (u >= nout) return;
+#pragma unroll
+    for (int d = 0; d < G; d++)
         if (d < nd) out[(long long) (d0 + d) * nout + u] = acc[d];
+}
+
+// largest spread of one subband's offsets over a group of g consecutive DMs
+int group_spread(const int *off, int ndm, int nsub, int g)
+{
+    int m = 0;
+    for (int d0 = 0; d0 < ndm; d0 += g)
+        for (int s = 0; s < nsub; s++) {
+            int lo = off[(size_t) d0 * nsub + s], hi = lo;
+            for (int d = d0 + 1; d < ndm && d < d0 + g; d++) {
+                lo = off[(size_t) d * nsub + s] < lo ? off[(size_t) d * nsub + s] : lo;
+                hi = off[(size_t) d * nsub + s] > hi ? off[(size_t) d * nsub + s] : hi;
+            }
+            m = hi - lo > m ? hi - lo : m;
+        }
+    return m;
+}
+
+size_t dms_smem(int g, int nsub, int wcap)
+{
+    return sizeof(int) * ((size_t) nsub * g + 2 * (size_t) nsub) + sizeof(float) * STAGES * (size_t) wcap;
+}
+
+template <int G>
+cudaError_t launch_dms(const float *D, long long nout, int nsub, const int *off, int ndm, int wcap,
+                       size_t smem, float *out, cudaStream_t st)
+{
+    const int ngroups = (ndm + G - 1) / G;
+    const long long ntiles = (nout + DM_TILE - 1) / DM_TILE;
+    if (ntiles * ngroups > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_dd_dms<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024);
+    if (e != cudaSuccess) return e;
+    k_dd_dms<G><<<(unsigned) (ntiles * ngroups), DM_TILE, smem, st>>>(D, nout, nsub, off, ndm,
+                                                                      ngroups, wcap, out);
+    return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_dedisp(const float *x, long long nspec, int nchan, const int *cd, int maxcd,
-                          int nsub, int ds, const int *off, int ndm, float *D, float *out,
-                          cudaStream_t st)
+                          int nsub, int ds, const int *off, const int *off_host, int ndm, float *D,
+                          float *out, cudaStream_t st)
 {
-    if (nspec < 1 || nchan < 1 || nsub < 1 || nchan % nsub || ds < 1 || ndm < 1 || maxcd < 0)
+    if (nspec < 1 || nchan < 1 || nsub < 1 || nchan % nsub || ds < 1 || ndm < 1 || maxcd < 0 ||
+        nsub > 1024)
         return cudaErrorInvalidValue;
     const int cps = nchan / nsub;
     const long long nout = nspec / ds;
     const size_t smem = sizeof(float) * (size_t) (SB_TILE * ds + maxcd) * (size_t) (cps | 1);
-    const int ngroups = (ndm + DM_GROUP - 1) / DM_GROUP;
-    const long long ntiles = (nout + 255) / 256;
-    if (nout < 1 || cps > 1024 || nsub > 65535 || ntiles * ngroups > 0x7FFFFFFFLL ||
-        smem > 200 * 1024)
+    const long long stiles = (nout + SB_TILE - 1) / SB_TILE;
+    if (nout < 1 || cps > 1024 || stiles * nsub > 0x7FFFFFFFLL || smem > 200 * 1024)
         return cudaErrorInvalidValue;
-    cudaFuncSetAttribute(k_dd_subbands, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    dim3 sg((unsigned) ((nout + SB_TILE - 1) / SB_TILE), nsub);
-    k_dd_subbands<<<sg, SB_TILE, smem, st>>>(x, nspec, nchan, cd, cps, ds, nout, maxcd, D);
-    k_dd_dms<<<(unsigned) (ntiles * ngroups), 256, sizeof(int) * DM_GROUP * nsub, st>>>(
-        D, nout, nsub, off, ndm, ngroups, out);
-    return cudaGetLastError();
+    // DMs per thread: the most of 32 / 16 / 8 (no more than the trials, in
+    // steps of 8) whose windows leave room for four CTAs per SM; else the
+    // fewest that fit at all
+    int g = 0;
+    size_t smem2 = 0;
+    const int gs[3] = {32, 16, 8};
+    for (int i = 0; i < 3 && !g; i++) {
+        if (gs[i] > 8 && gs[i] >= ndm + 8) continue;
+        const size_t m = dms_smem(gs[i], nsub, DM_TILE + group_spread(off_host, ndm, nsub, gs[i]));
+        if (m <= 48 * 1024) g = gs[i], smem2 = m;
+    }
+    if (!g) {
+        g = 8;
+        smem2 = dms_smem(8, nsub, DM_TILE + group_spread(off_host, ndm, nsub, 8));
+        if (smem2 > 200 * 1024) return cudaErrorInvalidValue;
+    }
+    const int wcap = DM_TILE + group_spread(off_host, ndm, nsub, g);
+    const bool vec = cps % 4 == 0 && nchan % 4 == 0 && ((uintptr_t) x & 15) == 0;
+    cudaError_t e;
+    if (vec) {
+        e = cudaFuncSetAttribute(k_dd_subbands<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024);
+        if (e != cudaSuccess) return e;
+        k_dd_subbands<true><<<(unsigned) (stiles * nsub), SB_TILE, smem, st>>>(
+            x, nspec, nchan, cd, cps, ds, nout, maxcd, D);
+    } else {
+        e = cudaFuncSetAttribute(k_dd_subbands<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024);
+        if (e != cudaSuccess) return e;
+        k_dd_subbands<false><<<(unsigned) (stiles * nsub), SB_TILE, smem, st>>>(
+            x, nspec, nchan, cd, cps, ds, nout, maxcd, D);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    switch (g) {
+    case 32: return launch_dms<32>(D, nout, nsub, off, ndm, wcap, smem2, out, st);
+    case 16: return launch_dms<16>(D, nout, nsub, off, ndm, wcap, smem2, out, st);
+    default: return launch_dms<8>(D, nout, nsub, off, ndm, wcap, smem2, out, st);
+    }
 }
 
 }  // namespace ab

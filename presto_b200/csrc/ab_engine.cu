@@ -1445,12 +1445,18 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
         CK(ctx->dd_out.ensure((size_t) ndm * nout));
         dout = ctx->dd_out.p;
     }
-    tick(ctx, 7, true);
     const int maxcd = *std::max_element(cd.begin(), cd.end());
-    CK(launch_dedisp(dx, nspec, nchan, ctx->dd_cd.p, maxcd, nsub, downsamp, ctx->dd_off.p, ndm,
-                     ctx->dd_sub.p, dout, ctx->stream));
+    tick(ctx, 7, true);
+    const cudaError_t le = launch_dedisp(dx, nspec, nchan, ctx->dd_cd.p, maxcd, nsub, downsamp,
+                                         ctx->dd_off.p, off.data(), ndm, ctx->dd_sub.p, dout,
+                                         ctx->stream);
     tick(ctx, 7, false);
-    ctx->launches += 3;
+    if (le != cudaSuccess)
+        return fail(ctx, AB_ERR_ARG, "dedispersion launch refused (%s): a subband's channel delays "
+                    "or a group of 8 DMs' subband offsets spread too far for the "
+                    "shared-memory tiles",
+                    cudaGetErrorString(le));
+    ctx->launches += 2;
     if (!out_on_device)
         CK(cudaMemcpyAsync(out, dout, sizeof(float) * (size_t) ndm * nout, cudaMemcpyDeviceToHost,
                            ctx->stream));

@@ -25,14 +25,19 @@ def _spectra(nspec, nchan, seed, dm=None, f0=None):
     return X
 
 
-@pytest.mark.parametrize("nchan,nsub,ds", [(64, 8, 1), (64, 16, 2), (128, 8, 4)])
-def test_dedisperse_matches_streamed_reference(ctx, oracle, nchan, nsub, ds):
+@pytest.mark.parametrize("nchan,nsub,ds,dmstep", [(64, 8, 1, 5.0), (64, 16, 2, 5.0),
+                                                  (128, 8, 4, 5.0), (128, 16, 1, 23.0),
+                                                  (32, 32, 3, 61.0)])
+def test_dedisperse_matches_streamed_reference(ctx, oracle, nchan, nsub, ds, dmstep):
+    """DM steps of 23 and 61 (14 and 4 trials: a ragged last group of DMs,
+    wide offset spreads within a group), one channel per subband, and an odd
+    downsampling factor among the cases."""
     L = oracle.ref_dedisp_lib()
     if L is None:
         pytest.skip("oracle/_ref/libref_dedisp.so is built where the reference tree is present")
-    W, nb = 4096, 4
+    W, nb = 4096 - 4096 % ds, 4                   # blocks of a multiple of ds spectra
     X = _spectra(W * nb, nchan, nchan + ds, dm=60.0, f0=37.0)
-    dms = np.arange(0.0, 200.0, 5.0)
+    dms = np.arange(0.0, 200.0 if dmstep < 10 else 300.0, dmstep)
     want = oracle.ref_dedisperse(L, X, LO, BW, DT, nsub, dms, ds, W)
     got = ctx.dedisperse(X, LO, BW, DT, nsub, dms, downsamp=ds)
     assert got.shape == want.shape
