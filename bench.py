@@ -465,6 +465,9 @@ def run_ours(args):
                                     "cores": os.cpu_count() or 1, "kind": "port",
                                     "sample": cs["desc"], "searches_per_s": cs["searches_per_s"],
                                     "fft_share_of_thread_time": cs["fft_share"]}
+            dcs = cpu_dedisp_sample()
+            if dcs:
+                dd_line["cpu_baseline"] = dcs
             if polish and polish["candidates"]:
                 pms, pdesc = cpu_polish_sample(fft, obs.lobin, cl, os.cpu_count() or 1,
                                                jerk=bool(obs.numw))
@@ -520,6 +523,30 @@ def dedisp_measure(ctx, torch, local, nspec=1 << 20, nchan=1024, nsub=64, ndm=12
             "what": "subband sums at the DMs' mean from the time-major spectra, then DM sums "
                     "(prepsubband's two stages, 1400 MHz + 256 MHz band, DM 0-300), device in "
                     "and out; algorithmic bytes = spectra read once + trials written"}
+
+
+def cpu_dedisp_sample(nspec=1 << 17, nchan=1024, nsub=64, ndm=128, full_nspec=1 << 20):
+    """The reference's own dedisp_subbands / float_dedisp (src/dispersion.c,
+    compiled unmodified into oracle/_ref/libref_dedisp.so; dedisp_subbands is
+    OpenMP-parallel over subbands) streamed in 8192-spectrum blocks as
+    prepsubband streams them, on a 1/8-length sample of dedisp_measure's
+    workload; trials/s at the full length, scaled by spectra.  None where the
+    library is absent."""
+    from oracle import pyoracle as po
+    L = po.ref_dedisp_lib()
+    if L is None:
+        return None
+    X = np.random.default_rng(5).standard_normal((nspec, nchan), dtype=np.float32)
+    dms = np.linspace(0.0, 300.0, ndm)
+    t0 = time.perf_counter()
+    po.ref_dedisperse(L, X, 1400.0, 0.25, 64e-6, nsub, dms, 1, 8192)
+    full_ms = (time.perf_counter() - t0) * 1e3 * full_nspec / nspec
+    cores = os.cpu_count() or 1
+    return {"value": ndm / (full_ms / 1e3), "unit": "trials/s", "cores": cores,
+            "kind": "reference", "ms_full_length": full_ms,
+            "sample": f"{nspec} of {full_nspec} spectra x {nchan} channels into {ndm} DM trials "
+                      f"(nsub {nsub}), blocks of 8192 with the transposes prepsubband makes, "
+                      f"OpenMP threads up to {cores}; scaled to the full length by spectra"}
 
 
 def measured_fp32_peak(ctx):
@@ -670,6 +697,10 @@ def run_dedisp_mode(args):
         dd = dedisp_measure(ctx, torch, 0, reps=max(1, args.steps))
     finally:
         ctx.close()
+    if not args.no_cpu:
+        dcs = cpu_dedisp_sample()
+        if dcs:
+            dd["cpu_baseline"] = dcs
     line = {"metric": "DM trials/s", "value": dd["trials_per_s"], "unit": "trials/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "steps": max(1, args.steps), "ms_per_step": dd["ms"], "dedisperse": dd}
