@@ -694,11 +694,11 @@ def run_dedisp_mode(args):
     import presto_b200 as pb
     ctx = pb.Context(0)
     try:
-        dd = dedisp_measure(ctx, torch, 0, reps=max(1, args.steps))
+        dd = dedisp_measure(ctx, torch, 0, nspec=args.dd_nspec, reps=max(1, args.steps))
     finally:
         ctx.close()
     if not args.no_cpu:
-        dcs = cpu_dedisp_sample()
+        dcs = cpu_dedisp_sample(nspec=min(1 << 17, args.dd_nspec), full_nspec=args.dd_nspec)
         if dcs:
             dd["cpu_baseline"] = dcs
     line = {"metric": "DM trials/s", "value": dd["trials_per_s"], "unit": "trials/s",
@@ -738,6 +738,8 @@ def main():
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
+    ap.add_argument("--dd-nspec", type=int, default=1 << 20,
+                    help="dedisperse mode: spectra (of 1024 channels) to dedisperse")
     ap.add_argument("--no-pool", action="store_true",
                     help="leave the batched / served comparison out of the default line")
     args = ap.parse_args()

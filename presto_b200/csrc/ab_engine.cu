@@ -1439,7 +1439,7 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
                            ctx->stream));
         dx = ctx->dd_x.p;
     }
-    CK(ctx->dd_sub.ensure((size_t) nsub * nout));
+    CK(ctx->dd_sub.ensure((size_t) nsub * (size_t) dedisp_sub_pitch(nout)));
     float *dout = out;
     if (!out_on_device) {
         CK(ctx->dd_out.ensure((size_t) ndm * nout));
@@ -1454,7 +1454,7 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
     if (le != cudaSuccess)
         return fail(ctx, AB_ERR_ARG, "dedispersion launch refused (%s): a subband's channel delays "
                     "or a group of 8 DMs' subband offsets spread too far for the "
-                    "shared-memory tiles",
+                    "shared-memory tiles (200 KB)",
                     cudaGetErrorString(le));
     ctx->launches += 2;
     if (!out_on_device)

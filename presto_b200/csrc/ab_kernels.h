@@ -188,9 +188,10 @@ int rzw_optimize_each(const float2 *data, long long numdata, long long lobin, co
                       cudaStream_t st, char *err, size_t errlen, long long *launches);
 
 // subband dedispersion (prepsubband): x time-major [nspec][nchan] ->
-// D [nsub][nspec / ds] -> out [ndm][nspec / ds]; maxcd the largest channel
-// delay; off the subband offsets on the device, off_host the same on the host
-// (the DM stage's window sizes are chosen from them)
+// D [nsub][dedisp_sub_pitch(nspec / ds)] -> out [ndm][nspec / ds]; maxcd the
+// largest channel delay; off the subband offsets on the device, off_host the
+// same on the host (the DM stage's window sizes are chosen from them)
+long long dedisp_sub_pitch(long long nout);
 cudaError_t launch_dedisp(const float *x, long long nspec, int nchan, const int *cd, int maxcd,
                           int nsub, int ds, const int *off, const int *off_host, int ndm, float *D,
                           float *out, cudaStream_t st);

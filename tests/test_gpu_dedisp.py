@@ -28,12 +28,13 @@ def _spectra(nspec, nchan, seed, dm=None, f0=None):
 @pytest.mark.parametrize("nchan,nsub,ds,dmstep", [(64, 8, 1, 5.0), (64, 16, 2, 5.0),
                                                   (128, 8, 4, 5.0), (128, 16, 1, 23.0),
                                                   (32, 32, 3, 61.0), (256, 8, 1, 11.0),
-                                                  (96, 8, 2, 7.0)])
+                                                  (96, 8, 2, 7.0), (128, 2, 1, 10.0),
+                                                  (64, 32, 2, 13.0)])
 def test_dedisperse_matches_streamed_reference(ctx, oracle, nchan, nsub, ds, dmstep):
-    """4, 8, 16, 32, 12 and 1 channels per subband (the compiled widths and
-    the general path); DM steps of 23, 61 and 11 (14, 4 and 28 trials: ragged
-    last groups of DMs, wide offset spreads within a group); an odd
-    downsampling factor among the cases."""
+    """1, 2, 4, 8, 16, 32 and 64 channels per subband (the compiled widths)
+    and 12 (the general path); DM steps of 23, 61, 11 and 13 (14, 4, 28 and 24
+    trials: ragged last groups of 16 DMs, a group of 8, wide offset spreads
+    within a group); an odd downsampling factor among the cases."""
     L = oracle.ref_dedisp_lib()
     if L is None:
         pytest.skip("oracle/_ref/libref_dedisp.so is built where the reference tree is present")
