@@ -721,12 +721,17 @@ __global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_std(c
     __shared__ long long s_rlo[NS1];
     __shared__ int s_zlo[NS1], s_wind[NS1];
     const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
-    int x = blockIdx.x;
-    const int zt = x % nzt;
-    x /= nzt;
-    const int wi = x % sc.numws;
-    const int bi = x / sc.numws;
-    const int r = blockIdx.y * HS_RT + threadIdx.x;
+    const int nrt = (sc.corr_uselen + HS_RT - 1) / HS_RT;
+    // r tile fastest: CTAs that share subharmonic row segments at their r
+    // boundaries run together, so the shared sectors come from L2
+    unsigned x = blockIdx.x;
+    const int rt = (int) (x % (unsigned) nrt);
+    x /= (unsigned) nrt;
+    const int zt = (int) (x % (unsigned) nzt);
+    x /= (unsigned) nzt;
+    const int wi = (int) (x % (unsigned) sc.numws);
+    const int bi = (int) (x / (unsigned) sc.numws);
+    const int r = rt * HS_RT + threadIdx.x;
     const int z0 = zt * HS_ZT;
     const double startr = bb.startr[bi];
     const double lastr = startr + sc.rstep - AB_DR;
@@ -798,8 +803,11 @@ cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
                                long long plane_per_block, HitBuf hb, float *dbg, int dbg_bi,
                                cudaStream_t st)
 {
-    int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
-    dim3 grid((unsigned) (bb.nblk * sc.numws * nzt), (sc.corr_uselen + HS_RT - 1) / HS_RT);
+    const long long nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
+    const long long nrt = (sc.corr_uselen + HS_RT - 1) / HS_RT;
+    const long long ncta = (long long) bb.nblk * sc.numws * nzt * nrt;
+    if (ncta < 1 || ncta > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+    const unsigned grid = (unsigned) ncta;
     switch (sc.stages) {
 #define AB_HS_CASE(S)                                                                          \
     case S:                                                                                    \
