@@ -36,11 +36,12 @@ sys.path.insert(0, ROOT)
 # kernel on the zmax=600 numharm=16 search at N=2^20 (one batch of 49 blocks,
 # 1.87 GB of planes): the 4096-point correlation launch read 0.17 GB and wrote
 # 1.81 GB for its 1.84 GB of planes (profiles/k_corr_4096_accelsearch_zmax600_
-# N2e20.md); the harmonic sum read 2.22 GB of the batch's 1.87 GB (profiles/
-# k_harmsum_std5_accelsearch_zmax600_N2e20.md).  Both move bytes in proportion
-# to the planes, so full-size launches scale by their plane bytes.
+# N2e20.md); the harmonic sum read 1.885 GB and wrote 0.005 GB for the batch's
+# 1.87 GB (profiles/k_harmsum_std5_accelsearch_zmax600_N2e20.md).  Both move
+# bytes in proportion to the planes, so full-size launches scale by their
+# plane bytes.
 CORR_DRAM_PER_PLANE_BYTE = (0.17 + 1.81) / 1.84
-HARMSUM_DRAM_PER_PLANE_BYTE = 2.22 / 1.87
+HARMSUM_DRAM_PER_PLANE_BYTE = (1.885 + 0.005) / 1.87
 
 WORKLOADS = {
     "cfg2": dict(N=1 << 23, dt=64e-6, zmax=600, wmax=None, numharm=16, sigma=2.0,
