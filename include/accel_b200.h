@@ -477,6 +477,22 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
                   double lofreq, double chanwidth, double dt, int nsub, const double *dms, int ndm,
                   int downsamp, float *out, int out_on_device);
 
+/* The DM-trial pipeline on the device (prepsubband, then accelsearch on each
+ * trial's .dat, src/accel_utils.c:1552-1562 for the series): the spectra are
+ * dedispersed as ab_dedisperse does, each trial becomes a spectrum as
+ * ab_series_to_fft makes it (realfft + deredden), and that spectrum is
+ * searched as ab_search searches it, without the trials or their spectra
+ * leaving the device.  obs must describe the trials: N = (nspec / downsamp)
+ * rounded down to even (an odd last sample is dropped, as realfft needs an
+ * even length) and dt = dt * downsamp.  Trial d's candidates, in ab_search's
+ * order, are cands[first[d] .. first[d + 1]) (first: ndm + 1 offsets, always
+ * filled); AB_ERR_OVERFLOW when they exceed maxcands (cands may be NULL to
+ * count them).  ab_last_cands afterwards holds the last trial's. */
+int ab_search_dedispersed(ab_ctx *ctx, const float *data, int data_on_device, long long nspec,
+                          int nchan, double lofreq, double chanwidth, double dt, int nsub,
+                          const double *dms, int ndm, int downsamp, const ab_obs *obs,
+                          ab_cand *cands, long long maxcands, long long *first);
+
 /* Host-side statistics and candidate-list helpers. */
 double ab_candidate_sigma(double power, int numsum, double numtrials);
 double ab_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -39,7 +39,7 @@ EXPORTS = [
     "ab_write_accelfile", "ab_nice_output_1", "ab_nice_output_2", "ab_set_worklog",
     "ab_last_worklog", "ab_candlist_set_worklog", "ab_candlist_worklog", "ab_ffdot_hits",
     "ab_read_zaplist", "ab_zapbirds", "ab_zapbirds_host", "ab_mt19937_output",
-    "ab_pool_set_corr_path", "ab_dedisp_delays", "ab_dedisperse",
+    "ab_pool_set_corr_path", "ab_dedisp_delays", "ab_dedisperse", "ab_search_dedispersed",
 ]
 
 COST_SLOTS = 16
@@ -187,6 +187,8 @@ def lib():
     L.ab_search_ffdotpows.argtypes = [vp, C.POINTER(Obs), C.POINTER(FFDotPows), i, vp]
     L.ab_dedisp_delays.argtypes = [i, d, d, d, i, vp, i, i, vp, vp]
     L.ab_dedisperse.argtypes = [vp, vp, i, ll, i, d, d, d, i, vp, i, i, vp, i]
+    L.ab_search_dedispersed.argtypes = [vp, vp, i, ll, i, d, d, d, i, vp, i, i, C.POINTER(Obs),
+                                        C.POINTER(Cand), ll, C.POINTER(ll)]
     L.ab_read_zaplist.argtypes = [C.c_char_p, d, d, vp, vp, i, C.POINTER(i)]
     L.ab_zapbirds.argtypes = [vp, vp, i, ll, ll, vp, vp, i, C.POINTER(i)]
     L.ab_zapbirds_host.argtypes = [vp, ll, ll, vp, vp, i, C.POINTER(i)]
@@ -707,6 +709,39 @@ class Context:
         self._check(self.L.ab_dedisperse(self.ptr, x.ctypes.data, 0, nspec, nchan, lofreq,
                                          chanwidth, dt, nsub, dmv.ctypes.data, dmv.size,
                                          downsamp, out.ctypes.data, 0), "ab_dedisperse")
+        return out
+
+    def search_dedispersed(self, data, lofreq, chanwidth, dt, nsub, dms, obs, downsamp=1,
+                           device_ptr=None, nspec=None, nchan=None):
+        """Dedisperses time-major float spectra data[nspec][nchan] and searches
+        every DM trial on the device (ab_search_dedispersed): returns one
+        candidate list per DM, each as search() returns it.  obs describes a
+        trial: obs_init(make_params((nspec // downsamp) & ~1, dt * downsamp,
+        ...))."""
+        dmv = np.ascontiguousarray(dms, dtype=np.float64)
+        if device_ptr is not None:
+            src, on_dev, ns, nc = C.c_void_p(device_ptr), 1, int(nspec), int(nchan)
+        else:
+            x = np.ascontiguousarray(data, dtype=np.float32)
+            ns, nc = x.shape
+            src, on_dev = C.c_void_p(x.ctypes.data), 0
+        first = (C.c_longlong * (dmv.size + 1))()
+        args = (self.ptr, src, on_dev, ns, nc, lofreq, chanwidth, dt, nsub, dmv.ctypes.data,
+                dmv.size, downsamp, C.byref(obs))
+        cap = 1 << 16
+        cands = (Cand * cap)()
+        rc = self.L.ab_search_dedispersed(*args, cands, cap, first)
+        if rc == -4 and first[dmv.size] > cap:
+            # more candidates than the first buffer held: search again into one
+            # of the size the first pass counted
+            cap = first[dmv.size]
+            cands = (Cand * cap)()
+            rc = self.L.ab_search_dedispersed(*args, cands, cap, first)
+        self._check(rc, "ab_search_dedispersed")
+        out = []
+        for k in range(dmv.size):
+            out.append([(c.power, c.sigma, c.numharm, c.r, c.z, c.w)
+                        for c in cands[first[k]:first[k + 1]]])
         return out
 
     def autotune(self):

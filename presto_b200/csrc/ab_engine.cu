@@ -95,6 +95,7 @@ struct ab_ctx {
     DevBuf<float2> ser_in, ser_scr;         // time-series input path
     DevBuf<float2> blu_a, blu_b;            // Bluestein work and chirp-kernel transform
     DevBuf<float> dd_x, dd_sub, dd_out;     // dedispersion: spectra, subbands, DM trials
+    DevBuf<float2> dd_fft;                  // spectrum of one DM trial (ab_search_dedispersed)
     DevBuf<int> dd_cd, dd_off;              // dedispersion delays
     long long blu_M = 0;                    // the length blu_b was built for
     DevBuf<int2> dered_blocks;
@@ -995,6 +996,10 @@ static int check_device_error(ab_ctx *ctx)
     return AB_OK;
 }
 
+// Device arrays of float2 (complex spectra, series read in pairs) must be
+// 8-byte aligned; a misaligned pointer is refused instead of faulting.
+static bool misaligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) != 0; }
+
 static int use_device(ab_ctx *ctx)
 {
     CK(cudaSetDevice(ctx->device));
@@ -1072,6 +1077,7 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->dd_x.release();
     ctx->dd_sub.release();
     ctx->dd_out.release();
+    ctx->dd_fft.release();
     ctx->dd_cd.release();
     ctx->dd_off.release();
     ctx->dered_blocks.release();
@@ -1200,6 +1206,8 @@ int ab_optimize_cands(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, in
     if (!ctx || !obs || !fft || (n > 0 && (!cands || !out)) || n < 0) return AB_ERR_ARG;
     if (n == 0) return AB_OK;
     if (n > (1 << 24)) return fail(ctx, AB_ERR_ARG, "too many candidates");
+    if (fft_on_device && misaligned8(fft))
+        return fail(ctx, AB_ERR_ARG, "device spectrum not 8-byte aligned");
     int rc = use_device(ctx);
     if (rc) return rc;
     const float2 *dfft = reinterpret_cast<const float2 *>(fft);
@@ -1299,9 +1307,12 @@ static int realfft_dev(ab_ctx *ctx, const float *series, long long n, int series
         return fail(ctx, AB_ERR_ARG, "realfft length %lld: need an even length from 1024 to 2^26 "
                                      "(n/2 a power of two up to 2^26, else up to 2^25)", n);
     const float *din = series;
-    if (!series_on_device) {
+    if (!series_on_device || misaligned8(series)) {
+        // host series, or a device series not on an 8-byte boundary (the
+        // transforms read it in pairs): into the aligned input buffer
         CK(ctx->ser_in.ensure((size_t) ((n + 1) / 2)));
-        CK(cudaMemcpyAsync(ctx->ser_in.p, series, sizeof(float) * n, cudaMemcpyHostToDevice,
+        CK(cudaMemcpyAsync(ctx->ser_in.p, series, sizeof(float) * n,
+                           series_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                            ctx->stream));
         din = reinterpret_cast<const float *>(ctx->ser_in.p);
     }
@@ -1370,6 +1381,8 @@ int ab_deredden(ab_ctx *ctx, ab_fcomplex *fft, long long numbins, int startwidth
                 double endfreq, double T, int fft_on_device)
 {
     if (!ctx || !fft || numbins < 1) return AB_ERR_ARG;
+    if (fft_on_device && misaligned8(fft))
+        return fail(ctx, AB_ERR_ARG, "device spectrum not 8-byte aligned");
     int rc = use_device(ctx);
     if (rc) return rc;
     float2 *d = reinterpret_cast<float2 *>(fft);
@@ -1391,6 +1404,8 @@ int ab_series_to_fft(ab_ctx *ctx, const float *series, long long n, double dt, i
                      ab_fcomplex *out, int out_on_device)
 {
     if (!ctx || !series || !out || dt <= 0.0) return AB_ERR_ARG;
+    if (out_on_device && misaligned8(out))
+        return fail(ctx, AB_ERR_ARG, "device spectrum not 8-byte aligned");
     int rc = use_device(ctx);
     if (rc) return rc;
     float2 *dout = reinterpret_cast<float2 *>(out);
@@ -1465,6 +1480,48 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
     return AB_OK;
 }
 
+int ab_search_dedispersed(ab_ctx *ctx, const float *data, int data_on_device, long long nspec,
+                          int nchan, double lofreq, double chanwidth, double dt, int nsub,
+                          const double *dms, int ndm, int downsamp, const ab_obs *obs,
+                          ab_cand *cands, long long maxcands, long long *first)
+{
+    if (!ctx || !data || !dms || !obs || !first || ndm < 1 || downsamp < 1 || nspec < 1)
+        return fail(ctx, AB_ERR_ARG, "dedispersed-search arguments");
+    const long long nout = nspec / downsamp;
+    const long long n = nout & ~1LL;
+    if (n < 2 || obs->N != n || obs->numbins > n / 2 ||
+        std::fabs(obs->dt - dt * downsamp) > 1e-9 * dt * downsamp)
+        return fail(ctx, AB_ERR_ARG, "obs must describe the trials: N = %lld, dt = %.9g", n,
+                    dt * downsamp);
+    int rc = use_device(ctx);
+    if (rc) return rc;
+    // the trials stay in the context's trial buffer, then one spectrum at a time
+    CK(ctx->dd_out.ensure((size_t) ndm * (size_t) nout));
+    rc = ab_dedisperse(ctx, data, data_on_device, nspec, nchan, lofreq, chanwidth, dt, nsub, dms,
+                       ndm, downsamp, ctx->dd_out.p, 1);
+    if (rc) return rc;
+    CK(ctx->dd_fft.ensure((size_t) (n / 2)));
+    std::vector<ab_cand> all;
+    first[0] = 0;
+    for (int d = 0; d < ndm; d++) {
+        rc = ab_series_to_fft(ctx, ctx->dd_out.p + (size_t) d * (size_t) nout, n, dt * downsamp, 1,
+                              reinterpret_cast<ab_fcomplex *>(ctx->dd_fft.p), 1);
+        if (rc) return rc;
+        long long nc = 0;
+        rc = ab_search(ctx, obs, reinterpret_cast<const ab_fcomplex *>(ctx->dd_fft.p), 1, 0, -1,
+                       nullptr, 0, &nc);
+        if (rc) return rc;
+        all.insert(all.end(), ctx->last_cands.begin(), ctx->last_cands.end());
+        first[d + 1] = (long long) all.size();
+    }
+    const long long total = (long long) all.size();
+    if (cands)
+        for (long long i = 0; i < total && i < maxcands; i++) cands[i] = all[(size_t) i];
+    if (cands && total > maxcands)
+        return fail(ctx, AB_ERR_OVERFLOW, "%lld candidates > maxcands", total);
+    return AB_OK;
+}
+
 int ab_zapbirds(ab_ctx *ctx, ab_fcomplex *fft, int fft_on_device, long long numbins, long long N,
                 const double *lobins, const double *hibins, int numbirds, int *numzapped)
 {
@@ -1472,6 +1529,7 @@ int ab_zapbirds(ab_ctx *ctx, ab_fcomplex *fft, int fft_on_device, long long numb
         return AB_ERR_ARG;
     if (!fft_on_device)
         return ab_zapbirds_host(fft, numbins, N, lobins, hibins, numbirds, numzapped);
+    if (misaligned8(fft)) return fail(ctx, AB_ERR_ARG, "device spectrum not 8-byte aligned");
     int rc = use_device(ctx);
     if (rc) return rc;
     long long lo = 0, hi = 0;
@@ -1544,6 +1602,8 @@ int ab_search(ab_ctx *ctx, const ab_obs *obs, const ab_fcomplex *fft, int fft_on
               long long *numcands)
 {
     if (!ctx || !obs || !fft) return fail(ctx, AB_ERR_ARG, "null argument");
+    if (fft_on_device && misaligned8(fft))
+        return fail(ctx, AB_ERR_ARG, "device spectrum not 8-byte aligned");
     const double t_start = now_ms();
     int rc = use_device(ctx);
     if (rc) return rc;

@@ -10,6 +10,7 @@
 // the bank descriptor, the block start and the correlation work list) live
 // in a file-scope static device array instead of context memory.
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include <cstdio>
 #include <mutex>
@@ -123,6 +124,11 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
                                       ab_ffdotpows *meta_out)
 {
     if (!obs || !d_fft || !d_templates || !d_powers) return AB_ERR_ARG;
+    // complex arrays are read as 8-byte pairs, powers as 4-byte words: a
+    // pointer off those boundaries would fault the kernels
+    if ((reinterpret_cast<uintptr_t>(d_fft) | reinterpret_cast<uintptr_t>(d_templates)) & 7u ||
+        reinterpret_cast<uintptr_t>(d_powers) & 3u)
+        return AB_ERR_ARG;
     // a CUDA error left pending by the caller's own work stays the caller's:
     // nothing is launched, so no error check below can consume it
     if (cudaPeekAtLastError() != cudaSuccess) return AB_ERR_STATE;

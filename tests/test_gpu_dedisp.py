@@ -80,3 +80,45 @@ def test_dedispersed_trial_finds_the_pulsar(ctx, ablib):
     ratio = top[3] / (37.0 * T)
     assert min(abs(ratio - p / q) for p in range(1, 9) for q in range(1, 9)) < 0.01, top
     assert best[0.0] is None or best[0.0][1] < top[1]
+
+
+@pytest.mark.parametrize("nspec,ds", [(1 << 16, 1), ((1 << 16) + 2, 2)])
+def test_search_dedispersed_equals_host_chain(ctx, ablib, nspec, ds):
+    """ab_search_dedispersed (trials and their spectra stay on the device)
+    gives, trial by trial, exactly the candidates of the same steps chained
+    through host arrays: ab_dedisperse, ab_series_to_fft, ab_search.  With
+    ds = 2 the trials have an odd length and lose their last sample; the
+    pulsar at DM 60 is the strongest candidate of its trial."""
+    X = _spectra(nspec, 64, 21, dm=60.0, f0=37.0)
+    dms = [0.0, 30.0, 60.0, 90.0]
+    n = (nspec // ds) & ~1
+    obs = ablib.obs_init(ablib.make_params(n, DT * ds, n // 2, zmax=10, numharm=4, sigma=2.0))
+    got = ctx.search_dedispersed(X, LO, BW, DT, 8, dms, obs, downsamp=ds)
+    trials = ctx.dedisperse(X, LO, BW, DT, 8, dms, downsamp=ds)
+    assert len(got) == len(dms)
+    for d in range(len(dms)):
+        fft = ctx.series_to_fft(trials[d][:n], DT * ds)
+        want = ctx.search(obs, fft)
+        assert got[d] == want, d
+    top = max(got[2], key=lambda c: c[1])
+    ratio = top[3] / (37.0 * n * DT * ds)
+    assert min(abs(ratio - p / q) for p in range(1, 9) for q in range(1, 9)) < 0.01, top
+
+
+def test_search_dedispersed_device_input_and_checks(ctx, ablib):
+    """Spectra already on the device give the host input's result; an obs that
+    does not describe the trials is refused."""
+    import torch
+
+    X = _spectra(1 << 15, 32, 5, dm=40.0, f0=29.0)
+    dms = [0.0, 40.0]
+    n = X.shape[0]
+    obs = ablib.obs_init(ablib.make_params(n, DT, n // 2, zmax=6, numharm=2, sigma=2.0))
+    host = ctx.search_dedispersed(X, LO, BW, DT, 4, dms, obs)
+    dx = torch.from_numpy(X).cuda()
+    dev = ctx.search_dedispersed(None, LO, BW, DT, 4, dms, obs, device_ptr=dx.data_ptr(),
+                                 nspec=X.shape[0], nchan=X.shape[1])
+    assert dev == host and sum(len(c) for c in host) > 0
+    bad = ablib.obs_init(ablib.make_params(n // 2, DT, n // 4, zmax=6, numharm=2, sigma=2.0))
+    with pytest.raises(ablib.AccelError):
+        ctx.search_dedispersed(X, LO, BW, DT, 4, dms, bad)

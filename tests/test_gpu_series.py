@@ -111,3 +111,32 @@ def test_zapbirds_on_device_matches_host(ctx, ablib):
     assert ctx.last_numzapped == 6
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     assert not np.array_equal(got, spec)
+
+
+def test_device_pointers_off_their_boundary(ctx, ablib):
+    """A device series that starts 4 bytes off an 8-byte boundary (a trial of
+    odd length inside a DM-trial array) is read through the aligned input
+    buffer and gives the aligned result bit for bit; a device spectrum off its
+    8-byte boundary is refused before anything is launched."""
+    import ctypes as C
+
+    import torch
+
+    n = 1 << 16
+    x = synth.time_series(n, 17, [dict(r=900.3, z=0.0, harms=[(0.2, 0.0)])]).astype(np.float32)
+    want = ctx.series_to_fft(x, DT)
+    buf = torch.zeros(n + 1, dtype=torch.float32, device="cuda")
+    buf[1:] = torch.from_numpy(x).cuda()
+    out = torch.empty(n, dtype=torch.float32, device="cuda")     # n/2 complex bins
+    rc = ctx.L.ab_series_to_fft(ctx.ptr, C.c_void_p(buf.data_ptr() + 4), n, DT, 1,
+                                C.c_void_p(out.data_ptr()), 1)
+    assert rc == 0
+    got = out.cpu().numpy().view(np.complex64)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    rc = ctx.L.ab_series_to_fft(ctx.ptr, C.c_void_p(buf.data_ptr()), n, DT, 1,
+                                C.c_void_p(out.data_ptr() + 4), 1)
+    assert rc == -1                                               # AB_ERR_ARG
+    obs = ablib.obs_init(ablib.make_params(n, DT, n // 2, zmax=10, numharm=2))
+    with pytest.raises(ablib.AccelError):
+        ctx.search(obs, None, device_ptr=out.data_ptr() + 4)
+    assert len(ctx.search(obs, None, device_ptr=out.data_ptr())) == len(ctx.search(obs, want))
