@@ -750,6 +750,8 @@ def run_pipeline_mode(args):
         # the same with the spectra already in device memory
         dx = torch.from_numpy(X).cuda()
         res_dev_ms = []
+        ctx.reset_kernel_times()
+        ctx.set_profiling(True)
         for _ in range(max(1, args.steps)):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -757,6 +759,12 @@ def run_pipeline_mode(args):
                                         device_ptr=dx.data_ptr(), nspec=nspec, nchan=nchan)
             res_dev_ms.append((time.perf_counter() - t0) * 1e3)
             assert rd == res
+        kms, _ = ctx.kernel_times()
+        ctx.set_profiling(False)
+        per_trial = {k: v / (ndm * len(res_dev_ms)) for k, v in
+                     zip(("templates", "prep", "corr", "harmsum", "host_outside_replay",
+                          "replay_overlapped", "wait_and_readback"), kms[:7])}
+        per_trial["dedispersion"] = kms[7] / (ndm * len(res_dev_ms))
         del dx
     finally:
         ctx.close()
@@ -767,6 +775,7 @@ def run_pipeline_mode(args):
             "config": {"workload": "pipeline", "nspec": nspec, "nchan": nchan, "nsub": nsub,
                        "ndm": ndm, "dm_range": [0.0, 300.0], "zmax": 200, "numharm": 8},
             "spectra_on_device_ms_per_step": statistics.median(res_dev_ms),
+            "ms_per_trial_by_stage": per_trial,
             "spectra_h2d_bytes_per_step": int(X.nbytes),
             "host_chain_ms_per_step": statistics.median(host_ms),
             "device_vs_host_chain": statistics.median(host_ms) / ms,

@@ -5,6 +5,7 @@
  * with the replay of device threshold crossings in reference order.
  */
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -12,6 +13,7 @@
 #include <string.h>
 #include <pthread.h>
 #include <unistd.h>
+#include <sys/mman.h>
 
 #include "ab_host.h"
 #include "ab_index.h"
@@ -522,6 +524,10 @@ struct ab_list {
     double wlog_T;
     char *wlog;
     size_t wlen, wcap;
+    /* scratch of the batch replays (ab_replay_hits), kept for the list's
+       next batch */
+    void *scr;
+    size_t scr_cap;
 };
 
 ab_list *ab_list_new(void)
@@ -537,6 +543,7 @@ void ab_list_free(ab_list *l)
     free(l->c);
     free(l->seg);
     free(l->wlog);
+    free(l->scr);
     free(l);
 }
 
@@ -749,11 +756,10 @@ long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout)
 }
 
 /* Parallel LSD radix sort of hit indices by key.  Keys are taken relative
- * to the smallest block present, so a batch's keys fit in 48 bits: four
- * passes of 12-bit digits, each pass a per-thread histogram, an exclusive
- * scan over (digit, thread) and a stable scatter. */
-#define RS_BITS 12
-#define RS_BINS (1 << RS_BITS)
+ * to the smallest present and sorted in equal digits of at most 14 bits (a
+ * batch's re-packed keys need two or three passes), each pass a per-thread
+ * histogram, an exclusive scan over (digit, thread) and a stable scatter. */
+#define RS_MAXBITS 14                   /* digit width at most; 2^14 bins per thread */
 #define RS_MAXT 16
 
 typedef struct {
@@ -763,15 +769,17 @@ typedef struct {
     unsigned long long *o1;
     size_t lo, hi;
     int shift;
-    size_t *hist;                       /* [RS_BINS] of this thread */
+    unsigned mask;
+    size_t *hist;                       /* [nbins] of this thread */
 } rs_job;
 
 typedef struct {
     rs_job job[RS_MAXT];
     int nt, phase;
     pthread_barrier_t bar;
-    size_t (*hist)[RS_BINS];
-    int npasses;
+    size_t *hist;                       /* [nt][nbins] */
+    int npasses, dbits;
+    size_t nbins;
     unsigned long long *ka, *kb;
     unsigned long long *oa, *ob;
     size_t n;
@@ -781,14 +789,14 @@ typedef struct { rs_ctx *c; int id; } rs_arg;
 
 static void rs_count(rs_job *j)
 {
-    memset(j->hist, 0, sizeof(size_t) * RS_BINS);
-    for (size_t i = j->lo; i < j->hi; i++) j->hist[(j->k0[i] >> j->shift) & (RS_BINS - 1)]++;
+    memset(j->hist, 0, sizeof(size_t) * ((size_t) j->mask + 1));
+    for (size_t i = j->lo; i < j->hi; i++) j->hist[(j->k0[i] >> j->shift) & j->mask]++;
 }
 
 static void rs_scatter(rs_job *j)
 {
     for (size_t i = j->lo; i < j->hi; i++) {
-        size_t pos = j->hist[(j->k0[i] >> j->shift) & (RS_BINS - 1)]++;
+        size_t pos = j->hist[(j->k0[i] >> j->shift) & j->mask]++;
         j->k1[pos] = j->k0[i];
         j->o1[pos] = j->o0[i];
     }
@@ -797,10 +805,10 @@ static void rs_scatter(rs_job *j)
 static void rs_scan(rs_ctx *c)
 {
     size_t sum = 0;
-    for (int d = 0; d < RS_BINS; d++)
+    for (size_t d = 0; d < c->nbins; d++)
         for (int t = 0; t < c->nt; t++) {
-            size_t v = c->hist[t][d];
-            c->hist[t][d] = sum;
+            size_t v = c->hist[(size_t) t * c->nbins + d];
+            c->hist[(size_t) t * c->nbins + d] = sum;
             sum += v;
         }
 }
@@ -812,7 +820,8 @@ static void rs_setup_pass(rs_ctx *c, int pass)
     for (int t = 0; t < c->nt; t++) {
         rs_job *j = &c->job[t];
         j->k0 = k0; j->k1 = k1; j->o0 = o0; j->o1 = o1;
-        j->shift = RS_BITS * pass;
+        j->shift = c->dbits * pass;
+        j->mask = (unsigned) (c->nbins - 1);
     }
 }
 
@@ -835,8 +844,10 @@ static void *rs_worker(void *p)
 
 static int g_active_sorts = 0;
 
-/* Sorts keys[] (and the payload pl[] with it) in place by key. */
-static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long long n)
+/* Sorts keys[] (and the payload pl[] with it) in place by key; kb and ob
+ * (n each) are work arrays, allocated here when NULL. */
+static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long long n,
+                         unsigned long long *kb, unsigned long long *ob)
 {
     unsigned long long kmin = ~0ull, kmax = 0;
     for (long long i = 0; i < n; i++) {
@@ -845,8 +856,9 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     }
     int bits = 0;
     while (bits < 64 && ((kmax - kmin) >> bits)) bits++;
-    int npasses = (bits + RS_BITS - 1) / RS_BITS;
+    int npasses = (bits + RS_MAXBITS - 1) / RS_MAXBITS;
     if (npasses == 0) return AB_OK;
+    const int dbits = (bits + npasses - 1) / npasses;     /* equal digits, at most 14 bits */
     rs_ctx c;
     memset(&c, 0, sizeof(c));
     /* sorts running at once (several contexts replaying, e.g. a request
@@ -858,13 +870,17 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     c.nt = n < (1 << 16) ? 1 : (int) (share > RS_MAXT ? RS_MAXT : share);
     c.n = (size_t) n;
     c.npasses = npasses;
+    c.dbits = dbits;
+    c.nbins = (size_t) 1 << dbits;
     c.ka = keys;
     c.oa = pl;
-    c.kb = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
-    c.ob = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n);
-    c.hist = malloc(sizeof(size_t) * RS_BINS * (size_t) c.nt);
+    const int own = !kb || !ob;
+    c.kb = own ? (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n) : kb;
+    c.ob = own ? (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) n) : ob;
+    c.hist = (size_t *) malloc(sizeof(size_t) * c.nbins * (size_t) c.nt);
     if (!c.kb || !c.ob || !c.hist) {
-        free(c.kb); free(c.ob); free(c.hist);
+        if (own) { free(c.kb); free(c.ob); }
+        free(c.hist);
         __atomic_sub_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
         return AB_ERR_NOMEM;
     }
@@ -872,7 +888,7 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
     for (int t = 0; t < c.nt; t++) {
         c.job[t].lo = (size_t) n * t / c.nt;
         c.job[t].hi = (size_t) n * (t + 1) / c.nt;
-        c.job[t].hist = c.hist[t];
+        c.job[t].hist = c.hist + (size_t) t * c.nbins;
     }
     if (c.nt == 1) {
         for (int pass = 0; pass < npasses; pass++) {
@@ -899,61 +915,450 @@ static int radix_sort_kv(unsigned long long *keys, unsigned long long *pl, long 
         memcpy(pl, c.ob, sizeof(unsigned long long) * (size_t) n);
     }
     for (long long i = 0; i < n; i++) keys[i] += kmin;
-    free(c.kb); free(c.ob); free(c.hist);
+    if (own) { free(c.kb); free(c.ob); }
+    free(c.hist);
     __atomic_sub_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
     return AB_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* exact parallel replay of one batch of threshold crossings            */
+/* ------------------------------------------------------------------ */
+/* An insertion at rr reads and changes only candidates closer than
+ * AB_CLOSEST_R to rr, with two exceptions at the list's last node (the
+ * reference's walk stops there whatever its r).  So the batch's crossings and
+ * the list's candidates are cut into clusters: runs of occupied r bins 16
+ * wide, which puts every two points of different clusters more than
+ * AB_CLOSEST_R apart.  Each cluster replays its crossings, in the
+ * batch's order, through ab_list_insert on a list of its own candidates.
+ * While a higher cluster holds a candidate, the walk of this cluster's
+ * insertions stops at that candidate rather than at this cluster's last one;
+ * a sentinel node at r = +inf (never within AB_CLOSEST_R, never replaced)
+ * stands for it from the first crossing of the batch after which it exists.
+ * The clusters' lists are then concatenated in r order and the work-file
+ * lines written in the batch's order. */
+typedef struct {
+    long long h0, nh;                   /* crossings: idx[h0 .. h0 + nh) */
+    long long e0, ne;                   /* candidates: list positions [e0, e0 + ne) */
+    long long tail_until;               /* first crossing index with a higher candidate */
+    ab_list *out;
+} rp_cluster;
+
+typedef struct {
+    const float *pw, *sg;
+    const int *nh;
+    const double *rr, *zz, *ww;
+    const long long *idx;               /* crossings grouped by cluster, batch order within */
+    unsigned char *added;
+    const ab_cand *old;                 /* the list before the batch */
+    rp_cluster *cl;
+    const int *order;                   /* clusters, most crossings first */
+    int ncl;
+    int next;                           /* work counter */
+    int err;
+} rp_ctx;
+
+static void *rp_worker(void *arg)
+{
+    rp_ctx *c = (rp_ctx *) arg;
+    for (;;) {
+        const int k = __atomic_fetch_add(&c->next, 1, __ATOMIC_SEQ_CST);
+        if (k >= c->ncl) break;
+        rp_cluster *q = &c->cl[c->order[k]];
+        if (q->nh == 0) continue;            /* unchanged: its candidates are copied as they are */
+        ab_list *l = ab_list_new();
+        if (!l || list_reserve(l, q->ne + 2)) { __atomic_store_n(&c->err, 1, __ATOMIC_SEQ_CST); ab_list_free(l); continue; }
+        for (long long i = 0; i < q->ne; i++) {
+            l->c[i] = c->old[q->e0 + i];
+            if (i > 0 && l->c[i - 1].r > l->c[i].r) l->ninv++;
+        }
+        l->n = q->ne;
+        l->last = -1;
+        int sentinel = 0;
+        for (long long j = 0; j < q->nh; j++) {
+            const long long h = c->idx[q->h0 + j];
+            if (!sentinel && h >= q->tail_until) {
+                if (list_reserve(l, l->n + 1)) { __atomic_store_n(&c->err, 1, __ATOMIC_SEQ_CST); break; }
+                set_cand(&l->c[l->n], 0.0f, INFINITY, 0, INFINITY, 0.0, 0.0);
+                l->n++;
+                l->seg_dirty = 1;
+                sentinel = 1;
+            }
+            const int a = ab_list_insert(l, c->pw[h], c->sg[h], c->nh[h], c->rr[h], c->zz[h], c->ww[h]);
+            if (a < 0) { __atomic_store_n(&c->err, 1, __ATOMIC_SEQ_CST); break; }
+            c->added[h] = (unsigned char) a;
+        }
+        if (sentinel) l->n--;                 /* the sentinel stays the last node */
+        q->out = l;
+    }
+    return NULL;
+}
+
+/* Replays n crossings (power, sigma, harmonics, r, z, w in the reference's
+ * visit order) into l exactly as n calls of ab_list_insert would, on up to
+ * nthreads threads.  Returns AB_OK, or AB_ERR_ARG when the clusters cannot be
+ * formed (the caller then replays serially), or AB_ERR_NOMEM. */
+static int cmp_ll_desc(const void *a, const void *b)
+{
+    const long long x = *(const long long *) a, y = *(const long long *) b;
+    return (x < y) - (x > y);
+}
+
+static int replay_clusters(ab_list *l, long long n, const float *pw, const float *sg,
+                           const int *nh, const double *rr, const double *zz, const double *ww,
+                           int nthreads, int *hcl, long long *idx, unsigned char *added)
+{
+    if (n <= 0) return AB_OK;
+    /* bins of width AB_CLOSEST_R over every point */
+    double rmax = 0.0;
+    for (long long i = 0; i < n; i++) {
+        if (!(rr[i] >= 0.0) || rr[i] > 1e12) return AB_ERR_ARG;
+        if (rr[i] > rmax) rmax = rr[i];
+    }
+    for (long long i = 0; i < l->n; i++) {
+        if (!(l->c[i].r >= 0.0) || l->c[i].r > 1e12) return AB_ERR_ARG;
+        if (l->c[i].r > rmax) rmax = l->c[i].r;
+    }
+    /* bins 16 bins wide (>= AB_CLOSEST_R; r * 1/16 is exact) */
+    const long long nb = (long long) (rmax * 0.0625) + 2;
+    if (nb > (1LL << 31)) return AB_ERR_ARG;
+    int *bin = (int *) calloc((size_t) nb, sizeof(int));          /* occupied, then cluster + 1 */
+    if (!bin) return AB_ERR_NOMEM;
+    memset(added, 0, (size_t) n);
+    for (long long i = 0; i < n; i++) {
+        hcl[i] = (int) (rr[i] * 0.0625);
+        bin[hcl[i]] = 1;
+    }
+    for (long long i = 0; i < l->n; i++) bin[(long long) (l->c[i].r * 0.0625)] = 1;
+    int ncl = 0;
+    for (long long b = 0; b < nb; b++)
+        if (bin[b]) bin[b] = (b > 0 && bin[b - 1]) ? bin[b - 1] : ++ncl;
+    if (ncl >= (1 << 24)) { free(bin); return AB_ERR_ARG; }
+    rp_cluster *cl = (rp_cluster *) calloc((size_t) ncl, sizeof(rp_cluster));
+    int *order = (int *) malloc(sizeof(int) * (size_t) ncl);
+    int rc = AB_OK;
+    if (!cl || !order) { rc = AB_ERR_NOMEM; goto done; }
+    /* crossings grouped by cluster, each group in batch order */
+    for (long long i = 0; i < n; i++) {
+        hcl[i] = bin[hcl[i]] - 1;
+        cl[hcl[i]].nh++;
+    }
+    {
+        long long s = 0;
+        for (int k = 0; k < ncl; k++) { cl[k].h0 = s; s += cl[k].nh; cl[k].nh = 0; }
+    }
+    for (long long i = 0; i < n; i++) {
+        rp_cluster *q = &cl[hcl[i]];
+        idx[q->h0 + q->nh++] = i;
+    }
+    /* each cluster's candidates must be one run of list positions, in cluster order */
+    for (int k = 0; k < ncl; k++) cl[k].e0 = -1;
+    {
+        int prev = -1;
+        for (long long i = 0; i < l->n; i++) {
+            const int k = bin[(long long) (l->c[i].r * 0.0625)] - 1;
+            if (k < prev) { rc = AB_ERR_ARG; goto done; }
+            if (k != prev) {
+                if (cl[k].e0 >= 0) { rc = AB_ERR_ARG; goto done; }
+                cl[k].e0 = i;
+            }
+            cl[k].ne++;
+            prev = k;
+        }
+    }
+    for (int k = 0; k < ncl; k++) if (cl[k].e0 < 0) cl[k].e0 = 0;
+    /* the first crossing after which a higher cluster holds a candidate */
+    {
+        long long t = LLONG_MAX;
+        for (int k = ncl - 1; k >= 0; k--) {
+            cl[k].tail_until = t;
+            const long long own = cl[k].ne > 0 ? -1 : (cl[k].nh > 0 ? idx[cl[k].h0] : LLONG_MAX);
+            if (own < t) t = own;
+        }
+    }
+    /* largest clusters first */
+    {
+        long long *ord = (long long *) malloc(sizeof(long long) * (size_t) ncl);
+        if (!ord) { rc = AB_ERR_NOMEM; goto done; }
+        for (int k = 0; k < ncl; k++) ord[k] = (cl[k].nh << 24) | (long long) ((1 << 24) - 1 - k);
+        qsort(ord, (size_t) ncl, sizeof(long long), cmp_ll_desc);
+        for (int k = 0; k < ncl; k++) order[k] = (1 << 24) - 1 - (int) (ord[k] & ((1 << 24) - 1));
+        free(ord);
+    }
+    {
+        rp_ctx c = {pw, sg, nh, rr, zz, ww, idx, added, l->c, cl, order, ncl, 0, 0};
+        int nt = nthreads < 1 ? 1 : nthreads;
+        if (nt > ncl) nt = ncl;
+        if (nt > RS_MAXT) nt = RS_MAXT;
+        pthread_t th[RS_MAXT];
+        int started = 1;
+        for (int t = 1; t < nt; t++)
+            if (pthread_create(&th[t], NULL, rp_worker, &c) == 0) started++;
+            else break;
+        rp_worker(&c);
+        for (int t = 1; t < started; t++) pthread_join(th[t], NULL);
+        if (c.err) { rc = AB_ERR_NOMEM; goto done; }
+    }
+    /* concatenate the clusters' lists (or their unchanged candidates) in r order */
+    {
+        long long total = 0;
+        for (int k = 0; k < ncl; k++) total += cl[k].out ? cl[k].out->n : cl[k].ne;
+        long long cap = total > 256 ? total : 256;
+        ab_cand *nc = (ab_cand *) malloc(sizeof(ab_cand) * (size_t) cap);
+        if (!nc) { rc = AB_ERR_NOMEM; goto done; }
+        long long pos = 0;
+        for (int k = 0; k < ncl; k++) {
+            ab_list *o = cl[k].out;
+            const ab_cand *src = o ? o->c : l->c + cl[k].e0;
+            const long long m = o ? o->n : cl[k].ne;
+            if (m) memcpy(&nc[pos], src, sizeof(ab_cand) * (size_t) m);
+            pos += m;
+        }
+        free(l->c);
+        l->c = nc;
+        l->cap = cap;
+        l->n = total;
+        l->ninv = 0;
+        for (long long i = 0; i + 1 < l->n; i++) l->ninv += l->c[i].r > l->c[i + 1].r;
+        l->last = -1;
+        l->seg_dirty = 1;
+    }
+    if (l->wlog_on)
+        for (long long i = 0; i < n; i++)
+            if (added[i] && wlog_line(l, pw[i], sg[i], nh[i], rr[i], zz[i], ww[i])) {
+                rc = AB_ERR_NOMEM;
+                goto done;
+            }
+done:
+    if (cl)
+        for (int k = 0; k < ncl; k++) ab_list_free(cl[k].out);
+    free(cl); free(order); free(bin);
+    return rc;
+}
+
+int ab_list_replay_parallel(ab_list *l, long long n, const float *pw, const float *sg,
+                            const int *nh, const double *rr, const double *zz, const double *ww,
+                            int nthreads)
+{
+    if (n <= 0) return AB_OK;
+    int *hcl = (int *) malloc(sizeof(int) * (size_t) n);
+    long long *idx = (long long *) malloc(sizeof(long long) * (size_t) n);
+    unsigned char *added = (unsigned char *) malloc((size_t) n);
+    int rc = (hcl && idx && added)
+                 ? replay_clusters(l, n, pw, sg, nh, rr, zz, ww, nthreads, hcl, idx, added)
+                 : AB_ERR_NOMEM;
+    free(hcl); free(idx); free(added);
+    return rc;
+}
+
+/* Runs fn on nt jobs (job t at base + t * size), job 0 on this thread and
+ * the others on threads of their own (on this one when a thread cannot be
+ * started). */
+static void run_jobs(void *(*fn)(void *), void *base, size_t size, int nt)
+{
+    pthread_t th[RS_MAXT];
+    int ok[RS_MAXT] = {0};
+    for (int t = 1; t < nt; t++)
+        ok[t] = pthread_create(&th[t], NULL, fn, (char *) base + (size_t) t * size) == 0;
+    fn(base);
+    for (int t = 1; t < nt; t++) {
+        if (ok[t]) pthread_join(th[t], NULL);
+        else fn((char *) base + (size_t) t * size);
+    }
+}
+
+/* Packing of crossings [lo, hi): power and sigma bits into one word, the
+ * keys' used field bits and block range (pk_scan), then the keys re-packed
+ * in those widths (pk_pack). */
+typedef struct {
+    unsigned long long *keys;
+    const float *pows, *sigs;
+    unsigned long long *pl;
+    long long lo, hi;
+    unsigned long long low, bmin, bmax;
+    int wr, wz, ww, ws;
+} pk_job;
+
+static void *pk_scan(void *p)
+{
+    pk_job *j = (pk_job *) p;
+    const int bsh = AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS + AB_KEY_SBITS;
+    unsigned long long low = 0, bmin = ~0ull, bmax = 0;
+    for (long long i = j->lo; i < j->hi; i++) {
+        unsigned pb, sb = 0;
+        memcpy(&pb, &j->pows[i], 4);
+        if (j->sigs) memcpy(&sb, &j->sigs[i], 4);
+        j->pl[i] = ((unsigned long long) pb << 32) | sb;
+        const unsigned long long k = j->keys[i], b = k >> bsh;
+        low |= k & ((1ull << bsh) - 1);
+        if (b < bmin) bmin = b;
+        if (b > bmax) bmax = b;
+    }
+    j->low = low; j->bmin = bmin; j->bmax = bmax;
+    return NULL;
+}
+
+static void *pk_pack(void *p)
+{
+    pk_job *j = (pk_job *) p;
+    for (long long i = j->lo; i < j->hi; i++) {
+        const unsigned long long k = j->keys[i];
+        const unsigned long long r = k & 0xFFFF, z = (k >> AB_KEY_RBITS) & 0xFFF,
+                                 w = (k >> (AB_KEY_RBITS + AB_KEY_ZBITS)) & 0x7F,
+                                 st = (k >> (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS)) & 0x7,
+                                 b = k >> (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS + AB_KEY_SBITS);
+        j->keys[i] = (((((((b - j->bmin) << j->ws) | st) << j->ww | w) << j->wz) | z) << j->wr) | r;
+    }
+    return NULL;
+}
+
+/* The candidate fields of crossings [lo, hi) of a sorted batch (threads
+ * share the loop; each keeps its own block geometry). */
+typedef struct {
+    const ab_obs *obs;
+    unsigned long long *keys;           /* in: compact keys; out: the search's keys */
+    const unsigned long long *pl;
+    int wr, wz, ww, ws;                 /* field widths of the compact keys */
+    unsigned long long bmin;
+    float *pows, *sigs;                 /* out: the sorted powers (and sigmas) */
+    const double *startr_tab;
+    long long ntab, lo, hi;
+    float *fsg; int *fnh; double *frr, *fzz, *fww;
+    int err;
+} rf_job;
+
+static void *rf_worker(void *p)
+{
+    rf_job *j = (rf_job *) p;
+    /* 1 / 2^stage is exact, so the products equal the reference's quotients */
+    static const double inv[8] = {1.0, 0.5, 0.25, 0.125, 0.0625, 0.03125, 0.015625, 0.0078125};
+    long long cur_block = -1;
+    ab_hgeom g = {0, 0, 0, 0};
+    for (long long i = j->lo; i < j->hi; i++) {
+        unsigned long long k = j->keys[i];
+        unsigned pb = (unsigned) (j->pl[i] >> 32), sb = (unsigned) j->pl[i];
+        float pw, sg;
+        memcpy(&pw, &pb, 4);
+        memcpy(&sg, &sb, 4);
+        j->pows[i] = pw;
+        if (j->sigs) j->sigs[i] = sg;
+        const int ri = (int) (k & ((1ull << j->wr) - 1)); k >>= j->wr;
+        const int zi = (int) (k & ((1ull << j->wz) - 1)); k >>= j->wz;
+        const int wi = (int) (k & ((1ull << j->ww) - 1)); k >>= j->ww;
+        const int stage = (int) (k & ((1ull << j->ws) - 1)); k >>= j->ws;
+        const long long block = (long long) (k + j->bmin);
+        j->keys[i] = ((unsigned long long) block << (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS + AB_KEY_SBITS)) |
+                     ((unsigned long long) stage << (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS)) |
+                     ((unsigned long long) wi << (AB_KEY_RBITS + AB_KEY_ZBITS)) |
+                     ((unsigned long long) zi << AB_KEY_RBITS) | (unsigned long long) ri;
+        if (block >= j->ntab || stage > 7) { j->err = 1; return NULL; }
+        if (block != cur_block) {
+            /* the fundamental plane of the block (src/accel_utils.c:1034-1039) */
+            double startr = j->startr_tab[block];
+            g = ab_harm_geom(startr, startr + j->obs->rstep - AB_DR, 1, 1, j->obs->zlo,
+                             j->obs->wlo, j->obs->corr_uselen);
+            cur_block = block;
+        }
+        const int numharm = 1 << stage;
+        j->fsg[i] = j->sigs ? sg
+                            : (float) ab_candidate_sigma(pw, numharm,
+                                                         (double) j->obs->numindep[stage]);
+        j->fnh[i] = numharm;
+        j->frr[i] = (g.rlo + ri * (double) AB_DR) * inv[stage];
+        j->fzz[i] = (g.zlo + zi * (double) AB_DZ) * inv[stage];
+        j->fww[i] = (g.wlo + wi * (double) AB_DW) * inv[stage];
+    }
+    return NULL;
 }
 
 /* Device hits carry (key, power, sigma); the key orders them as the
  * reference visits them (block, stage, w, z, r).  Sorts them (keys, pows and
  * sigs are reordered in place) and replays search_ffdotpows' per-hit work
  * (src/accel_utils.c:1430-1442).  sigs may be NULL, in which case
- * candidate_sigma is evaluated here. */
+ * candidate_sigma is evaluated here.  Batches of AB_REPLAY_PARALLEL_MIN
+ * crossings or more fill their candidate fields and replay on several threads
+ * (ab_list_replay_parallel), into scratch the list keeps for its next batch. */
 int ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows, float *sigs,
                    long long nhits, const double *startr_tab, long long ntab, ab_list *l)
 {
     if (nhits <= 0) return AB_OK;
-    unsigned long long *pl = (unsigned long long *) malloc(sizeof(unsigned long long) * (size_t) nhits);
-    if (!pl) return AB_ERR_NOMEM;
-    for (long long i = 0; i < nhits; i++) {
-        unsigned pb, sb = 0;
-        memcpy(&pb, &pows[i], 4);
-        if (sigs) memcpy(&sb, &sigs[i], 4);
-        pl[i] = ((unsigned long long) pb << 32) | sb;
+    const size_t n = (size_t) nhits;
+    /* pl, kb, ob (8 B), fsg, fnh, hcl (4 B), frr, fzz, fww (8 B), idx (8 B), added (1 B) */
+    const size_t need = n * (8 * 3 + 4 * 3 + 8 * 3 + 8 + 1) + 64;
+    if (need > l->scr_cap) {
+        /* 2 MiB-aligned and marked for huge pages: a batch of millions of
+           crossings touches hundreds of MB once, and 4 KiB page faults on it
+           would cost more than the replay */
+        void *p = NULL;
+        const size_t cap = (need + ((size_t) 2 << 20) - 1) & ~(((size_t) 2 << 20) - 1);
+        if (posix_memalign(&p, (size_t) 2 << 20, cap)) return AB_ERR_NOMEM;
+#ifdef MADV_HUGEPAGE
+        madvise(p, cap, MADV_HUGEPAGE);
+#endif
+        free(l->scr);
+        l->scr = p;
+        l->scr_cap = cap;
     }
-    int rc = radix_sort_kv(keys, pl, nhits);
-    if (rc) { free(pl); return rc; }
-    long long cur_block = -1;
-    ab_hgeom g = {0, 0, 0, 0};
-    for (long long i = 0; i < nhits; i++) {
-        unsigned long long k = keys[i];
-        unsigned pb = (unsigned) (pl[i] >> 32), sb = (unsigned) pl[i];
-        float pw, sg;
-        memcpy(&pw, &pb, 4);
-        memcpy(&sg, &sb, 4);
-        pows[i] = pw;
-        if (sigs) sigs[i] = sg;
-        int ri = (int) (k & 0xFFFF); k >>= AB_KEY_RBITS;
-        int zi = (int) (k & 0xFFF); k >>= AB_KEY_ZBITS;
-        int wi = (int) (k & 0x7F); k >>= AB_KEY_WBITS;
-        int stage = (int) (k & 0x7); k >>= AB_KEY_SBITS;
-        long long block = (long long) k;
-        if (block >= ntab) { free(pl); return AB_ERR_ARG; }
-        if (block != cur_block) {
-            /* the fundamental plane of the block (src/accel_utils.c:1034-1039) */
-            double startr = startr_tab[block];
-            g = ab_harm_geom(startr, startr + obs->rstep - AB_DR, 1, 1, obs->zlo, obs->wlo,
-                             obs->corr_uselen);
-            cur_block = block;
-        }
-        int numharm = 1 << stage;
-        float sig = sigs ? sg : (float) ab_candidate_sigma(pw, numharm, (double) obs->numindep[stage]);
-        double rr = (g.rlo + ri * (double) AB_DR) / (double) numharm;
-        double zz = (g.zlo + zi * (double) AB_DZ) / (double) numharm;
-        double ww = (g.wlo + wi * (double) AB_DW) / (double) numharm;
-        if (ab_list_insert(l, pw, sig, numharm, rr, zz, ww) < 0) { free(pl); return AB_ERR_NOMEM; }
+    unsigned long long *pl = (unsigned long long *) l->scr;
+    unsigned long long *kb = pl + n, *ob = kb + n;
+    double *frr = (double *) (ob + n), *fzz = frr + n, *fww = fzz + n;
+    long long *idx = (long long *) (fww + n);
+    float *fsg = (float *) (idx + n);
+    int *fnh = (int *) (fsg + n), *hcl = fnh + n;
+    unsigned char *added = (unsigned char *) (hcl + n);
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    const int active = __atomic_add_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
+    long share = (ncpu < 1 ? 1 : ncpu) / active;
+    __atomic_sub_fetch(&g_active_sorts, 1, __ATOMIC_SEQ_CST);
+    if (share < 1) share = 1;
+    const int big = nhits >= AB_REPLAY_PARALLEL_MIN;
+    int nt = big ? (int) (share > RS_MAXT ? RS_MAXT : share) : 1;
+    /* the keys re-packed in the field widths this batch uses (the same
+       order, fewer radix passes) */
+    pk_job pk[RS_MAXT];
+    for (int t = 0; t < nt; t++) {
+        pk_job j = {keys, pows, sigs, pl, nhits * t / nt, nhits * (t + 1) / nt, 0, ~0ull, 0,
+                    0, 0, 0, 0};
+        pk[t] = j;
     }
-    free(pl);
+    run_jobs(pk_scan, pk, sizeof(pk_job), nt);
+    unsigned long long low = 0, bmin = ~0ull, bmax = 0;
+    for (int t = 0; t < nt; t++) {
+        low |= pk[t].low;
+        if (pk[t].bmin < bmin) bmin = pk[t].bmin;
+        if (pk[t].bmax > bmax) bmax = pk[t].bmax;
+    }
+    int wr = 0, wz = 0, ww = 0, ws = 0;
+    while (wr < 16 && ((low & 0xFFFF) >> wr)) wr++;
+    while (wz < 12 && (((low >> AB_KEY_RBITS) & 0xFFF) >> wz)) wz++;
+    while (ww < 7 && (((low >> (AB_KEY_RBITS + AB_KEY_ZBITS)) & 0x7F) >> ww)) ww++;
+    while (ws < 3 && (((low >> (AB_KEY_RBITS + AB_KEY_ZBITS + AB_KEY_WBITS)) & 0x7) >> ws)) ws++;
+    for (int t = 0; t < nt; t++) {
+        pk[t].bmin = bmin;
+        pk[t].wr = wr; pk[t].wz = wz; pk[t].ww = ww; pk[t].ws = ws;
+    }
+    run_jobs(pk_pack, pk, sizeof(pk_job), nt);
+    (void) bmax;
+    int rc = radix_sort_kv(keys, pl, nhits, kb, ob);
+    if (rc) return rc;
+    rf_job jobs[RS_MAXT];
+    for (int t = 0; t < nt; t++) {
+        rf_job j = {obs, keys, pl, wr, wz, ww, ws, bmin, pows, sigs, startr_tab, ntab,
+                    nhits * t / nt, nhits * (t + 1) / nt, fsg, fnh, frr, fzz, fww, 0};
+        jobs[t] = j;
+    }
+    run_jobs(rf_worker, jobs, sizeof(rf_job), nt);
+    for (int t = 0; t < nt; t++)
+        if (jobs[t].err) return AB_ERR_ARG;
+    if (big) {
+        rc = replay_clusters(l, nhits, pows, fsg, fnh, frr, fzz, fww, (int) share, hcl, idx,
+                             added);
+        if (rc != AB_ERR_ARG) return rc;
+    }
+    /* small batches, or crossings that cannot be cut into clusters */
+    for (long long i = 0; i < nhits; i++)
+        if (ab_list_insert(l, pows[i], fsg[i], fnh[i], frr[i], fzz[i], fww[i]) < 0)
+            return AB_ERR_NOMEM;
     return AB_OK;
 }
 

@@ -85,6 +85,12 @@ long long ab_list_get(const ab_list *l, ab_cand *out, long long maxout);
  * observation's length, s) for every candidate an insertion adds */
 void      ab_list_worklog(ab_list *l, int on, double T);
 const char *ab_list_worklog_text(const ab_list *l, size_t *len);
+/* Batches of at least this many crossings are replayed by clusters of r on
+ * several threads (ab_list_replay_parallel), with the serial result. */
+#define AB_REPLAY_PARALLEL_MIN 32768
+int       ab_list_replay_parallel(ab_list *l, long long n, const float *pw, const float *sg,
+                                  const int *nh, const double *rr, const double *zz,
+                                  const double *ww, int nthreads);
 int       ab_replay_hits(const ab_obs *obs, unsigned long long *keys, float *pows,
                          float *sigs, long long nhits, const double *startr_tab,
                          long long ntab, ab_list *l);
