@@ -708,6 +708,14 @@ __device__ __forceinline__ void flush_hits(unsigned mask, const float *sums, lon
 // Latency-bound gathers: the register cap keeps 6 / 4 / 3 CTAs per SM at
 // 3-4 / 5 / 6 stages.
 constexpr int harmsum_min_ctas(int stages) { return stages <= 2 ? 1 : stages <= 4 ? 6 : (stages == 5 ? 4 : 3); }
+// The in-memory sum, up to 4 stages, keeps each subharmonic's last value in a
+// register and reads it again only when the subharmonic's row changes with z
+// (a subharmonic f keeps its row for ~1/f consecutive z rows); 5 CTAs per SM
+// leave room for it.  At 5 and 6 stages the 15 / 31 extra registers would go
+// to the stack (measured 2x slower), and in the standard-mode sum the same
+// change measured slower (jerk search 93.5 -> 111 ms), so those read every
+// value.
+constexpr int inmem_min_ctas(int stages) { return stages <= 2 ? 1 : stages <= 4 ? 5 : (stages == 5 ? 4 : 3); }
 
 template <int STAGES>
 __global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_std(const ab_bank *banks, SearchConsts sc,
@@ -830,12 +838,16 @@ cudaError_t launch_harmsum_std(const ab_bank *banks_dev, const SearchConsts &sc,
 // In-memory mode: fundamental and subharmonic powers come from the full
 // f-fdot plane (inmem_add_ffdotpows).  CTA = (block, z tile, r cells).
 template <int STAGES>
-__global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
+__global__ void __launch_bounds__(256, inmem_min_ctas(STAGES)) k_harmsum_inmem(SearchConsts sc, BlockBatch bb,
                                                        const float *plane, HitBuf hb, float *dbg,
                                                        int dbg_bi)
 {
     constexpr int NSUB = (1 << (STAGES - 1)) - 1;
     __shared__ int s_zrow[NSUB > 0 ? NSUB : 1][HS_ZT];
+    // bit h: subharmonic h reads another row than at the previous z row
+    // (subharmonic f keeps its row for ~1/f consecutive z rows; the value read
+    // there is kept in a register instead of read again)
+    __shared__ unsigned s_new[HS_ZT];
     const int nzt = (sc.numz + HS_ZT - 1) / HS_ZT;
     const int zt = blockIdx.x % nzt, bi = blockIdx.x / nzt;
     const int r = blockIdx.y * HS_RT + threadIdx.x, z0 = zt * HS_ZT;
@@ -862,14 +874,28 @@ __global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_inmem
             }
     }
     __syncthreads();
+    if (STAGES <= 4) {
+        for (int zz = threadIdx.x; zz < HS_ZT; zz += blockDim.x) {
+            unsigned m = 0;
+            for (int h = 0; h < NSUB; h++)
+                if (zz == 0 || s_zrow[h][zz] != s_zrow[h][zz - 1]) m |= 1u << h;
+            s_new[zz] = m;
+        }
+        __syncthreads();
+    }
     float pc[STAGES];
 #pragma unroll
     for (int s = 0; s < STAGES; s++) pc[s] = sc.powcut[s];
     const long long block = bb.block0 + bi;
     const int zend = min(z0 + HS_ZT, sc.numz);
     const bool dump = dbg && bi == dbg_bi && ok;
+    constexpr bool REUSE = STAGES <= 4;
+    float sv[REUSE && NSUB > 0 ? NSUB : 1];
+#pragma unroll
+    for (int h = 0; h < (REUSE ? NSUB : 1); h++) sv[h] = 0.f;
     for (int z = z0; z < zend; z++) {
         const int zz = z - z0;
+        const unsigned nm = STAGES <= 4 ? s_new[zz] : 0u;
         float sums[STAGES];
         float sum = ok ? plane[(long long) z * sc.rlen + (long long) rlo * AB_RDR + r] : 0.f;
         sums[0] = sum;
@@ -878,8 +904,15 @@ __global__ void __launch_bounds__(256, harmsum_min_ctas(STAGES)) k_harmsum_inmem
 #pragma unroll
         for (int s = 1; s < STAGES; s++) {
 #pragma unroll
-            for (int j = 0; j < (1 << (s - 1)); j++, h++)
-                if (ok) sum += plane[(long long) s_zrow[h][zz] * sc.rlen + rind[h]];
+            for (int j = 0; j < (1 << (s - 1)); j++, h++) {
+                if constexpr (REUSE) {
+                    if (ok && ((nm >> h) & 1u))
+                        sv[h] = plane[(long long) s_zrow[h][zz] * sc.rlen + rind[h]];
+                    if (ok) sum += sv[h];
+                } else {
+                    if (ok) sum += plane[(long long) s_zrow[h][zz] * sc.rlen + rind[h]];
+                }
+            }
             sums[s] = sum;
             if (ok && !(sum <= pc[s])) mask |= 1u << s;
         }
