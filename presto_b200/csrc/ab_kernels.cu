@@ -522,6 +522,7 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
     __shared__ long long s_off[AB_MAX_SBM];
     __shared__ float s_scale[AB_MAX_SBM];
     __shared__ int s_c0[AB_MAX_SBM], s_lim[AB_MAX_SBM];
+    __shared__ int s_sblim;                             // superblock: columns < s_sblim may be kept
     float2 *xs = fsm;                                   // [L/2]
     const CorrItem it = items[blockIdx.x];              // it.bi: transform unit
     const ab_bank b = banks[it.bank];
@@ -560,6 +561,11 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
             s_scale[j] = (float) (r * r);
         }
         __syncthreads();
+        if (threadIdx.x == 0) {
+            int e = 0;
+            for (int j = 0; j < mb; j++) e = max(e, s_c0[j] + s_lim[j]);
+            s_sblim = e;
+        }
         for (int kk = threadIdx.x; kk < L; kk += blockDim.x) {
             unsigned code = 0xFFu;
             for (int j = 0; j < mb; j++)
@@ -589,9 +595,20 @@ __global__ void __launch_bounds__(FftShape<L>::CTA, FftShape<L>::MINB) k_corr(co
         }
         fft_run<L, 1>(v, sm, t, tw, sm2);
         if (valid && sb) {
+            // outputs m of this warp's lanes that can land in a block's
+            // columns [0, s_sblim): a warp spans 32 consecutive t of one
+            // transform, so the range is uniform and the rest is skipped
+            // (superblock outputs cost a column lookup and one or two scaled
+            // stores each; the single-block stores are cheaper than the test,
+            // measured; not at 8192 points, where the bounds would spill)
+            constexpr bool PRUNE = L <= 4096;
+            const int tw0 = t & ~31;
             const long long row = (long long) tl * b.numrs_max;
+            const int m_lo = PRUNE ? max(0, (offset - tw0 - 31 + SH::NT - 1) / SH::NT) : 0;
+            const int m_hi = PRUNE ? (s_sblim + offset - tw0 - 1) / SH::NT : 15;
 #pragma unroll
             for (int m = 0; m < 16; m++) {
+                if (m < m_lo || m > m_hi) continue;
                 const int kk = t + SH::NT * m - offset;
                 if (kk >= 0) {
                     const unsigned code = cmap[kk];
