@@ -1468,8 +1468,8 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
     tick(ctx, 7, false);
     if (le != cudaSuccess)
         return fail(ctx, AB_ERR_ARG, "dedispersion launch refused (%s): a subband's channel delays "
-                    "or a group of 8 DMs' subband offsets spread too far for the "
-                    "shared-memory tiles (200 KB)",
+                    "or a group of 8 consecutive DMs' subband offsets spread too far "
+                    "for the shared-memory tiles (200 KB)",
                     cudaGetErrorString(le));
     ctx->launches += 2;
     if (!out_on_device)
