@@ -490,6 +490,12 @@ def run_ours(args):
                                        workers=args.workers),
                           pool_compare("served", 2 * args.requests, rate=args.rate,
                                        workers=args.workers, corr="tc16")]
+    if rank == 0 and world == 1 and not args.no_pipeline:
+        # filterbank spectra to candidates over 32 DM trials (one pass each way)
+        try:
+            line["pipeline"] = pipeline_measure(1)
+        except Exception as e:          # a side measurement: the line stands without it
+            line["pipeline"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -710,13 +716,20 @@ def run_dedisp_mode(args):
 
 
 def run_pipeline_mode(args):
-    """--mode pipeline: float filterbank spectra (1024 channels x 2^20 samples of
-    64 us, 1400 MHz + 256 MHz, a pulsar at DM 150, 0.05 sigma per channel) to
-    candidates: 32 DM trials
-    over 0-300 searched with the smaller search's parameters (zmax 200,
-    numharm 8), all on the device (ab_search_dedispersed), against the same
-    steps chained through host arrays.  Wall-clock per step; the spectra start
-    in host memory in both."""
+    """--mode pipeline: pipeline_measure as a line of its own."""
+    line = pipeline_measure(max(1, args.steps))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def pipeline_measure(steps):
+    """Float filterbank spectra (1024 channels x 2^20 samples of 64 us,
+    1400 MHz + 256 MHz, a pulsar at DM 150, 0.05 sigma per channel) to
+    candidates: 32 DM trials over 0-300 searched with the smaller search's
+    parameters (zmax 200, numharm 8), all on the device
+    (ab_search_dedispersed), against the same steps chained through host
+    arrays.  Wall-clock per step; the spectra start in host memory in both,
+    then once more already in device memory."""
     import presto_b200 as pb
     nspec, nchan, nsub, ndm, dt = 1 << 20, 1024, 64, 32, 64e-6
     import torch
@@ -736,7 +749,7 @@ def run_pipeline_mode(args):
         obs = pb.obs_init(pb.make_params(n, dt, n // 2, zmax=200, numharm=8, sigma=2.0))
         ctx.search_dedispersed(X, 1400.0, 0.25, dt, nsub, dms, obs)          # warm-up
         dev_ms, host_ms, ncand = [], [], 0
-        for _ in range(max(1, args.steps)):
+        for _ in range(steps):
             t0 = time.perf_counter()
             res = ctx.search_dedispersed(X, 1400.0, 0.25, dt, nsub, dms, obs)
             dev_ms.append((time.perf_counter() - t0) * 1e3)
@@ -752,7 +765,7 @@ def run_pipeline_mode(args):
         res_dev_ms = []
         ctx.reset_kernel_times()
         ctx.set_profiling(True)
-        for _ in range(max(1, args.steps)):
+        for _ in range(steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             rd = ctx.search_dedispersed(None, 1400.0, 0.25, dt, nsub, dms, obs,
@@ -783,8 +796,7 @@ def run_pipeline_mode(args):
             "what": "ab_search_dedispersed: spectra in host memory, dedispersion, then per trial "
                     "realfft + deredden + search on the device; host_chain = the same steps with "
                     "the trials and spectra through host arrays (identical candidates)"}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_pool_mode(args):
@@ -820,6 +832,8 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
     ap.add_argument("--dd-nspec", type=int, default=1 << 20,
                     help="dedisperse mode: spectra (of 1024 channels) to dedisperse")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="leave the filterbank-to-candidates pipeline out of the default line")
     ap.add_argument("--no-pool", action="store_true",
                     help="leave the batched / served comparison out of the default line")
     args = ap.parse_args()
