@@ -675,15 +675,22 @@ struct Replayer {
         }
     }
     // the context's copy of the search's hits (ab_last_hits); bounded: past
-    // 2^24 only the latest batches are kept
-    static void keep_hits(ab_ctx *ctx, const std::vector<unsigned long long> &k,
-                          const std::vector<float> &p, const std::vector<float> &sg)
+    // 2^24 only the latest batches are kept.  The batch's vectors are taken
+    // over when the copy is empty (the common case: one batch holds them all).
+    static void keep_hits(ab_ctx *ctx, std::vector<unsigned long long> &k, std::vector<float> &p,
+                          std::vector<float> &sg)
     {
         if (ctx->hkeys.size() + k.size() > (size_t) 1 << 24) {
             ctx->hkeys.clear();
             ctx->hpows.clear();
             ctx->hsigs.clear();
             ctx->hits_truncated = true;
+        }
+        if (ctx->hkeys.empty()) {
+            ctx->hkeys.swap(k);
+            ctx->hpows.swap(p);
+            ctx->hsigs.swap(sg);
+            return;
         }
         ctx->hkeys.insert(ctx->hkeys.end(), k.begin(), k.end());
         ctx->hpows.insert(ctx->hpows.end(), p.begin(), p.end());
