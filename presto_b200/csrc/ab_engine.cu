@@ -96,6 +96,7 @@ struct ab_ctx {
     DevBuf<float2> blu_a, blu_b;            // Bluestein work and chirp-kernel transform
     DevBuf<float> dd_x, dd_sub, dd_out;     // dedispersion: spectra, subbands, DM trials
     DevBuf<float2> dd_fft;                  // spectrum of one DM trial (ab_search_dedispersed)
+    DevBuf<int> bidx;                       // bank lists of the grouped preparation launches
     DevBuf<int> dd_cd, dd_off;              // dedispersion delays
     long long blu_M = 0;                    // the length blu_b was built for
     DevBuf<int2> dered_blocks;
@@ -396,10 +397,17 @@ static int run_prep(ab_ctx *ctx, const SearchConsts &sc, const BlockBatch &bb, c
                     int bank_lo, int bank_hi)
 {
     tick(ctx, 1, true);
+    CK(ctx->bidx.ensure((size_t) std::max(1, bank_hi - bank_lo)));
     cudaError_t e = launch_prep(ctx->dbanks.p + bank_lo, ctx->bs.b + bank_lo, bank_hi - bank_lo,
-                                sc, bb, fft, ctx->xhat.p, ctx->bs.xhat_per_block, ctx->stream);
+                                sc, bb, fft, ctx->xhat.p, ctx->bs.xhat_per_block, ctx->bidx.p,
+                                ctx->stream);
     tick(ctx, 1, false);
-    ctx->launches += bank_hi - bank_lo;
+    {
+        // one launch per distinct transform length
+        unsigned seen = 0;
+        for (int k = bank_lo; k < bank_hi; k++) seen |= 1u << (31 - __builtin_clz((unsigned) ctx->bs.b[k].L));
+        ctx->launches += __builtin_popcount(seen);
+    }
     if (e != cudaSuccess)
         return fail(ctx, AB_ERR_CUDA, "prep launch failed: %s", cudaGetErrorString(e));
     return AB_OK;
@@ -932,7 +940,9 @@ static int search_core(ab_ctx *ctx, const ab_obs *obs, const float2 *dfft, long 
             if (rc) return rc;
         } else {
             tick(ctx, 1, true);
-            cudaError_t en = launch_norms(ctx->dbanks.p, bs.b, bs.nbanks, sc, bb, dfft, ctx->stream);
+            CK(ctx->bidx.ensure((size_t) std::max(1, bs.nbanks)));
+            cudaError_t en = launch_norms(ctx->dbanks.p, bs.b, bs.nbanks, sc, bb, dfft, ctx->bidx.p,
+                                          ctx->stream);
             tick(ctx, 1, false);
             ctx->launches++;
             if (en != cudaSuccess)
@@ -1085,6 +1095,7 @@ void ab_ctx_destroy(ab_ctx *ctx)
     ctx->dd_sub.release();
     ctx->dd_out.release();
     ctx->dd_fft.release();
+    ctx->bidx.release();
     ctx->dd_cd.release();
     ctx->dd_off.release();
     ctx->dered_blocks.release();

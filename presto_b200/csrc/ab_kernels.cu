@@ -20,6 +20,9 @@
 #include "ab_fft.cuh"
 #include "ab_index.h"
 #include "ab_kernels.h"
+
+#include <algorithm>
+#include <vector>
 #include "ab_norm.cuh"
 #include "ab_resp.cuh"
 #include "ab_select.cuh"
@@ -318,20 +321,24 @@ __device__ double block_norm(const SearchConsts &sc, long long lobin, int numdat
     return *s_norm;
 }
 
+// blockIdx.x: bank (bidx[blockIdx.x] when a list is given), blockIdx.y:
+// transform unit; rows past a bank's units (a launch covers banks of one
+// transform length with different superblock heights) return at once
 template <int LH>
-__global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
-                                              const float2 *fft, float2 *xhat,
+__global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, const int *bidx, SearchConsts sc,
+                                              BlockBatch bb, const float2 *fft, float2 *xhat,
                                               long long xhat_per_block)
 {
     using SH = FftShape<LH>;
     extern __shared__ float2 fsm[];
     __shared__ double s_norm;
-    const int bank = blockIdx.x, bi = blockIdx.y;      // bi: transform unit
+    const int bank = bidx ? bidx[blockIdx.x] : blockIdx.x, bi = blockIdx.y;
     const ab_bank b = banks[bank];
     // superblock: the window of its first block, the normalisation of that
     // block (computed by k_norms), the data unrepeated over L/2 bins
     const bool sb = sc.superblocks && b.sbm > 1;
     const int blk = sb ? bi * b.sbm : bi;
+    if (blk >= bb.nblk) return;
     ab_hgeom g;
     block_geom(sc, b, bb.startr[blk], &g);
     const long long lobin = g.rlo - b.hw0;
@@ -379,36 +386,79 @@ __global__ void __launch_bounds__(256) k_prep(const ab_bank *banks, SearchConsts
     }
 }
 
-cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
-                        const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
-                        float2 *xhat, long long xhat_per_block, cudaStream_t st)
+static size_t prep_smem(const ab_bank &b)
 {
-    // one launch per distinct L (banks of equal L are contiguous or not; launch per bank)
-    for (int k = 0; k < nbanks; k++) {
-        const ab_bank &b = banks_host[k];
-        int numdata = b.fftlen_ref / AB_NUMBETWEEN, n2 = 1;
-        while (n2 < numdata) n2 <<= 1;
-        int LH = b.L / 2;
-        size_t fftsm = (size_t) 256 * 16 * 17 / 16 * sizeof(float2);  // G * SMEM float2
-        size_t smem = fftsm > (size_t) n2 * sizeof(float) ? fftsm : (size_t) n2 * sizeof(float);
-        dim3 grid(1, corr_units(b, sc, bb.nblk));
-        // launch a 1-bank grid by offsetting the bank pointer
-        const ab_bank *bp = banks_dev + k;
-        switch (LH) {
+    int numdata = b.fftlen_ref / AB_NUMBETWEEN, n2 = 1;
+    while (n2 < numdata) n2 <<= 1;
+    const size_t fftsm = (size_t) 256 * 16 * 17 / 16 * sizeof(float2);   // G * SMEM float2
+    return fftsm > (size_t) n2 * sizeof(float) ? fftsm : (size_t) n2 * sizeof(float);
+}
+
+static cudaError_t launch_prep_one(int LH, dim3 grid, size_t smem, const ab_bank *bp, const int *bidx,
+                                   const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                                   float2 *xhat, long long xhat_per_block, cudaStream_t st)
+{
+    switch (LH) {
 #define AB_PREP_CASE(N)                                                                       \
     case N:                                                                                   \
         cudaFuncSetAttribute(k_prep<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
-        k_prep<N><<<grid, 256, smem, st>>>(bp, sc, bb, fft, xhat, xhat_per_block);           \
+        k_prep<N><<<grid, 256, smem, st>>>(bp, bidx, sc, bb, fft, xhat, xhat_per_block);      \
         break;
-            AB_PREP_CASE(256)
-            AB_PREP_CASE(512)
-            AB_PREP_CASE(1024)
-            AB_PREP_CASE(2048)
-            AB_PREP_CASE(4096)
+        AB_PREP_CASE(256)
+        AB_PREP_CASE(512)
+        AB_PREP_CASE(1024)
+        AB_PREP_CASE(2048)
+        AB_PREP_CASE(4096)
 #undef AB_PREP_CASE
-            default:
-                return cudaErrorInvalidValue;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
+                        const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
+                        float2 *xhat, long long xhat_per_block, int *bidx, cudaStream_t st)
+{
+    cudaError_t e;
+    if (!bidx) {
+        // one launch per bank (a 1-bank grid by offsetting the bank pointer)
+        for (int k = 0; k < nbanks; k++) {
+            const ab_bank &b = banks_host[k];
+            e = launch_prep_one(b.L / 2, dim3(1, corr_units(b, sc, bb.nblk)), prep_smem(b),
+                                banks_dev + k, nullptr, sc, bb, fft, xhat, xhat_per_block, st);
+            if (e != cudaSuccess) return e;
         }
+        return cudaGetLastError();
+    }
+    // one launch per transform length over the banks listed in bidx: the
+    // separate launches of a batch's banks are small grids that leave most of
+    // the GPU idle and run one after another
+    std::vector<int> order;
+    std::vector<int> starts;
+    for (int LH = 256; LH <= 4096; LH *= 2) {
+        starts.push_back((int) order.size());
+        for (int k = 0; k < nbanks; k++)
+            if (banks_host[k].L / 2 == LH) order.push_back(k);
+    }
+    starts.push_back((int) order.size());
+    if ((int) order.size() != nbanks) return cudaErrorInvalidValue;
+    e = cudaMemcpyAsync(bidx, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    int gi = 0;
+    for (int LH = 256; LH <= 4096; LH *= 2, gi++) {
+        const int lo = starts[gi], hi = starts[gi + 1];
+        if (hi == lo) continue;
+        int units = 0;
+        size_t smem = 0;
+        for (int i = lo; i < hi; i++) {
+            const ab_bank &b = banks_host[order[i]];
+            units = std::max(units, corr_units(b, sc, bb.nblk));
+            smem = std::max(smem, prep_smem(b));
+        }
+        e = launch_prep_one(LH, dim3(hi - lo, units), smem, banks_dev, bidx + lo, sc, bb, fft,
+                            xhat, xhat_per_block, st);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }
@@ -416,12 +466,12 @@ cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int
 // Block normalisations of one superblock bank: sc.norms[block * nbanks +
 // bank index] = 1/sqrt(median/ln 2) over the block's own window of
 // fftlen_ref / 2 bins (src/accel_utils.c:1079-1099).
-__global__ void __launch_bounds__(256) k_norms(const ab_bank *banks, SearchConsts sc, BlockBatch bb,
-                                               const float2 *fft, double *norms)
+__global__ void __launch_bounds__(256) k_norms(const ab_bank *banks, const int *bidx, SearchConsts sc,
+                                               BlockBatch bb, const float2 *fft, double *norms)
 {
     extern __shared__ float2 fsm[];
     __shared__ double s_norm;
-    const ab_bank b = banks[blockIdx.x];
+    const ab_bank b = banks[bidx[blockIdx.x]];
     const int bi = blockIdx.y;
     ab_hgeom g;
     block_geom(sc, b, bb.startr[bi], &g);
@@ -432,20 +482,28 @@ __global__ void __launch_bounds__(256) k_norms(const ab_bank *banks, SearchConst
 
 cudaError_t launch_norms(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
                          const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
-                         cudaStream_t st)
+                         int *bidx, cudaStream_t st)
 {
     if (!sc.superblocks) return cudaSuccess;
-    cudaFuncSetAttribute(k_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    // every superblock bank of the batch in one launch
+    std::vector<int> list;
+    size_t smem = 0;
     for (int k = 0; k < nbanks; k++) {
         const ab_bank &b = banks_host[k];
         if (b.sbm <= 1) continue;
         int numdata = b.fftlen_ref / AB_NUMBETWEEN, n2 = 1;
         while (n2 < numdata) n2 <<= 1;
-        size_t smem = (size_t) n2 * sizeof(float);
-        if (smem > 200 * 1024) return cudaErrorInvalidValue;
-        k_norms<<<dim3(1, bb.nblk), 256, smem, st>>>(banks_dev + k, sc, bb, fft,
-                                                       const_cast<double *>(sc.norms));
+        smem = std::max(smem, (size_t) n2 * sizeof(float));
+        list.push_back(k);
     }
+    if (list.empty()) return cudaSuccess;
+    if (smem > 200 * 1024 || !bidx) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemcpyAsync(bidx, list.data(), sizeof(int) * list.size(),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    cudaFuncSetAttribute(k_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    k_norms<<<dim3((unsigned) list.size(), bb.nblk), 256, smem, st>>>(
+        banks_dev, bidx, sc, bb, fft, const_cast<double *>(sc.norms));
     return cudaGetLastError();
 }
 

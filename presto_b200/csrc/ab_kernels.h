@@ -55,15 +55,18 @@ cudaError_t launch_response(double roffset, int numbetween, double z, double w, 
                             float2 *out, const double2 *tw_chirp_all, int chirp_max_log2,
                             double2 *scratch, cudaStream_t st);
 
-// kernel set (b): spectrum preparation and correlation
+// kernel set (b): spectrum preparation and correlation.  bidx (device, room
+// for nbanks ints): banks of one transform length go out in one launch,
+// listed there; NULL: one launch per bank (no upload)
 cudaError_t launch_prep(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
                         const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
-                        float2 *xhat, long long xhat_per_block, cudaStream_t st);
+                        float2 *xhat, long long xhat_per_block, int *bidx, cudaStream_t st);
 // per-block normalisations of the superblock banks among banks_host[0..nbanks)
-// into sc.norms[block * sc.nbanks + bank index]
+// into sc.norms[block * sc.nbanks + bank index], in one launch listing them in
+// bidx (device, room for nbanks ints)
 cudaError_t launch_norms(const ab_bank *banks_dev, const ab_bank *banks_host, int nbanks,
                          const SearchConsts &sc, const BlockBatch &bb, const float2 *fft,
-                         cudaStream_t st);
+                         int *bidx, cudaStream_t st);
 // transform units (superblocks, or blocks) of a bank in a batch of nblk blocks
 inline int corr_units(const ab_bank &b, const SearchConsts &sc, int nblk)
 {

@@ -201,7 +201,7 @@ extern "C" int ab_fderivs_vol_noalloc(const ab_obs *obs, int numharm, int harmnu
     sc.norm_type = obs->norm_type;
     BlockBatch bb{d_start, 0, 1, 0};
     if (launch_prep(d_desc, &b, 1, sc, bb, reinterpret_cast<const float2 *>(d_fft), d_xhat,
-                    b.L / 2, st) != cudaSuccess)
+                    b.L / 2, nullptr, st) != cudaSuccess)
         return AB_ERR_CUDA;
     if (launch_corr(b.L, d_desc, sc, bb, d_items, nitems, d_xhat, b.L / 2,
                     reinterpret_cast<const float2 *>(d_templates), d_powers, 0, nullptr,
