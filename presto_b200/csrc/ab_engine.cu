@@ -133,6 +133,10 @@ struct ab_ctx {
     DevBuf<float> sigs, sigs_x[kHitSets - 1];
     std::vector<float> hsigs;
     unsigned *hcount = nullptr;              // pinned [kHitSets]
+    // pinned staging of large uploads from pageable host memory (h2d_staged)
+    static constexpr size_t kStage = (size_t) 64 << 20;
+    char *stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_done[2] = {};
     cudaEvent_t batch_done[kHitSets] = {};
     cudaStream_t cstream = nullptr;          // device->host copies of hits
     unsigned int hit_cap = 1u << 22;
@@ -1017,6 +1021,55 @@ static int check_device_error(ab_ctx *ctx)
 // 8-byte aligned; a misaligned pointer is refused instead of faulting.
 static bool misaligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) != 0; }
 
+// Upload of `bytes` from pageable host memory on the context's stream.  A
+// pageable copy is staged by the driver on one host thread (~11 GB/s); copies
+// of 256 MB or more (filterbank spectra) go instead through two pinned
+// buffers that several host threads fill in parallel, each buffer's transfer
+// overlapping the filling of the other.  The call returns when the source has
+// been read.
+static int h2d_staged(ab_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    const size_t chunk = ab_ctx::kStage;
+    if (bytes < 4 * chunk) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return AB_OK;
+    }
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->stage[i]) CK(cudaHostAlloc((void **) &ctx->stage[i], chunk, cudaHostAllocDefault));
+        if (!ctx->stage_done[i])
+            CK(cudaEventCreateWithFlags(&ctx->stage_done[i], cudaEventDisableTiming));
+    }
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthr = (int) std::max(1u, std::min(8u, hw / 2));
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    size_t off = 0;
+    for (int k = 0; off < bytes; k++) {
+        const size_t n = std::min(chunk, bytes - off);
+        char *buf = ctx->stage[k & 1];
+        // the buffer's last transfer (of this call or an earlier one) is done
+        CK(cudaEventSynchronize(ctx->stage_done[k & 1]));
+        std::vector<std::thread> th;
+        int started = 1;
+        try {
+            for (int t = 1; t < nthr; t++, started++)
+                th.emplace_back([=] {
+                    const size_t a = n * t / nthr, b = n * (t + 1) / nthr;
+                    memcpy(buf + a, s + off + a, b - a);
+                });
+        } catch (...) {                 // no thread: this one copies the rest
+        }
+        memcpy(buf, s + off, n / nthr);
+        if (started < nthr)
+            memcpy(buf + n * started / nthr, s + off + n * started / nthr, n - n * started / nthr);
+        for (auto &x : th) x.join();
+        CK(cudaMemcpyAsync(d + off, buf, n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaEventRecord(ctx->stage_done[k & 1], ctx->stream));
+        off += n;
+    }
+    return AB_OK;
+}
+
 static int use_device(ab_ctx *ctx)
 {
     CK(cudaSetDevice(ctx->device));
@@ -1113,6 +1166,10 @@ void ab_ctx_destroy(ab_ctx *ctx)
         ctx->sigs_x[i].release();
     }
     if (ctx->hcount) cudaFreeHost(ctx->hcount);
+    for (int i = 0; i < 2; i++) {
+        if (ctx->stage[i]) cudaFreeHost(ctx->stage[i]);
+        if (ctx->stage_done[i]) cudaEventDestroy(ctx->stage_done[i]);
+    }
     for (int i = 0; i < ab_ctx::kHitSets; i++)
         if (ctx->batch_done[i]) cudaEventDestroy(ctx->batch_done[i]);
     if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
@@ -1468,8 +1525,8 @@ int ab_dedisperse(ab_ctx *ctx, const float *data, int data_on_device, long long 
     const float *dx = data;
     if (!data_on_device) {
         CK(ctx->dd_x.ensure(nx));
-        CK(cudaMemcpyAsync(ctx->dd_x.p, data, sizeof(float) * nx, cudaMemcpyHostToDevice,
-                           ctx->stream));
+        rc = h2d_staged(ctx, ctx->dd_x.p, data, sizeof(float) * nx);
+        if (rc) return rc;
         dx = ctx->dd_x.p;
     }
     CK(ctx->dd_sub.ensure((size_t) nsub * (size_t) dedisp_sub_pitch(nout)));
